@@ -1,0 +1,430 @@
+#!/usr/bin/env python
+"""Benchmark: PBiCGSTAB + RB-GS(5) time-to-eps on the Heat3ds Mode-3 IC stack, 240x240x30.
+
+One step = one steady solve from theta = 300 K to ||r||/||r0|| <= 1e-8 on inputs resident in
+HBM: the headline is the mixed-precision solver (FP32 operator, smoother and Krylov vectors
+inside FP64 iterative refinement); the plain FP64 GPU solver is timed on the same inputs.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 (torchrun, one process per GPU): every rank runs its own replica of the solve (the solve
+does not shard), timing is the max over ranks.  --impl reference times the
+reference's CPU algorithm (the oracle port, OpenMP on all host cores) on a bounded sample of
+iterations, scaled to the iterations its FP64 solve needs.  One JSON line on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "PBiCGSTAB time-to-eps (s) + stencil HBM GB/s, mixed vs FP64 GPU at 240^2x30"
+L2_FLUSH_BYTES = 256 << 20
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--nx", type=int, default=240)
+    ap.add_argument("--nz", type=int, default=30)
+    ap.add_argument("--tol", type=float, default=1e-8)
+    ap.add_argument("--inner-tol", type=float, default=1e-4)
+    ap.add_argument("--kernel-reps", type=int, default=30)
+    ap.add_argument("--cpu-sample-iters", type=int, default=0, help="0 = choose ~10 s of CPU work")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def workload_name(a):
+    return (f"{a.nx}x{a.nx}x{a.nz} Mode-3 IC stack, steady, PBiCGSTAB + RB-GS(5 sweeps), "
+            f"FP32 inner / FP64 refinement to ||r||/||r0|| <= {a.tol:g}")
+
+
+# ----------------------------------------------------------------------------------------------
+# distributed plumbing (one process per GPU; replicas)
+# ----------------------------------------------------------------------------------------------
+class Dist:
+    def __init__(self):
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+
+    def init(self, backend):
+        if self.world > 1:
+            import datetime
+
+            import torch.distributed as dist
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, x: float) -> float:
+        if not self.pg:
+            return x
+        import torch
+        dev = "cuda" if torch.cuda.is_available() else "cpu"
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", self.gpu_id, f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception as e:  # pragma: no cover
+            log("clock sampling unavailable:", e)
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) >= 9:
+                rows.append(p)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+        sm = [num(r[1]) for r in rows if num(r[1]) is not None]
+        smax = max(num(r[2]) or 0 for r in rows)
+        load = [s for s in sm if s > 0.5 * smax] or sm
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for n, v in zip(names, r[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(load)), "sm_max_mhz": smax, "samples": len(rows),
+                "power_w_max": max(num(r[3]) or 0 for r in rows), "reasons": sorted(reasons)}
+
+
+def gpu_id_for(torch, dev: int) -> str:
+    try:
+        u = str(torch.cuda.get_device_properties(dev).uuid)
+        return u if u.startswith("GPU-") else "GPU-" + u
+    except Exception:
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+        return vis.split(",")[dev] if vis else str(dev)
+
+
+# ----------------------------------------------------------------------------------------------
+# CPU baseline / reference arm: the oracle port (the reference's algorithm), all host threads
+# ----------------------------------------------------------------------------------------------
+def fp64_reference_iterations(nx: int, nz: int, tol: float) -> int | None:
+    """Iterations the reference's FP64 PBiCGSTAB needs for this workload (committed oracle run)."""
+    p = os.path.join(ROOT, "tests", "golden", "oracle_240_1e-8.json")
+    if nx == 240 and nz == 30 and tol == 1e-8 and os.path.exists(p):
+        return int(json.load(open(p))["itr"])
+    return None
+
+
+class CpuBaseline:
+    def __init__(self, nx, nz):
+        from oracle import oracle as O  # the reference's algorithm restated in C (checker/baseline only)
+        O.build()
+        self.O = O
+        self.cores = os.cpu_count()
+        t = time.perf_counter()
+        self.prob0 = O.build_mode3(nx, nx, nz, threads=self.cores)
+        log(f"oracle model {nx}x{nx}x{nz}: {time.perf_counter() - t:.1f} s")
+
+    def time_iters(self, iters: int) -> float:
+        import copy
+        prob = copy.deepcopy(self.prob0)
+        t = time.perf_counter()
+        self.O.pbicgstab(prob, tol=0.0, maxItr=iters, smoother="gs", red_mode=self.O.RED_OMP, threads=self.cores)
+        return time.perf_counter() - t
+
+    def calibrate(self, target_s=10.0) -> int:
+        t1 = self.time_iters(2) / 2
+        return max(3, min(200, int(target_s / max(t1, 1e-4))))
+
+
+def run_reference(a, dist: Dist):
+    dist.init("gloo")
+    if dist.rank != 0:
+        dist.close()
+        return
+    iters_ref = fp64_reference_iterations(a.nx, a.nz, a.tol)
+    cb = CpuBaseline(a.nx, a.nz)
+    per_step = a.cpu_sample_iters or max(3, cb.calibrate(target_s=2.5))
+    for _ in range(a.warmup):
+        cb.time_iters(per_step)
+    times = [cb.time_iters(per_step) for _ in range(a.steps)]
+    t_iter = float(np.mean(times)) / per_step
+    if iters_ref is None:
+        iters_ref = 315
+    value = t_iter * iters_ref
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "s", "n_gpus": a.gpus, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": 1e3 * float(np.mean(times)), "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (reference Mode-3 model)",
+        "config": {"workload": workload_name(a).replace("FP32 inner / FP64 refinement", "FP64"),
+                   "grid": [a.nx, a.nx, a.nz], "tol": a.tol, "parallelism": "host threads"},
+        "cpu_baseline": {"value": value, "unit": "s", "cores": cb.cores, "kind": "port",
+                         "sample": f"{per_step} PBiCGSTAB iterations per step (OpenMP reductions, "
+                                   f"{cb.cores} threads), scaled to the {iters_ref} iterations the FP64 "
+                                   f"solve needs"},
+        "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "seconds_per_iteration": t_iter,
+    }
+    print(json.dumps(line), flush=True)
+    dist.close()
+
+
+# ----------------------------------------------------------------------------------------------
+# our arm
+# ----------------------------------------------------------------------------------------------
+def run_ours(a, dist: Dist):
+    import torch
+
+    import h2_b200
+    from h2_b200 import _lib as L
+    from h2_b200 import model as M
+
+    dist.init("nccl")
+    dev = dist.local
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream()
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+
+    t = time.perf_counter()
+    m = M.build_mode3(a.nx, a.nx, a.nz)
+    log(f"[rank {dist.rank}] model {a.nx}x{a.nx}x{a.nz} (GPU fillID!): {time.perf_counter() - t:.2f} s")
+    w = m.wk
+
+    def make(precision):
+        s = h2_b200.Solver(*m.shape, precision=precision, stream=stream.cuda_stream)
+        s.set_grid(m.ZC, m.dZ, m.dx, m.dy, m.dt, m.HC, True)
+        s.set_fields(w.lam, w.mask)
+        s.set_rhs(w.b)
+        s.set_theta(w.theta)
+        s.snapshot()
+        if precision == "mixed":
+            s.set_mixed_params(a.inner_tol, 40)
+        return s
+
+    solvers = {"mixed": make("mixed"), "fp64": make("fp64")}
+
+    def one(s, timed: bool):
+        s.snapshot(restore=True)
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        st, res = s.solve("pbicgstab", tol=a.tol, maxItr=20000, smoother="gs")
+        ev1.record(stream)
+        ev1.synchronize()
+        if st != 0:
+            raise RuntimeError(f"solve did not converge: status {st}")
+        return ev0.elapsed_time(ev1) * 1e-3, res
+
+    results = {}
+    clocks = Clocks(gpu_id_for(torch, dev))
+    for name in ("mixed", "fp64"):
+        s = solvers[name]
+        for _ in range(a.warmup):
+            one(s, False)
+        torch.cuda.synchronize()
+        dist.barrier()
+        if name == "mixed":
+            clocks.start()
+        times, launches, res = [], 0, None
+        for _ in range(a.steps):
+            dt_, res = one(s, True)
+            times.append(dt_)
+            launches += res.launches
+        torch.cuda.synchronize()
+        dist.barrier()
+        results[name] = dict(t=dist.max(float(np.mean(times))), times=times, res=res, launches=launches)
+    clk = clocks.stop()
+
+    th = {k: solvers[k].get_theta()[1:-1, 1:-1, 1:-1] for k in solvers}
+    max_dtheta = float(np.abs(th["mixed"] - th["fp64"]).max())
+
+    # ---- roofline of the dominant kernel: one RB-GS sweep (2 colour passes) of the FP32 smoother
+    peak, peak_kind = measured_peaks()
+    N = a.nx * a.nx * a.nz
+    roof = {}
+    for name, w_elem in (("mixed", 4), ("fp64", 8)):
+        s = solvers[name]
+        for kind, bytes_per_cell, label in ((0, 3 * w_elem + 1, "rb_sweep"), (1, 2 * w_elem + 1, "calcax")):
+            ts = []
+            for r in range(a.kernel_reps + 3):
+                with torch.cuda.stream(stream):
+                    flush.zero_()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                s.bench_kernel(kind, 1)
+                e1.record(stream)
+                e1.synchronize()
+                if r >= 3:
+                    ts.append(e0.elapsed_time(e1) * 1e-3)
+            tk = float(np.mean(ts))
+            roof[(name, label)] = dict(seconds=tk, bytes=bytes_per_cell * N, gbs=bytes_per_cell * N / tk / 1e9)
+
+    # ---- end to end through the public drop-in call with pinned host buffers
+    e2e = None
+    try:
+        shape = m.shape
+        nf = int(np.prod(shape))
+
+        def pinned():
+            t_ = torch.empty(nf, dtype=torch.float64, pin_memory=True)
+            return t_, np.ndarray(shape, dtype=np.float64, buffer=t_.numpy(), order="F")
+
+        keep = []
+        wk = h2_b200.WorkBuffers.allocate(*shape)
+        for f in ("theta", "b", "lam", "mask", "rho", "cp"):
+            t_, arr = pinned()
+            keep.append(t_)
+            arr[...] = getattr(w, f)
+            setattr(wk, f, arr)
+        theta0 = w.theta.copy(order="F")
+        et = []
+        for r in range(a.warmup + a.steps):
+            wk.theta[...] = theta0
+            t0 = time.perf_counter()
+            conv, itr, res0 = h2_b200.PBiCGSTAB(wk, (m.dx, m.dy, 1.0), m.dt, m.ZC, m.dZ, m.HC, tol=a.tol,
+                                                smoother="gs", par="gpu", is_steady=True, precision="mixed")
+            t1 = time.perf_counter()
+            if not conv:
+                raise RuntimeError("e2e solve did not converge")
+            if r >= a.warmup:
+                et.append(t1 - t0)
+        L.load().h2g_release_cached()
+        e2e = {"value": dist.max(float(np.mean(et))), "unit": "s",
+               "h2d_bytes_per_step": 4 * 8 * nf + 8 * (2 * shape[2] + 6),
+               "d2h_bytes_per_step": 8 * nf,
+               "call": "h2g_PBiCGSTAB (one-call drop-in, host arrays in pinned memory)"}
+    except Exception as e:  # pragma: no cover
+        log("e2e failed:", e)
+
+    cpu = None
+    if dist.rank == 0 and dist.world == 1 and not a.no_cpu_baseline:
+        try:
+            cb = CpuBaseline(a.nx, a.nz)
+            iters = a.cpu_sample_iters or cb.calibrate(target_s=10.0)
+            tcpu = cb.time_iters(iters)
+            it64 = results["fp64"]["res"].itr
+            cpu = {"value": tcpu / iters * it64, "unit": "s", "cores": cb.cores, "kind": "port",
+                   "sample": f"{iters} FP64 PBiCGSTAB+RB-GS iterations of the oracle (OpenMP, {cb.cores} threads) "
+                             f"in {tcpu:.2f} s, scaled to the {it64} iterations of the FP64 solve"}
+        except Exception as e:  # pragma: no cover
+            log("cpu baseline failed:", e)
+
+    rm = roof[("mixed", "rb_sweep")]
+    out = {
+        "metric": METRIC,
+        "value": results["mixed"]["t"],
+        "unit": "s",
+        "n_gpus": dist.world,
+        "steps": a.steps,
+        "warmup": a.warmup,
+        "ms_per_step": results["mixed"]["t"] * 1e3,
+        "higher_is_better": False,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32+f64",
+        "data": "synthetic: the reference's Mode-3 IC-stack model (GPU fillID!, heat source 1.6e11 W/m^3 "
+                "on the power grids), theta_init = 300 K",
+        "config": {"workload": workload_name(a), "grid": [a.nx, a.nx, a.nz], "tol": a.tol,
+                   "inner_tol": a.inner_tol, "smoother": "RB-GS, 5 sweeps",
+                   "l2": "flushed (256 MiB write) before every timed solve and kernel launch",
+                   "parallelism": f"replicas x{dist.world}" if dist.world > 1 else "single GPU"},
+        "mixed": {"seconds": results["mixed"]["t"], "inner_iterations": results["mixed"]["res"].itr,
+                  "outer_passes": results["mixed"]["res"].outer, "final_rel_residual": results["mixed"]["res"].res,
+                  "max_abs_dtheta_vs_fp64_K": max_dtheta},
+        "fp64": {"seconds": results["fp64"]["t"], "iterations": results["fp64"]["res"].itr,
+                 "final_rel_residual": results["fp64"]["res"].res},
+        "speedup_mixed_vs_fp64": results["fp64"]["t"] / results["mixed"]["t"],
+        "roofline": {"bound": "hbm", "achieved": rm["gbs"], "peak": peak, "unit": "GB/s",
+                     "frac": rm["gbs"] / peak, "traffic": None,
+                     "kernel": "k_rb_pass<float>: one RB-GS sweep (both colour passes) of the FP32 smoother",
+                     "algorithmic_bytes": rm["bytes"], "seconds": rm["seconds"], "peak_kind": peak_kind},
+        "kernels": {f"{k[0]}_{k[1]}": v for k, v in roof.items()},
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+        "gpu_launches": results["mixed"]["launches"],
+        "clocks": clk,
+    }
+    if dist.rank == 0:
+        print(json.dumps(out), flush=True)
+    for s in solvers.values():
+        s.close()
+    dist.close()
+
+
+def main():
+    a = parse()
+    dist = Dist()
+    if a.impl == "reference":
+        run_reference(a, dist)
+    else:
+        run_ours(a, dist)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,671 @@
+// h2g_kernels.cuh -- sm_100a kernels of the Heat3ds solver path.
+//
+// Operator (src/NonUniform.jl:372-511, 848-915).  Every stencil evaluation needs, per cell,
+// six face conductances, six convective terms and the diagonal dd.  The reference recomputes
+// them from lambda and mask with eight FP64 divisions per cell.  Here each cell carries one
+// byte: a material key (index of its lambda value, bits 0-6) and its mask (bit 7).  The face
+// conductance between two keys a, b at plane k,
+//     ((lambda_f(a,b,ma,mb) * dy0) * dz_k) * ddx           (x faces, NonUniform.jl:482-483)
+// depends only on (k, a, b, fac) with fac = 2 - div(ma+mb, 2) in {1, 2}, so the host tabulates
+// it once per solve in exactly the reference's operation order; the kernels look it up.
+// FP64 results are therefore bit-identical to the reference's per-cell arithmetic.
+#pragma once
+#include "h2g_internal.cuh"
+
+namespace h2g {
+
+constexpr int kBX = 32;  // threads along the half-row
+constexpr int kBY = 8;   // rows per block
+constexpr int kThreads = kBX * kBY;
+
+// ------------------------------------------------------------------------------------------
+// Deterministic reductions: every block writes its partial sums; the last block to finish
+// (atomic ticket) adds all partials in a fixed order and runs the stage's scalar logic.
+// ------------------------------------------------------------------------------------------
+template <int NV>
+__device__ __forceinline__ void block_sum(double (&v)[NV], double (*sm)[NV], int tid, int nthr) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+    for (int q = 0; q < NV; ++q) v[q] += __shfl_down_sync(0xffffffffu, v[q], o);
+  const int lane = tid & 31, warp = tid >> 5, nw = (nthr + 31) >> 5;
+  if (lane == 0)
+#pragma unroll
+    for (int q = 0; q < NV; ++q) sm[warp][q] = v[q];
+  __syncthreads();
+  if (warp == 0) {
+#pragma unroll
+    for (int q = 0; q < NV; ++q) v[q] = lane < nw ? sm[lane][q] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+      for (int q = 0; q < NV; ++q) v[q] += __shfl_down_sync(0xffffffffu, v[q], o);
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ void set_cond(cudaGraphConditionalHandle h, int use_cond, int value) {
+  if (use_cond) cudaGraphSetConditional(h, value ? 1u : 0u);
+}
+
+// Scalar logic of each stage (runs on one thread).  Mirrors the control flow of PBiCGSTAB!
+// (NonUniform.jl:262-349) and CG! (NonUniform.jl:131-225).
+__device__ void finish_stage(int stage, SolverState* st, double s1, double s2) {
+  switch (stage) {
+    case kStageInit:  // NonUniform.jl:263-294: res0, early return, rho of iteration 1
+    case kStageInitCg: {
+      const double res0 = sqrt(s1);
+      st->res0 = res0;
+      st->res = 1.0;
+      st->rho = s1;
+      st->rho_old = 1.0;
+      st->alpha = 0.0;
+      st->omega = 1.0;
+      st->beta = 0.0;
+      st->itr = 1;
+      st->first = 1;
+      st->stop = 0;
+      st->converged = 0;
+      st->reason = kRunning;
+      if (res0 == 0.0) {
+        st->stop = 1; st->converged = 1; st->itr = 0; st->res = 0.0; st->reason = kConverged;
+      } else if (!isfinite(res0)) {
+        st->stop = 1; st->itr = 0; st->reason = kNonFinite;
+      } else if (stage == kStageInit && fabs(s1) < kFloatMin) {
+        st->stop = 1; st->reason = kBreakdown;
+      }
+      break;
+    }
+    case kStageAlpha:  // NonUniform.jl:309
+      st->alpha = __ddiv_rn(st->rho, s1);
+      break;
+    case kStageOmega:  // NonUniform.jl:320-326
+      if (fabs(s1) < kFloatMin) { st->stop = 1; st->reason = kBreakdown; }
+      else st->omega = __ddiv_rn(s2, s1);
+      break;
+    case kStageUpdate: {  // NonUniform.jl:331-346 and the top of the next iteration 289-299
+      const double res = __ddiv_rn(sqrt(s1), st->res0);
+      if (st->hist && st->itr >= 1 && st->itr <= st->hist_len) st->hist[st->itr - 1] = res;
+      st->res = res;
+      st->first = 0;
+      if (res < st->tol) { st->stop = 1; st->converged = 1; st->reason = kConverged; break; }
+      if (!isfinite(res)) { st->stop = 1; st->reason = kNonFinite; break; }
+      if (st->itr >= st->maxItr) { st->stop = 1; st->reason = kMaxItr; break; }
+      st->rho_old = st->rho;
+      st->rho = s2;
+      st->itr += 1;
+      if (fabs(s2) < kFloatMin) { st->stop = 1; st->reason = kBreakdown; break; }
+      st->beta = __ddiv_rn(__dmul_rn(__ddiv_rn(st->rho, st->rho_old), st->alpha), st->omega);
+      break;
+    }
+    case kStageResid:
+      st->scale = sqrt(s1);
+      break;
+    case kStageCgInit:  // NonUniform.jl:155
+      st->rho_old = s1;
+      st->itr = 1;
+      break;
+    case kStageCgAlpha:  // NonUniform.jl:168-176
+      if (fabs(s1) < kFloatMin) { st->stop = 1; st->reason = kBreakdown; }
+      else st->alpha = __ddiv_rn(st->rho_old, s1);
+      break;
+    case kStageCgRes: {  // NonUniform.jl:185-198
+      const double res = __ddiv_rn(sqrt(s1), st->res0);
+      if (st->hist && st->itr >= 1 && st->itr <= st->hist_len) st->hist[st->itr - 1] = res;
+      st->res = res;
+      if (res < st->tol) { st->stop = 1; st->converged = 1; st->reason = kConverged; break; }
+      if (!isfinite(res)) { st->stop = 1; st->reason = kNonFinite; }
+      break;
+    }
+    case kStageCgBeta:  // NonUniform.jl:206-222, then the loop bound
+      if (fabs(s1) < kFloatMin) { st->stop = 1; st->reason = kBreakdown; break; }
+      st->beta = __ddiv_rn(s1, st->rho_old);
+      st->rho_old = s1;
+      if (st->itr >= st->maxItr) { st->stop = 1; st->reason = kMaxItr; break; }
+      st->itr += 1;
+      break;
+    case kStageDot:
+      st->dot1 = s1;
+      st->dot2 = s2;
+      break;
+    default:
+      break;
+  }
+}
+
+template <int NV>
+__device__ __forceinline__ void reduce_finish(double (&v)[NV], double* __restrict__ partials, SolverState* st,
+                                              int stage, cudaGraphConditionalHandle hc, int use_cond) {
+  __shared__ double sm[32][NV];
+  __shared__ int am_last;
+  const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+  const int nthr = blockDim.x * blockDim.y * blockDim.z;
+  const unsigned nb = gridDim.x * gridDim.y * gridDim.z;
+  const unsigned bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+  block_sum<NV>(v, sm, tid, nthr);
+  if (tid == 0) {
+#pragma unroll
+    for (int q = 0; q < NV; ++q) partials[(size_t)q * nb + bid] = v[q];
+    __threadfence();
+    const unsigned t = atomicAdd(&st->ticket, 1u);
+    am_last = (t == nb - 1);
+  }
+  __syncthreads();
+  if (!am_last) return;
+  __threadfence();
+  double acc[NV];
+#pragma unroll
+  for (int q = 0; q < NV; ++q) acc[q] = 0.0;
+  for (unsigned b = tid; b < nb; b += nthr)
+#pragma unroll
+    for (int q = 0; q < NV; ++q) acc[q] += __ldcg(partials + (size_t)q * nb + b);
+  block_sum<NV>(acc, sm, tid, nthr);
+  if (tid == 0) {
+    st->ticket = 0;
+    finish_stage(stage, st, acc[0], NV > 1 ? acc[NV > 1 ? 1 : 0] : 0.0);
+    // the loop continues only while the solve runs and the pass count is within maxItr + 1
+    set_cond(hc, use_cond, !st->stop && st->passes <= st->maxItr + 1);
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// Stencil coefficients of one cell from the key tables.
+// ------------------------------------------------------------------------------------------
+template <typename T>
+struct Coef {
+  T cxm, cxp, cym, cyp, czm, czp, dd;
+};
+
+template <typename T>
+__device__ __forceinline__ T face(const T* __restrict__ tab, int lvl, int P, int a0, uint8_t kn) {
+  const int f = (kn & 0x80) ? 0 : 1;  // fac = 2 - div(ma+mb,2): 1 if both unmasked, else 2
+  return __ldg(tab + (((size_t)lvl * 2 + f) * P + (kn & 0x7f)) * P + a0);
+}
+
+// Returns false for a masked cell (m0 = 0).  Order of the additions of dd follows
+// NonUniform.jl:501-502 exactly.
+template <typename T>
+__device__ __forceinline__ bool cell_coef(const OpParams<T>& op, int k, uint8_t k0, uint8_t kxm, uint8_t kxp,
+                                          uint8_t kym, uint8_t kyp, uint8_t kzm, uint8_t kzp, long long ci,
+                                          Coef<T>& c) {
+  if (!(k0 & 0x80)) return false;
+  const int P = op.P, a0 = k0 & 0x7f;
+  c.cxm = face(op.tx, k, P, a0, kxm);
+  c.cxp = face(op.tx, k, P, a0, kxp);
+  c.cym = face(op.ty, k, P, a0, kym);
+  c.cyp = face(op.ty, k, P, a0, kyp);
+  c.czm = face(op.tz, k, P, a0, kzm);
+  c.czp = face(op.tz, k + 1, P, a0, kzp);
+  const T* cv = op.conv + 4 * k;
+  const T vxm = (kxm & 0x80) ? T(0) : __ldg(cv + 0);
+  const T vxp = (kxp & 0x80) ? T(0) : __ldg(cv + 1);
+  const T vym = (kym & 0x80) ? T(0) : __ldg(cv + 2);
+  const T vyp = (kyp & 0x80) ? T(0) : __ldg(cv + 3);
+  const T vzm = (kzm & 0x80) ? T(0) : op.czm;
+  const T vzp = (kzp & 0x80) ? T(0) : op.czp;
+  T ap = T(0);
+  if (!op.steady) ap = mul(mul(mul(mul(op.rc[ci], op.dx0), op.dy0), __ldg(op.dzk + k)), op.ddt);
+  T s = add(c.cxp, c.cxm);
+  s = add(s, c.cyp);
+  s = add(s, c.cym);
+  s = add(s, c.czp);
+  s = add(s, c.czm);
+  s = add(s, vxp);
+  s = add(s, vxm);
+  s = add(s, vyp);
+  s = add(s, vym);
+  s = add(s, vzp);
+  s = add(s, vzm);
+  s = add(s, ap);
+  c.dd = add(T(0), s);  // (1 - m0) + (...) * m0 with m0 = 1
+  return true;
+}
+
+// ss of NonUniform.jl:505-507 (products summed left to right)
+template <typename T>
+__device__ __forceinline__ T nb_sum(const Coef<T>& c, T xp, T xm, T yp, T ym, T zp, T zm) {
+  T s = mul(c.cxp, xp);
+  s = add(s, mul(c.cxm, xm));
+  s = add(s, mul(c.cyp, yp));
+  s = add(s, mul(c.cym, ym));
+  s = add(s, mul(c.czp, zp));
+  s = add(s, mul(c.czm, zm));
+  return s;
+}
+
+// Offsets of a cell and its six neighbours in the device layout.
+struct Nbr {
+  long long c, xm, xp, ym, yp, zm, zp;
+};
+
+__device__ __forceinline__ Nbr neighbours(const Geo& g, int p, int col, int j, int k, int e) {
+  Nbr n;
+  const long long ro = g.row(col ^ 1, j, k);
+  n.c = g.row(col, j, k) + p;
+  n.xm = ro + p - 1 + e;
+  n.xp = ro + p + e;
+  n.ym = ro - 2 * g.HP + p;
+  n.yp = ro + 2 * g.HP + p;
+  n.zm = ro - g.plane + p;
+  n.zp = ro + g.plane + p;
+  return n;
+}
+
+// ------------------------------------------------------------------------------------------
+// rbsor_core! (NonUniform.jl:848-915): one colour pass of RB-SOR on x with rhs bb.
+// Grid (ceil(HI/32), ceil(NY/8), NZ); one thread per cell of the colour.
+// ------------------------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_rb_pass(OpParams<T> op, T* __restrict__ x, const T* __restrict__ bb,
+                                                       int color, T omega, const SolverState* __restrict__ st) {
+  if (st && st->stop) return;
+  const Geo& g = op.g;
+  const int p = blockIdx.x * kBX + threadIdx.x;
+  const int j = 1 + blockIdx.y * kBY + threadIdx.y;
+  const int k = 1 + blockIdx.z;
+  if (j > g.NY) return;
+  const int e = (1 + color + j + k) & 1;
+  const int i = 2 * p + e;
+  if (i < 1 || i > g.NX) return;
+  const Nbr n = neighbours(g, p, color, j, k, e);
+  const uint8_t* key = op.key;
+  Coef<T> c;
+  if (!cell_coef(op, k, key[n.c], key[n.xm], key[n.xp], key[n.ym], key[n.yp], key[n.zm], key[n.zp], n.c, c)) return;
+  const T pp = x[n.c];
+  const T ss = nb_sum(c, x[n.xp], x[n.xm], x[n.yp], x[n.ym], x[n.zp], x[n.zm]);
+  const T dp = sub(dvd(sub(ss, bb[n.c]), c.dd), pp);  // * m0 (= 1)
+  x[n.c] = add(pp, mul(omega, dp));
+}
+
+// ------------------------------------------------------------------------------------------
+// First colour pass of the preconditioner (xx starts at zero, the caller's myfill!,
+// NonUniform.jl:303/313), fused with the Krylov update that produces its right-hand side:
+//   VM 0: bb is given (CG: z = M^-1 r)
+//   VM 1: p = r (first iteration) or p = r + beta*(p - omega*q)    BiCG1!, NonUniform.jl:296-301
+//   VM 2: s = (-alpha)*q + r                                         Triad!, NonUniform.jl:310-311
+// Colour-0 cells get xx = ((0 - bb)/dd - 0)*m0; colour-1 cells get 0.  With smoother :none
+// (copy_only) xx = bb everywhere (mycopy!, NonUniform.jl:549-551).
+// Grid as k_rb_pass; each thread owns position p of both half-rows of row (j,k).
+// ------------------------------------------------------------------------------------------
+template <typename T, int VM>
+__global__ void __launch_bounds__(kThreads) k_rb_first(OpParams<T> op, T* __restrict__ xx, T* __restrict__ v,
+                                                        const T* __restrict__ r, const T* __restrict__ q,
+                                                        const SolverState* __restrict__ st, int copy_only) {
+  if (st && st->stop) return;
+  const Geo& g = op.g;
+  const int p = blockIdx.x * kBX + threadIdx.x;
+  const int j = 1 + blockIdx.y * kBY + threadIdx.y;
+  const int k = 1 + blockIdx.z;
+  if (j > g.NY) return;
+  T beta = T(0), omg = T(0), alpha = T(0);
+  int first = 0;
+  if (VM == 1) {
+    first = st->first;
+    beta = (T)st->beta;
+    omg = (T)st->omega;
+  } else if (VM == 2) {
+    alpha = (T)st->alpha;
+  }
+#pragma unroll
+  for (int col = 0; col < 2; ++col) {
+    const int e = (1 + col + j + k) & 1;
+    const int i = 2 * p + e;
+    if (i < 1 || i > g.NX) continue;
+    const long long ci = g.row(col, j, k) + p;
+    T b;
+    if (VM == 0) {
+      b = v[ci];
+    } else if (VM == 1) {
+      b = first ? r[ci] : add(r[ci], mul(beta, sub(v[ci], mul(omg, q[ci]))));
+      v[ci] = b;
+    } else {
+      b = add(mul(-alpha, q[ci]), r[ci]);
+      v[ci] = b;
+    }
+    T out = T(0);
+    if (copy_only) {
+      out = b;
+    } else if (col == 0) {
+      const Nbr n = neighbours(g, p, col, j, k, e);
+      const uint8_t* key = op.key;
+      Coef<T> c;
+      if (cell_coef(op, k, key[n.c], key[n.xm], key[n.xp], key[n.ym], key[n.yp], key[n.zm], key[n.zp], n.c, c)) {
+        const T ss = T(0);
+        const T dp = sub(dvd(sub(ss, b), c.dd), T(0));
+        out = add(T(0), dp);  // pp + omega*dp with pp = 0, omega = 1
+      }
+    }
+    xx[ci] = out;
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// CalcAX! (NonUniform.jl:454-511): y = A x, fused with up to two dot products
+//   d1 = sum y*u (u == nullptr: y*y),  d2 = sum y*w
+// and the stage finisher.  Grid (ceil(HI/32), ceil(2*NY/8), zc); block (32,8); rows of a block
+// interleave the two colours; each block walks planes k = 1+blockIdx.z, +gridDim.z, ...
+// ------------------------------------------------------------------------------------------
+template <typename T, int NDOT>
+__global__ void __launch_bounds__(kThreads) k_ax(OpParams<T> op, T* __restrict__ y, const T* __restrict__ x,
+                                                  const T* __restrict__ u, const T* __restrict__ w,
+                                                  SolverState* st, double* __restrict__ partials, int stage) {
+  if (st && st->stop) return;
+  const Geo& g = op.g;
+  const int p = blockIdx.x * kBX + threadIdx.x;
+  const int rr = blockIdx.y * kBY + threadIdx.y;
+  const int j = 1 + (rr >> 1), col = rr & 1;
+  double v[NDOT > 0 ? NDOT : 1];
+#pragma unroll
+  for (int q = 0; q < (NDOT > 0 ? NDOT : 1); ++q) v[q] = 0.0;
+  const int e0 = (1 + col + j) & 1;
+  for (int k = 1 + blockIdx.z; k <= g.NZ; k += gridDim.z) {
+    const int e = e0 ^ (k & 1);
+    const int i = 2 * p + e;
+    if (j > g.NY || i < 1 || i > g.NX) continue;
+    const Nbr n = neighbours(g, p, col, j, k, e);
+    const uint8_t* key = op.key;
+    Coef<T> c;
+    T out = T(0);
+    if (cell_coef(op, k, key[n.c], key[n.xm], key[n.xp], key[n.ym], key[n.yp], key[n.zm], key[n.zp], n.c, c)) {
+      const T ss = nb_sum(c, x[n.xp], x[n.xm], x[n.yp], x[n.ym], x[n.zp], x[n.zm]);
+      out = sub(ss, mul(c.dd, x[n.c]));
+    }
+    y[n.c] = out;
+    if (NDOT >= 1) v[0] += (double)out * (double)(u ? u[n.c] : out);
+    if (NDOT >= 2) v[1] += (double)out * (double)w[n.c];
+  }
+  if constexpr (NDOT > 0) reduce_finish<NDOT>(v, partials, st, stage, 0, 0);
+}
+
+// ------------------------------------------------------------------------------------------
+// CalcRK! (NonUniform.jl:372-434): r = (b - (ss - dd*th))*m0, sum r^2 -> stage.
+// Optional copy r0 = r (PBiCGSTAB's mycopy!, NonUniform.jl:274).  th and b are FP64; r is T.
+// ------------------------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_rk(OpParams<double> op, T* __restrict__ r, T* __restrict__ r0,
+                                                  const double* __restrict__ th, const double* __restrict__ b,
+                                                  SolverState* st, double* __restrict__ partials, int stage) {
+  const Geo& g = op.g;
+  const int p = blockIdx.x * kBX + threadIdx.x;
+  const int rr = blockIdx.y * kBY + threadIdx.y;
+  const int j = 1 + (rr >> 1), col = rr & 1;
+  double v[1] = {0.0};
+  const int e0 = (1 + col + j) & 1;
+  for (int k = 1 + blockIdx.z; k <= g.NZ; k += gridDim.z) {
+    const int e = e0 ^ (k & 1);
+    const int i = 2 * p + e;
+    if (j > g.NY || i < 1 || i > g.NX) continue;
+    const Nbr n = neighbours(g, p, col, j, k, e);
+    const uint8_t* key = op.key;
+    Coef<double> c;
+    double rs = 0.0;
+    if (cell_coef(op, k, key[n.c], key[n.xm], key[n.xp], key[n.ym], key[n.yp], key[n.zm], key[n.zp], n.c, c)) {
+      const double ss = nb_sum(c, th[n.xp], th[n.xm], th[n.yp], th[n.ym], th[n.zp], th[n.zm]);
+      rs = sub(b[n.c], sub(ss, mul(c.dd, th[n.c])));
+    }
+    r[n.c] = (T)rs;
+    if (r0) r0[n.c] = (T)rs;
+    v[0] += rs * rs;
+  }
+  reduce_finish<1>(v, partials, st, stage, 0, 0);
+}
+
+// ------------------------------------------------------------------------------------------
+// Element-wise kernels over whole vectors.  Guard and padding entries of every Krylov vector
+// are zero and stay zero, so these run linearly over the buffer with 16-byte accesses.
+// ------------------------------------------------------------------------------------------
+template <typename T>
+struct Vec16;
+template <>
+struct Vec16<double> {
+  using type = double2;
+  static constexpr int n = 2;
+};
+template <>
+struct Vec16<float> {
+  using type = float4;
+  static constexpr int n = 4;
+};
+
+template <typename T>
+__device__ __forceinline__ void ld16(const T* p, T (&a)[Vec16<T>::n]) {
+  const typename Vec16<T>::type v = *reinterpret_cast<const typename Vec16<T>::type*>(p);
+  const T* s = reinterpret_cast<const T*>(&v);
+#pragma unroll
+  for (int q = 0; q < Vec16<T>::n; ++q) a[q] = s[q];
+}
+template <typename T>
+__device__ __forceinline__ void st16(T* p, const T (&a)[Vec16<T>::n]) {
+  typename Vec16<T>::type v;
+  T* d = reinterpret_cast<T*>(&v);
+#pragma unroll
+  for (int q = 0; q < Vec16<T>::n; ++q) d[q] = a[q];
+  *reinterpret_cast<typename Vec16<T>::type*>(p) = v;
+}
+
+// BICG2! + Triad! + Fdot1/Fdot2 (NonUniform.jl:328-331 and the next 289):
+//   x += alpha*ph + omega*sh;  r = (-omega)*t + s;  d1 = (r,r), d2 = (r,r0) -> kStageUpdate
+template <typename T, typename TX>
+__global__ void __launch_bounds__(256) k_bicg_update(long long n, TX* __restrict__ x, const T* __restrict__ ph,
+                                                      const T* __restrict__ sh, T* __restrict__ r,
+                                                      const T* __restrict__ s, const T* __restrict__ t,
+                                                      const T* __restrict__ r0, SolverState* st,
+                                                      double* __restrict__ partials, cudaGraphConditionalHandle hc,
+                                                      int use_cond) {
+  // Fail-safe loop bound: block 0 counts the pass and ends the loop provisionally; only the
+  // finisher of this kernel (which runs after block 0 has arrived) can continue it.
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    st->passes += 1;
+    set_cond(hc, use_cond, 0);
+  }
+  if (st->stop) return;
+  constexpr int V = Vec16<T>::n;
+  const T alpha = (T)st->alpha, omega = (T)st->omega, nomega = (T)(-st->omega);
+  double v[2] = {0.0, 0.0};
+  const long long nv = n / V;
+  for (long long b = blockIdx.x * (long long)blockDim.x + threadIdx.x; b < nv; b += (long long)gridDim.x * blockDim.x) {
+    const long long o = b * V;
+    T a_ph[V], a_sh[V], a_s[V], a_t[V], a_r0[V], a_r[V];
+    ld16(ph + o, a_ph);
+    ld16(sh + o, a_sh);
+    ld16(s + o, a_s);
+    ld16(t + o, a_t);
+    ld16(r0 + o, a_r0);
+#pragma unroll
+    for (int q = 0; q < V; ++q) {
+      x[o + q] = (TX)add((T)x[o + q], add(mul(alpha, a_ph[q]), mul(omega, a_sh[q])));
+      a_r[q] = add(mul(nomega, a_t[q]), a_s[q]);
+      v[0] += (double)a_r[q] * (double)a_r[q];
+      v[1] += (double)a_r[q] * (double)a_r0[q];
+    }
+    st16(r + o, a_r);
+  }
+  reduce_finish<2>(v, partials, st, kStageUpdate, hc, use_cond);
+}
+
+// CG! fused update (NonUniform.jl:179-182) + Fdot1 (185): x += alpha*p; r -= alpha*q; (r,r)
+template <typename T, typename TX>
+__global__ void __launch_bounds__(256) k_cg_update(long long n, TX* __restrict__ x, const T* __restrict__ p,
+                                                    T* __restrict__ r, const T* __restrict__ q, SolverState* st,
+                                                    double* __restrict__ partials) {
+  if (st->stop) return;
+  constexpr int V = Vec16<T>::n;
+  const T alpha = (T)st->alpha;
+  double v[1] = {0.0};
+  const long long nv = n / V;
+  for (long long b = blockIdx.x * (long long)blockDim.x + threadIdx.x; b < nv; b += (long long)gridDim.x * blockDim.x) {
+    const long long o = b * V;
+    T a_p[V], a_q[V], a_r[V];
+    ld16(p + o, a_p);
+    ld16(q + o, a_q);
+    ld16(r + o, a_r);
+#pragma unroll
+    for (int k = 0; k < V; ++k) {
+      x[o + k] = (TX)add((T)x[o + k], mul(alpha, a_p[k]));
+      a_r[k] = sub(a_r[k], mul(alpha, a_q[k]));
+      v[0] += (double)a_r[k] * (double)a_r[k];
+    }
+    st16(r + o, a_r);
+  }
+  reduce_finish<1>(v, partials, st, kStageCgRes, 0, 0);
+}
+
+// d1 = (a,b) with an optional copy dst = b (CG: p = z and rho = (r,z), NonUniform.jl:152-155)
+template <typename T>
+__global__ void __launch_bounds__(256) k_dot(long long n, const T* __restrict__ a, const T* __restrict__ b,
+                                              T* __restrict__ dst, SolverState* st, double* __restrict__ partials,
+                                              int stage) {
+  if (st->stop) return;
+  constexpr int V = Vec16<T>::n;
+  double v[1] = {0.0};
+  const long long nv = n / V;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nv; i += (long long)gridDim.x * blockDim.x) {
+    const long long o = i * V;
+    T a_a[V], a_b[V];
+    ld16(a + o, a_a);
+    ld16(b + o, a_b);
+#pragma unroll
+    for (int k = 0; k < V; ++k) v[0] += (double)a_a[k] * (double)a_b[k];
+    if (dst) st16(dst + o, a_b);
+  }
+  reduce_finish<1>(v, partials, st, stage, 0, 0);
+}
+
+// CG! p = z + beta*p (NonUniform.jl:218-220); sets the loop condition.
+template <typename T>
+__global__ void __launch_bounds__(256) k_cg_pupd(long long n, T* __restrict__ p, const T* __restrict__ z,
+                                                  SolverState* st, cudaGraphConditionalHandle hc, int use_cond) {
+  const int stop = st->stop;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    st->passes += 1;
+    set_cond(hc, use_cond, !stop && st->passes <= st->maxItr + 1);
+  }
+  if (stop) return;
+  constexpr int V = Vec16<T>::n;
+  const T beta = (T)st->beta;
+  const long long nv = n / V;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nv; i += (long long)gridDim.x * blockDim.x) {
+    const long long o = i * V;
+    T a_p[V], a_z[V];
+    ld16(p + o, a_p);
+    ld16(z + o, a_z);
+#pragma unroll
+    for (int k = 0; k < V; ++k) a_p[k] = add(a_z[k], mul(beta, a_p[k]));
+    st16(p + o, a_p);
+  }
+}
+
+// Iterative refinement: scale the FP64 residual into the FP32 inner right-hand side,
+// r = r0 = (float)(r64 / ||r64||), e = 0, and start the inner solve (kStageInit).
+__global__ void __launch_bounds__(256) k_ir_prep(long long n, const double* __restrict__ r64, float* __restrict__ r,
+                                                  float* __restrict__ r0, float* __restrict__ e,
+                                                  const SolverState* __restrict__ outer, SolverState* inner,
+                                                  double* __restrict__ partials, int stage) {
+  const double inv = 1.0 / outer->scale;
+  double v[1] = {0.0};
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const float x = (float)(r64[i] * inv);
+    r[i] = x;
+    r0[i] = x;
+    e[i] = 0.0f;
+    v[0] += (double)x * (double)x;
+  }
+  reduce_finish<1>(v, partials, inner, stage, 0, 0);
+}
+
+// Host-controlled fields of a state: tolerance, iteration cap and residual history.
+__global__ void k_prime(SolverState* st, double tol, int maxItr, double* hist, int hist_len) {
+  st->tol = tol;
+  st->maxItr = maxItr;
+  st->hist = hist;
+  st->hist_len = hist_len;
+  st->stop = 0;
+  st->ticket = 0;
+  st->passes = 0;
+}
+
+// Iterative refinement: th += ||r64|| * e (FP64 accumulation of the FP32 correction).
+__global__ void __launch_bounds__(256) k_ir_apply(long long n, double* __restrict__ th, const float* __restrict__ e,
+                                                   const SolverState* __restrict__ outer) {
+  const double sc = outer->scale;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    th[i] += sc * (double)e[i];
+}
+
+// ------------------------------------------------------------------------------------------
+// Layout conversion between the reference's column-major arrays and the device layout.
+// ------------------------------------------------------------------------------------------
+template <typename T>
+__global__ void k_to_dev(Geo g, const double* __restrict__ src, T* __restrict__ dst) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y, k = blockIdx.z;
+  if (i >= g.MX) return;
+  dst[g.off(i, j, k)] = (T)src[(long long)i + (long long)g.MX * ((long long)j + (long long)g.MY * k)];
+}
+
+template <typename T>
+__global__ void k_from_dev(Geo g, const T* __restrict__ src, double* __restrict__ dst) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y, k = blockIdx.z;
+  if (i >= g.MX) return;
+  dst[(long long)i + (long long)g.MX * ((long long)j + (long long)g.MY * k)] = (double)src[g.off(i, j, k)];
+}
+
+// ------------------------------------------------------------------------------------------
+// Material keys.  Pass 1 collects the distinct lambda bit patterns into a small open-addressing
+// table and validates the fields; pass 2 writes key = index | mask << 7 in the device layout
+// (and rho*cp for transient grids).
+// ------------------------------------------------------------------------------------------
+enum FieldFlags { kFlagNonFinite = 1, kFlagMaskValue = 2, kFlagTooMany = 4 };
+
+__device__ __forceinline__ unsigned slot_hash(unsigned long long b) {
+  return (unsigned)((b * 0x9E3779B97F4A7C15ull) >> 56);
+}
+
+__global__ void k_collect_keys(Geo g, const double* __restrict__ lam, const double* __restrict__ mask,
+                               const double* __restrict__ rho, const double* __restrict__ cp,
+                               unsigned long long* __restrict__ slots, int* __restrict__ flags) {
+  const long long n = (long long)g.MX * g.MY * g.MZ;
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+    const double l = lam[c], m = mask[c];
+    int f = 0;
+    if (!isfinite(l) || !isfinite(m)) f |= kFlagNonFinite;
+    if (!(m == 0.0 || m == 1.0)) f |= kFlagMaskValue;
+    if (rho && !(isfinite(rho[c]) && isfinite(cp[c]))) f |= kFlagNonFinite;
+    if (f) atomicOr(flags, f);
+    if (!isfinite(l)) continue;
+    const unsigned long long b = (unsigned long long)__double_as_longlong(l);
+    unsigned h = slot_hash(b);
+    for (int probe = 0; probe < kHashSlots; ++probe, h = (h + 1) & (kHashSlots - 1)) {
+      unsigned long long cur = slots[h];
+      if (cur == b) break;
+      if (cur == ~0ull) {
+        cur = atomicCAS(slots + h, ~0ull, b);
+        if (cur == ~0ull || cur == b) break;
+      }
+      if (probe == kHashSlots - 1) atomicOr(flags, kFlagTooMany);
+    }
+  }
+}
+
+template <typename T>
+__global__ void k_make_keys(Geo g, const double* __restrict__ lam, const double* __restrict__ mask,
+                            const double* __restrict__ rho, const double* __restrict__ cp,
+                            const unsigned long long* __restrict__ slots, const int* __restrict__ slot_index,
+                            uint8_t* __restrict__ key, T* __restrict__ rc) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y, k = blockIdx.z;
+  if (i >= g.MX) return;
+  const long long c = (long long)i + (long long)g.MX * ((long long)j + (long long)g.MY * k);
+  const unsigned long long b = (unsigned long long)__double_as_longlong(lam[c]);
+  unsigned h = slot_hash(b);
+  int idx = 0;
+  for (int probe = 0; probe < kHashSlots; ++probe, h = (h + 1) & (kHashSlots - 1)) {
+    if (slots[h] == b) { idx = slot_index[h]; break; }
+  }
+  const long long o = g.off(i, j, k);
+  key[o] = (uint8_t)(idx | (mask[c] == 1.0 ? 0x80 : 0));
+  if (rc) rc[o] = (T)(rho[c] * cp[c]);
+}
+
+}  // namespace h2g

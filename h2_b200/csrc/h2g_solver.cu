@@ -1,0 +1,1154 @@
+// h2g_solver.cu -- host side of the B200 solver library: handle, operator tables, CUDA-graph
+// drivers for PBiCGSTAB!/CG! (src/NonUniform.jl:115-350) and the C ABI of include/h2g.h.
+//
+// One solve = one kernel (the initial residual) + one graph launch.  The graph holds a single
+// conditional WHILE node whose body is one Krylov iteration (about two dozen kernels); all
+// scalars (rho, alpha, omega, beta, the residual and the stop decision) live in device memory
+// and the last kernel of the body sets the loop condition, so the host does not synchronise
+// between iterations.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/h2g.h"
+#include "h2g_kernels.cuh"
+
+namespace h2g {
+
+static thread_local std::string g_err;
+
+static int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+#define CK(call)                                                                                      \
+  do {                                                                                                \
+    cudaError_t e_ = (call);                                                                          \
+    if (e_ != cudaSuccess) return fail(H2G_CUDA_ERROR, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), \
+                                       __FILE__, __LINE__);                                           \
+  } while (0)
+
+#define CKL()                                                                                             \
+  do {                                                                                                    \
+    cudaError_t e_ = cudaGetLastError();                                                                  \
+    if (e_ != cudaSuccess) return fail(H2G_CUDA_ERROR, "launch: %s (%s:%d)", cudaGetErrorString(e_), __FILE__, \
+                                       __LINE__);                                                         \
+  } while (0)
+
+// Graph of one solve: parent graph {WHILE node}, body = one iteration.
+struct SolveGraph {
+  cudaGraphExec_t exec = nullptr;
+  cudaGraph_t graph = nullptr;
+  bool cond = false;  // true: conditional WHILE node; false: body graph launched by a host loop
+  std::vector<unsigned char> sig;
+  void reset() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    exec = nullptr;
+    graph = nullptr;
+    sig.clear();
+  }
+};
+
+enum GraphKind { kGPbicg64 = 0, kGCg64 = 1, kGPbicg32 = 2, kGCg32 = 3, kGNum = 4 };
+
+template <typename T>
+struct OpTables {
+  T* tx = nullptr;
+  T* ty = nullptr;
+  T* tz = nullptr;
+  T* conv = nullptr;
+  T* dzk = nullptr;
+  T* rc = nullptr;
+  int pcap = 0;
+};
+
+struct Solver {
+  Geo g{};
+  int precision = H2G_FP64;
+  int device = 0;
+  int num_sms = 148;
+  cudaStream_t stream = nullptr;
+  cudaStream_t cap = nullptr;  // capture stream
+  bool grid_set = false, fields_set = false;
+  // grid (host)
+  std::vector<double> ZC, dZ;
+  double dx = 0, dy = 0, dt = 0, HC[6] = {0, 0, 0, 0, 0, 0};
+  int steady = 1;
+  // keys
+  uint8_t* key = nullptr;
+  int P = 0;
+  std::vector<double> lam_values;
+  unsigned long long* slots = nullptr;
+  int* slot_index = nullptr;
+  int* flags = nullptr;
+  OpTables<double> t64;
+  OpTables<float> t32;
+  bool rc_valid = false;
+  // FP64 state vectors (device layout)
+  double* th = nullptr;
+  double* b = nullptr;
+  double* th_snap = nullptr;
+  double* r64 = nullptr;
+  // Krylov vectors in working precision: r, r0, p, ph, q, s, sh, t (+ e for refinement)
+  void* kv[9] = {nullptr};
+  size_t elem = 8;
+  // column-major staging buffers (MX*MY*MZ doubles each)
+  double* stage[4] = {nullptr, nullptr, nullptr, nullptr};
+  // device scalars
+  SolverState* st = nullptr;     // outer / FP64 solve
+  SolverState* st_in = nullptr;  // inner FP32 solve
+  SolverState* st_host = nullptr;  // pinned mirror
+  double* partials = nullptr;
+  size_t partials_cap = 0;
+  double* hist = nullptr;
+  int hist_cap = 0;
+  SolveGraph graphs[kGNum][2];
+  // mixed-precision refinement settings
+  double inner_tol = 1e-4;
+  int max_outer = 40;
+  bool no_cond = false;
+
+  long long nfort() const { return (long long)g.MX * g.MY * g.MZ; }
+};
+
+}  // namespace h2g
+
+// The opaque handle of include/h2g.h is the solver itself.
+struct h2g_solver : public h2g::Solver {};
+
+namespace h2g {
+
+// ------------------------------------------------------------------------------------------
+// helpers
+// ------------------------------------------------------------------------------------------
+static int elementwise_blocks(const Solver* s) { return s->num_sms * 4; }
+
+static dim3 rb_grid(const Geo& g) { return dim3((g.HI + kBX - 1) / kBX, (g.NY + kBY - 1) / kBY, g.NZ); }
+
+static dim3 ax_grid(const Geo& g) {
+  const int xt = (g.HI + kBX - 1) / kBX, yt = (2 * g.NY + kBY - 1) / kBY;
+  int zc = (4096 + xt * yt - 1) / (xt * yt);
+  zc = std::max(1, std::min(zc, g.NZ));
+  return dim3(xt, yt, zc);
+}
+
+static size_t partials_needed(const Solver* s) {
+  dim3 a = ax_grid(s->g);
+  size_t nb = (size_t)a.x * a.y * a.z;
+  nb = std::max(nb, (size_t)elementwise_blocks(s));
+  return 2 * nb;
+}
+
+template <typename T>
+static T* kvec(Solver* s, int i) {
+  return reinterpret_cast<T*>(s->kv[i]);
+}
+enum { KR = 0, KR0 = 1, KP = 2, KPH = 3, KQ = 4, KS = 5, KSH = 6, KT = 7, KE = 8 };
+
+template <typename T>
+static OpParams<T> op_params(const Solver* s, const OpTables<T>& t) {
+  OpParams<T> op;
+  op.g = s->g;
+  op.key = s->key;
+  op.tx = t.tx;
+  op.ty = t.ty;
+  op.tz = t.tz;
+  op.conv = t.conv;
+  op.rc = t.rc;
+  op.dzk = t.dzk;
+  const double dx0 = s->dx, dy0 = s->dy;
+  op.czm = (T)((s->HC[4] * dx0) * dy0);
+  op.czp = (T)((s->HC[5] * dx0) * dy0);
+  op.dx0 = (T)dx0;
+  op.dy0 = (T)dy0;
+  op.ddt = (T)(1.0 / s->dt);
+  op.P = t.pcap;
+  op.steady = s->steady;
+  return op;
+}
+
+static void free_tables64(OpTables<double>& t) {
+  cudaFree(t.tx); cudaFree(t.ty); cudaFree(t.tz); cudaFree(t.conv); cudaFree(t.dzk); cudaFree(t.rc);
+  t = OpTables<double>();
+}
+static void free_tables32(OpTables<float>& t) {
+  cudaFree(t.tx); cudaFree(t.ty); cudaFree(t.tz); cudaFree(t.conv); cudaFree(t.dzk); cudaFree(t.rc);
+  t = OpTables<float>();
+}
+
+static void destroy(Solver* s) {
+  if (!s) return;
+  cudaSetDevice(s->device);
+  for (auto& gk : s->graphs)
+    for (auto& gg : gk) gg.reset();
+  cudaFree(s->key); cudaFree(s->slots); cudaFree(s->slot_index); cudaFree(s->flags);
+  free_tables64(s->t64);
+  free_tables32(s->t32);
+  cudaFree(s->th); cudaFree(s->b); cudaFree(s->th_snap); cudaFree(s->r64);
+  for (auto& p : s->kv) cudaFree(p);
+  for (auto& p : s->stage) cudaFree(p);
+  cudaFree(s->st); cudaFree(s->st_in); cudaFree(s->partials); cudaFree(s->hist);
+  if (s->st_host) cudaFreeHost(s->st_host);
+  if (s->cap) cudaStreamDestroy(s->cap);
+  delete static_cast<h2g_solver*>(s);
+}
+
+static int check_handle(const h2g_solver* hh) {
+  if (!hh) return fail(H2G_BAD_ARG, "null solver handle");
+  return H2G_OK;
+}
+
+// Column-major host array -> device layout (through the staging buffer).
+template <typename T>
+static int upload(Solver* s, const double* host, T* dev, int slot = 0) {
+  if (!host) return fail(H2G_BAD_ARG, "null host array");
+  const Geo& g = s->g;
+  CK(cudaMemcpyAsync(s->stage[slot], host, sizeof(double) * s->nfort(), cudaMemcpyHostToDevice, s->stream));
+  dim3 grid((g.MX + 127) / 128, g.MY, g.MZ);
+  k_to_dev<T><<<grid, 128, 0, s->stream>>>(g, s->stage[slot], dev);
+  CKL();
+  CK(cudaStreamSynchronize(s->stream));  // the caller may reuse its buffer on return
+  return H2G_OK;
+}
+
+template <typename T>
+static int download(Solver* s, const T* dev, double* host) {
+  if (!host) return fail(H2G_BAD_ARG, "null host array");
+  const Geo& g = s->g;
+  dim3 grid((g.MX + 127) / 128, g.MY, g.MZ);
+  k_from_dev<T><<<grid, 128, 0, s->stream>>>(g, dev, s->stage[0]);
+  CKL();
+  CK(cudaMemcpyAsync(host, s->stage[0], sizeof(double) * s->nfort(), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return H2G_OK;
+}
+
+static void invalidate_graphs(Solver* s) {
+  for (auto& gk : s->graphs)
+    for (auto& gg : gk) gg.reset();
+}
+
+// ------------------------------------------------------------------------------------------
+// Operator tables (host, FP64, in the reference's operation order; FP32 copies by rounding).
+// ------------------------------------------------------------------------------------------
+static int build_tables(Solver* s) {
+  if (!s->grid_set || !s->fields_set) return H2G_OK;
+  const Geo& g = s->g;
+  const int P = s->P;
+  const int pc = std::max(P, 8);
+  const double dx0 = s->dx, dy0 = s->dy;
+  const double ddx = 1.0 / dx0, ddy = 1.0 / dy0;
+  std::vector<double> LP((size_t)pc * pc, 0.0);
+  for (int a = 0; a < P; ++a)
+    for (int b = 0; b < P; ++b) {
+      const double la = s->lam_values[a], lb = s->lam_values[b];
+      LP[(size_t)a * pc + b] = 2.0 * la * lb / (la + lb);  // lambda_f without the mask factor, common.jl:35
+    }
+  const size_t lvl = (size_t)2 * pc * pc;
+  std::vector<double> tx(lvl * g.MZ, 0.0), ty(lvl * g.MZ, 0.0), tz(lvl * g.MZ, 0.0), conv(4 * (size_t)g.MZ, 0.0);
+  for (int k = 0; k < g.MZ; ++k) {
+    const double dz_k = s->dZ[k];
+    for (int f = 0; f < 2; ++f) {
+      const double fac = f == 0 ? 1.0 : 2.0;  // 2 - div(ma+mb, 2)
+      for (int a = 0; a < P; ++a)
+        for (int b = 0; b < P; ++b) {
+          const double lf = LP[(size_t)a * pc + b] * fac;
+          const size_t o = (size_t)k * lvl + (size_t)f * pc * pc + (size_t)a * pc + b;
+          tx[o] = lf * dy0 * dz_k * ddx;  // NonUniform.jl:482-483
+          ty[o] = lf * dx0 * dz_k * ddy;  // NonUniform.jl:484-485
+          if (k >= 1) tz[o] = lf * dx0 * dy0 / (s->ZC[k] - s->ZC[k - 1]);  // NonUniform.jl:486
+        }
+    }
+    conv[4 * k + 0] = s->HC[0] * dy0 * dz_k;  // NonUniform.jl:490-493
+    conv[4 * k + 1] = s->HC[1] * dy0 * dz_k;
+    conv[4 * k + 2] = s->HC[2] * dx0 * dz_k;
+    conv[4 * k + 3] = s->HC[3] * dx0 * dz_k;
+  }
+  // (re)allocate when the key capacity grows; graphs hold the pointers, so they are rebuilt
+  const size_t bytes_t = lvl * g.MZ;
+  if (s->t64.pcap != pc) {
+    free_tables64(s->t64);
+    free_tables32(s->t32);
+    invalidate_graphs(s);
+    CK(cudaMalloc(&s->t64.tx, sizeof(double) * bytes_t));
+    CK(cudaMalloc(&s->t64.ty, sizeof(double) * bytes_t));
+    CK(cudaMalloc(&s->t64.tz, sizeof(double) * bytes_t));
+    CK(cudaMalloc(&s->t64.conv, sizeof(double) * 4 * g.MZ));
+    CK(cudaMalloc(&s->t64.dzk, sizeof(double) * g.MZ));
+    s->t64.pcap = pc;
+    if (s->precision == H2G_MIXED) {
+      CK(cudaMalloc(&s->t32.tx, sizeof(float) * bytes_t));
+      CK(cudaMalloc(&s->t32.ty, sizeof(float) * bytes_t));
+      CK(cudaMalloc(&s->t32.tz, sizeof(float) * bytes_t));
+      CK(cudaMalloc(&s->t32.conv, sizeof(float) * 4 * g.MZ));
+      CK(cudaMalloc(&s->t32.dzk, sizeof(float) * g.MZ));
+      s->t32.pcap = pc;
+    }
+  }
+  CK(cudaMemcpyAsync(s->t64.tx, tx.data(), sizeof(double) * bytes_t, cudaMemcpyHostToDevice, s->stream));
+  CK(cudaMemcpyAsync(s->t64.ty, ty.data(), sizeof(double) * bytes_t, cudaMemcpyHostToDevice, s->stream));
+  CK(cudaMemcpyAsync(s->t64.tz, tz.data(), sizeof(double) * bytes_t, cudaMemcpyHostToDevice, s->stream));
+  CK(cudaMemcpyAsync(s->t64.conv, conv.data(), sizeof(double) * 4 * g.MZ, cudaMemcpyHostToDevice, s->stream));
+  CK(cudaMemcpyAsync(s->t64.dzk, s->dZ.data(), sizeof(double) * g.MZ, cudaMemcpyHostToDevice, s->stream));
+  if (s->precision == H2G_MIXED) {
+    auto to32 = [](const std::vector<double>& v) {
+      std::vector<float> o(v.size());
+      for (size_t i = 0; i < v.size(); ++i) o[i] = (float)v[i];
+      return o;
+    };
+    std::vector<float> fx = to32(tx), fy = to32(ty), fz = to32(tz), fc = to32(conv), fd = to32(s->dZ);
+    CK(cudaMemcpyAsync(s->t32.tx, fx.data(), sizeof(float) * bytes_t, cudaMemcpyHostToDevice, s->stream));
+    CK(cudaMemcpyAsync(s->t32.ty, fy.data(), sizeof(float) * bytes_t, cudaMemcpyHostToDevice, s->stream));
+    CK(cudaMemcpyAsync(s->t32.tz, fz.data(), sizeof(float) * bytes_t, cudaMemcpyHostToDevice, s->stream));
+    CK(cudaMemcpyAsync(s->t32.conv, fc.data(), sizeof(float) * 4 * g.MZ, cudaMemcpyHostToDevice, s->stream));
+    CK(cudaMemcpyAsync(s->t32.dzk, fd.data(), sizeof(float) * g.MZ, cudaMemcpyHostToDevice, s->stream));
+  }
+  // host vectors must stay alive until the copies ran
+  CK(cudaStreamSynchronize(s->stream));
+  return H2G_OK;
+}
+
+// ------------------------------------------------------------------------------------------
+// Graph capture of one Krylov iteration.
+// ------------------------------------------------------------------------------------------
+template <typename T, typename TX>
+static void launch_pbicg_body(Solver* s, cudaStream_t cs, const OpParams<T>& op, TX* x, SolverState* st,
+                              int smoother, cudaGraphConditionalHandle hc, int use_cond) {
+  const Geo& g = s->g;
+  T* r = kvec<T>(s, KR);
+  T* r0 = kvec<T>(s, KR0);
+  T* p = kvec<T>(s, KP);
+  T* ph = kvec<T>(s, KPH);
+  T* q = kvec<T>(s, KQ);
+  T* sv = kvec<T>(s, KS);
+  T* sh = kvec<T>(s, KSH);
+  T* t = kvec<T>(s, KT);
+  const dim3 rg = rb_grid(g), ag = ax_grid(g), blk(kBX, kBY);
+  const int none = smoother == H2G_SMOOTHER_NONE;
+  // p = r + beta (p - omega q); p_ = M^-1 p                     NonUniform.jl:296-305
+  k_rb_first<T, 1><<<rg, blk, 0, cs>>>(op, ph, p, r, q, st, none);
+  if (!none)
+    for (int pass = 1; pass < 2 * kSweeps; ++pass) k_rb_pass<T><<<rg, blk, 0, cs>>>(op, ph, p, pass & 1, T(1), st);
+  // q = A p_;  alpha = rho / (q, r0)                            NonUniform.jl:307-309
+  k_ax<T, 1><<<ag, blk, 0, cs>>>(op, q, ph, r0, nullptr, st, s->partials, kStageAlpha);
+  // s = r - alpha q; s_ = M^-1 s                                NonUniform.jl:310-315
+  k_rb_first<T, 2><<<rg, blk, 0, cs>>>(op, sh, sv, r, q, st, none);
+  if (!none)
+    for (int pass = 1; pass < 2 * kSweeps; ++pass) k_rb_pass<T><<<rg, blk, 0, cs>>>(op, sh, sv, pass & 1, T(1), st);
+  // t = A s_; omega = (t,s)/(t,t)                               NonUniform.jl:317-326
+  k_ax<T, 2><<<ag, blk, 0, cs>>>(op, t, sh, nullptr, sv, st, s->partials, kStageOmega);
+  // x += alpha p_ + omega s_; r = s - omega t; res; next rho    NonUniform.jl:328-346
+  k_bicg_update<T, TX><<<elementwise_blocks(s), 256, 0, cs>>>(g.n, x, ph, sh, r, sv, t, r0, st, s->partials, hc,
+                                                              use_cond);
+}
+
+template <typename T, typename TX>
+static void launch_cg_body(Solver* s, cudaStream_t cs, const OpParams<T>& op, TX* x, SolverState* st, int smoother,
+                           cudaGraphConditionalHandle hc, int use_cond) {
+  const Geo& g = s->g;
+  T* r = kvec<T>(s, KR);
+  T* p = kvec<T>(s, KP);
+  T* q = kvec<T>(s, KQ);
+  T* z = kvec<T>(s, KS);  // pcg_s holds z (NonUniform.jl:146)
+  const dim3 rg = rb_grid(g), ag = ax_grid(g), blk(kBX, kBY);
+  const int none = smoother == H2G_SMOOTHER_NONE;
+  const int nb = elementwise_blocks(s);
+  // q = A p; alpha = rho_old / (p,q)                             NonUniform.jl:164-176
+  k_ax<T, 1><<<ag, blk, 0, cs>>>(op, q, p, p, nullptr, st, s->partials, kStageCgAlpha);
+  // x += alpha p; r -= alpha q; res                              NonUniform.jl:179-198
+  k_cg_update<T, TX><<<nb, 256, 0, cs>>>(g.n, x, p, r, q, st, s->partials);
+  // z = M^-1 r                                                  NonUniform.jl:201-203
+  k_rb_first<T, 0><<<rg, blk, 0, cs>>>(op, z, r, nullptr, nullptr, st, none);
+  if (!none)
+    for (int pass = 1; pass < 2 * kSweeps; ++pass) k_rb_pass<T><<<rg, blk, 0, cs>>>(op, z, r, pass & 1, T(1), st);
+  // rho_new = (r,z); beta                                       NonUniform.jl:206-215
+  k_dot<T><<<nb, 256, 0, cs>>>(g.n, r, z, nullptr, st, s->partials, kStageCgBeta);
+  // p = z + beta p                                              NonUniform.jl:218-220
+  k_cg_pupd<T><<<nb, 256, 0, cs>>>(g.n, p, z, st, hc, use_cond);
+}
+
+template <typename T>
+static std::vector<unsigned char> signature(const OpParams<T>& op, int smoother, const void* x) {
+  std::vector<unsigned char> v(sizeof op + sizeof smoother + sizeof x);
+  memcpy(v.data(), &op, sizeof op);
+  memcpy(v.data() + sizeof op, &smoother, sizeof smoother);
+  memcpy(v.data() + sizeof op + sizeof smoother, &x, sizeof x);
+  return v;
+}
+
+template <typename T, typename TX>
+static int get_graph(Solver* s, int kind, int smoother, const OpParams<T>& op, TX* x, SolverState* st,
+                     SolveGraph** out) {
+  SolveGraph& G = s->graphs[kind][smoother ? 1 : 0];
+  std::vector<unsigned char> sig = signature(op, smoother, (const void*)x);
+  if (G.exec && G.sig == sig) {
+    *out = &G;
+    return H2G_OK;
+  }
+  G.reset();
+  const bool cg = (kind == kGCg64 || kind == kGCg32);
+  bool cond = !s->no_cond;
+  if (cond) {
+    cudaGraph_t parent = nullptr;
+    cudaGraphConditionalHandle hc = 0;
+    cudaGraphNode_t node;
+    cudaGraphNodeParams cp = {};
+    bool ok = cudaGraphCreate(&parent, 0) == cudaSuccess &&
+              cudaGraphConditionalHandleCreate(&hc, parent, 1, cudaGraphCondAssignDefault) == cudaSuccess;
+    if (ok) {
+      cp.type = cudaGraphNodeTypeConditional;
+      cp.conditional.handle = hc;
+      cp.conditional.type = cudaGraphCondTypeWhile;
+      cp.conditional.size = 1;
+      ok = cudaGraphAddNode(&node, parent, nullptr, 0, &cp) == cudaSuccess;
+    }
+    if (ok) {
+      cudaGraph_t body = cp.conditional.phGraph_out[0];
+      ok = cudaStreamBeginCaptureToGraph(s->cap, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) ==
+           cudaSuccess;
+      if (ok) {
+        if (cg) launch_cg_body<T, TX>(s, s->cap, op, x, st, smoother, hc, 1);
+        else launch_pbicg_body<T, TX>(s, s->cap, op, x, st, smoother, hc, 1);
+        cudaGraph_t got = nullptr;
+        ok = cudaStreamEndCapture(s->cap, &got) == cudaSuccess;
+      }
+    }
+    if (ok) ok = cudaGraphInstantiate(&G.exec, parent, 0) == cudaSuccess;
+    if (!ok) {
+      cudaGetLastError();
+      if (G.exec) cudaGraphExecDestroy(G.exec);
+      G.exec = nullptr;
+      if (parent) cudaGraphDestroy(parent);
+      cond = false;
+      s->no_cond = true;
+    } else {
+      G.graph = parent;
+      G.cond = true;
+    }
+  }
+  if (!cond) {
+    // fallback: a graph of one iteration, relaunched by the host until the state says stop
+    CK(cudaStreamBeginCapture(s->cap, cudaStreamCaptureModeRelaxed));
+    if (cg) launch_cg_body<T, TX>(s, s->cap, op, x, st, smoother, 0, 0);
+    else launch_pbicg_body<T, TX>(s, s->cap, op, x, st, smoother, 0, 0);
+    CK(cudaStreamEndCapture(s->cap, &G.graph));
+    CK(cudaGraphInstantiate(&G.exec, G.graph, 0));
+    G.cond = false;
+  }
+  G.sig = sig;
+  *out = &G;
+  return H2G_OK;
+}
+
+static int run_graph(Solver* s, SolveGraph* G, SolverState* st, int maxItr) {
+  if (G->cond) {
+    CK(cudaGraphLaunch(G->exec, s->stream));
+    return H2G_OK;
+  }
+  // host loop: batches of iterations between checks of the device stop flag
+  int done = 0;
+  const int batch = 8;
+  while (done < maxItr + 1) {
+    for (int i = 0; i < batch; ++i) CK(cudaGraphLaunch(G->exec, s->stream));
+    done += batch;
+    CK(cudaMemcpyAsync(s->st_host, st, sizeof(SolverState), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    if (s->st_host->stop) break;
+  }
+  return H2G_OK;
+}
+
+// Set the host-controlled fields of a device state (tolerance, iteration cap, history).
+static int prime_state(Solver* s, SolverState* st, double tol, int maxItr, double* hist, int hist_len) {
+  k_prime<<<1, 1, 0, s->stream>>>(st, tol, maxItr, hist, hist_len);
+  CKL();
+  return H2G_OK;
+}
+
+static int ensure_hist(Solver* s, int n) {
+  if (n <= s->hist_cap) return H2G_OK;
+  cudaFree(s->hist);
+  s->hist = nullptr;
+  s->hist_cap = 0;
+  CK(cudaMalloc(&s->hist, sizeof(double) * (size_t)n));
+  s->hist_cap = n;
+  return H2G_OK;
+}
+
+static int status_of(const SolverState& st) {
+  switch (st.reason) {
+    case kConverged: return H2G_OK;
+    case kBreakdown: return H2G_BREAKDOWN;
+    case kNonFinite: return H2G_NONFINITE;
+    default: return H2G_NOT_CONVERGED;
+  }
+}
+
+// Julia's shortest round-trip print of a Float64 (used for "Initial residual = ...").
+static void julia_repr(double x, char* out, size_t n) {
+  char buf[64];
+  for (int p = 1; p <= 17; ++p) {
+    snprintf(buf, sizeof buf, "%.*e", p - 1, x);
+    if (strtod(buf, nullptr) == x) break;
+  }
+  // buf = d.ddde[+-]XX
+  double ax = fabs(x);
+  if (x == 0.0 || (ax >= 1e-4 && ax < 1e16)) {
+    for (int p = 1; p <= 17; ++p) {
+      snprintf(out, n, "%.*f", p, x);
+      if (strtod(out, nullptr) == x) return;
+    }
+    snprintf(out, n, "%.17g", x);
+    return;
+  }
+  char* e = strchr(buf, 'e');
+  int ex = atoi(e + 1);
+  *e = 0;
+  if (!strchr(buf, '.')) strcat(buf, ".0");
+  snprintf(out, n, "%se%d", buf, ex);
+}
+
+static void print_log(const SolverState& st, const double* hist, int nhist, int converged) {
+  char rb[64];
+  julia_repr(st.res0, rb, sizeof rb);
+  printf("Initial residual = %s\n", rb);
+  for (int i = 0; i < nhist; ++i) printf("%10d %24.14E\n", i + 1, hist[i]);
+  if (converged) printf("Converged at %d\n", st.itr);
+  fflush(stdout);
+}
+
+// Kernels in one WHILE-body pass (one Krylov iteration).
+static long long body_kernels(bool cg, int smoother) {
+  const int pc = smoother == H2G_SMOOTHER_NONE ? 1 : 2 * kSweeps;  // passes per preconditioner call
+  return cg ? (1 + 1 + pc + 1 + 1) : (2 * pc + 2 + 1);
+}
+
+// FP64 PBiCGSTAB!/CG!: the same arithmetic as the reference, on the device.
+static int solve_fp64(Solver* s, bool cg, double tol, int maxItr, int smoother, int verbose, double* res_hist,
+                      h2g_result* out) {
+  const Geo& g = s->g;
+  int rc = ensure_hist(s, maxItr);
+  if (rc) return rc;
+  OpParams<double> op = op_params<double>(s, s->t64);
+  SolverState* st = s->st;
+  if ((rc = prime_state(s, st, tol, maxItr, s->hist, maxItr))) return rc;
+  double* r = kvec<double>(s, KR);
+  const dim3 ag = ax_grid(g), rg = rb_grid(g), blk(kBX, kBY);
+  // r = b - A theta, res0 (and r0 = r for PBiCGSTAB)            NonUniform.jl:131-141, 262-274
+  k_rk<double><<<ag, blk, 0, s->stream>>>(op, r, cg ? nullptr : kvec<double>(s, KR0), s->th, s->b, st, s->partials,
+                                          cg ? kStageInitCg : kStageInit);
+  CKL();
+  if (cg) {
+    // z = M^-1 r; p = z; rho_old = (r,z)                          NonUniform.jl:147-155
+    double* z = kvec<double>(s, KS);
+    const int none = smoother == H2G_SMOOTHER_NONE;
+    k_rb_first<double, 0><<<rg, blk, 0, s->stream>>>(op, z, r, nullptr, nullptr, st, none);
+    if (!none)
+      for (int pass = 1; pass < 2 * kSweeps; ++pass)
+        k_rb_pass<double><<<rg, blk, 0, s->stream>>>(op, z, r, pass & 1, 1.0, st);
+    k_dot<double><<<elementwise_blocks(s), 256, 0, s->stream>>>(g.n, r, z, kvec<double>(s, KP), st, s->partials,
+                                                                 kStageCgInit);
+    CKL();
+  }
+  SolveGraph* G = nullptr;
+  if ((rc = get_graph<double, double>(s, cg ? kGCg64 : kGPbicg64, smoother, op, s->th, st, &G))) return rc;
+  // a state that stopped at the start turns every kernel of the body into a no-op and the
+  // last one ends the WHILE loop after one pass
+  if ((rc = run_graph(s, G, st, maxItr))) return rc;
+  CK(cudaMemcpyAsync(s->st_host, st, sizeof(SolverState), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  SolverState fin = *s->st_host;
+  const int nh = std::min(std::max(fin.itr, 0), maxItr);
+  std::vector<double> hh(nh);
+  if (nh > 0 && (verbose || res_hist)) {
+    CK(cudaMemcpy(hh.data(), s->hist, sizeof(double) * nh, cudaMemcpyDeviceToHost));
+    if (res_hist) memcpy(res_hist, hh.data(), sizeof(double) * nh);
+  }
+  // a breakdown at the top of an iteration leaves no residual for that iteration
+  const int nprint = (fin.reason == kBreakdown || fin.reason == kNonFinite) ? std::min(nh, std::max(0, fin.itr - 1)) : nh;
+  if (verbose) print_log(fin, hh.data(), nprint, fin.converged);
+  if (out) {
+    const long long body = body_kernels(cg, smoother);
+    const long long pre = 2 + (cg ? (smoother == H2G_SMOOTHER_NONE ? 2 : 2 * kSweeps + 1) : 0);
+    out->launches = pre + body * std::max(1, fin.itr);
+    out->isconverged = fin.converged;
+    out->itr = fin.itr;
+    out->outer = 0;
+    out->status = status_of(fin);
+    out->res0 = fin.res0;
+    out->res = fin.res;
+  }
+  return status_of(fin);
+}
+
+// Mixed precision: FP32 PBiCGSTAB/CG (operator, smoother, Krylov vectors) inside FP64 iterative
+// refinement.  FP64 is kept for the true residual b - A theta, the accumulation of theta and
+// every inner product (the reductions accumulate in FP64).
+static int solve_mixed(Solver* s, bool cg, double tol, int maxItr, int smoother, int verbose, double* res_hist,
+                       h2g_result* out) {
+  const Geo& g = s->g;
+  int rc;
+  OpParams<double> op64 = op_params<double>(s, s->t64);
+  OpParams<float> op32 = op_params<float>(s, s->t32);
+  SolverState* st = s->st;
+  SolverState* si = s->st_in;
+  const dim3 ag = ax_grid(g), rg = rb_grid(g), blk(kBX, kBY);
+  const int nb = elementwise_blocks(s);
+  if ((rc = prime_state(s, st, tol, maxItr, nullptr, 0))) return rc;
+  // true residual r64 = b - A theta, ||r64||
+  k_rk<double><<<ag, blk, 0, s->stream>>>(op64, s->r64, nullptr, s->th, s->b, st, s->partials, kStageResid);
+  CKL();
+  CK(cudaMemcpyAsync(s->st_host, st, sizeof(SolverState), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  const double res0 = s->st_host->scale;
+  double res = res0 == 0.0 ? 0.0 : 1.0;
+  int total = 0, outer = 0, status = H2G_NOT_CONVERGED, converged = 0;
+  std::vector<double> hist_all;
+  if (res0 == 0.0) {
+    status = H2G_OK;
+    converged = 1;
+  } else if (!std::isfinite(res0)) {
+    status = H2G_NONFINITE;
+  }
+  if (!converged && status != H2G_NONFINITE) {
+    if ((rc = ensure_hist(s, maxItr))) return rc;
+    float* e = kvec<float>(s, KE);
+    SolveGraph* G = nullptr;
+    double scale = res0;
+    while (outer < s->max_outer && total < maxItr) {
+      ++outer;
+      const int cap = maxItr - total;
+      if ((rc = prime_state(s, si, s->inner_tol, cap, s->hist, cap))) return rc;
+      // inner right-hand side r = r64/||r64||, e = 0, inner res0 and rho
+      k_ir_prep<<<nb, 256, 0, s->stream>>>(g.n, s->r64, kvec<float>(s, KR), kvec<float>(s, KR0), e, st, si,
+                                           s->partials, cg ? kStageInitCg : kStageInit);
+      CKL();
+      if (cg) {
+        float* z = kvec<float>(s, KS);
+        const int none = smoother == H2G_SMOOTHER_NONE;
+        k_rb_first<float, 0><<<rg, blk, 0, s->stream>>>(op32, z, kvec<float>(s, KR), nullptr, nullptr, si, none);
+        if (!none)
+          for (int pass = 1; pass < 2 * kSweeps; ++pass)
+            k_rb_pass<float><<<rg, blk, 0, s->stream>>>(op32, z, kvec<float>(s, KR), pass & 1, 1.0f, si);
+        k_dot<float><<<nb, 256, 0, s->stream>>>(g.n, kvec<float>(s, KR), z, kvec<float>(s, KP), si, s->partials,
+                                                 kStageCgInit);
+        CKL();
+      }
+      if ((rc = get_graph<float, float>(s, cg ? kGCg32 : kGPbicg32, smoother, op32, e, si, &G))) return rc;
+      if ((rc = run_graph(s, G, si, cap))) return rc;
+      // theta += ||r64|| e ; r64 = b - A theta
+      k_ir_apply<<<nb, 256, 0, s->stream>>>(g.n, s->th, e, st);
+      k_rk<double><<<ag, blk, 0, s->stream>>>(op64, s->r64, nullptr, s->th, s->b, st, s->partials, kStageResid);
+      CKL();
+      SolverState inner;
+      CK(cudaMemcpyAsync(s->st_host, si, sizeof(SolverState), cudaMemcpyDeviceToHost, s->stream));
+      CK(cudaStreamSynchronize(s->stream));
+      inner = *s->st_host;
+      CK(cudaMemcpyAsync(s->st_host, st, sizeof(SolverState), cudaMemcpyDeviceToHost, s->stream));
+      CK(cudaStreamSynchronize(s->stream));
+      const double new_scale = s->st_host->scale;
+      const int ni = std::max(inner.itr, 0);
+      if (verbose || res_hist) {
+        std::vector<double> hh(std::min(ni, cap));
+        if (!hh.empty()) CK(cudaMemcpy(hh.data(), s->hist, sizeof(double) * hh.size(), cudaMemcpyDeviceToHost));
+        for (double v : hh) hist_all.push_back(v * scale / res0);
+      }
+      total += ni;
+      res = new_scale / res0;
+      scale = new_scale;
+      if (!std::isfinite(res)) { status = H2G_NONFINITE; break; }
+      if (res < tol) { status = H2G_OK; converged = 1; break; }
+      if (ni == 0) {  // the inner solve could not start (breakdown at its first iteration)
+        status = inner.reason == kNonFinite ? H2G_NONFINITE : H2G_BREAKDOWN;
+        break;
+      }
+    }
+  }
+  if (res_hist && !hist_all.empty())
+    memcpy(res_hist, hist_all.data(), sizeof(double) * std::min<size_t>(hist_all.size(), (size_t)maxItr));
+  if (verbose) {
+    SolverState fake;
+    memset(&fake, 0, sizeof fake);
+    fake.res0 = res0;
+    fake.itr = total;
+    print_log(fake, hist_all.data(), (int)std::min<size_t>(hist_all.size(), (size_t)maxItr), converged);
+  }
+  if (out) {
+    const long long body = body_kernels(cg, smoother);
+    const long long pre_inner = 2 + (cg ? (smoother == H2G_SMOOTHER_NONE ? 2 : 2 * kSweeps + 1) : 0);
+    out->launches = 2 + (long long)outer * (pre_inner + 2) + body * std::max(total, outer);
+    out->isconverged = converged;
+    out->itr = total;
+    out->outer = outer;
+    out->status = status;
+    out->res0 = res0;
+    out->res = res;
+  }
+  return status;
+}
+
+static int solve(Solver* s, bool cg, double tol, int maxItr, int smoother, int verbose, double* res_hist,
+                 h2g_result* out) {
+  if (!s->grid_set || !s->fields_set) return fail(H2G_BAD_ARG, "h2g_set_grid and h2g_set_fields must come first");
+  if (maxItr < 1 || maxItr > 10000000) return fail(H2G_BAD_ARG, "maxItr out of range: %d", maxItr);
+  if (smoother != H2G_SMOOTHER_NONE && smoother != H2G_SMOOTHER_GS)
+    return fail(H2G_BAD_ARG, "Unsupported smoother: %d. Use none (0) or gs (1)", smoother);
+  if (!(tol >= 0.0) || !std::isfinite(tol)) return fail(H2G_BAD_ARG, "bad tolerance");
+  CK(cudaSetDevice(s->device));
+  if (s->precision == H2G_MIXED) return solve_mixed(s, cg, tol, maxItr, smoother, verbose, res_hist, out);
+  return solve_fp64(s, cg, tol, maxItr, smoother, verbose, res_hist, out);
+}
+
+// ------------------------------------------------------------------------------------------
+// creation and set-up
+// ------------------------------------------------------------------------------------------
+static int create(int MX, int MY, int MZ, int precision, Solver** out) {
+  if (!out) return fail(H2G_BAD_ARG, "null output pointer");
+  *out = nullptr;
+  if (MX < 3 || MY < 3 || MZ < 3) return fail(H2G_BAD_ARG, "grid too small: (%d,%d,%d)", MX, MY, MZ);
+  if ((long long)MX * MY * MZ > (1ll << 31)) return fail(H2G_BAD_ARG, "grid too large");
+  if (precision != H2G_FP64 && precision != H2G_MIXED) return fail(H2G_BAD_ARG, "unknown precision %d", precision);
+  Solver* s = new h2g_solver();
+  s->g = make_geo(MX, MY, MZ);
+  s->precision = precision;
+  s->elem = precision == H2G_MIXED ? 4 : 8;
+  const char* nc = getenv("H2G_NO_COND");
+  s->no_cond = nc && nc[0] == '1';
+  int rc = H2G_OK;
+  auto bail = [&](int code) {
+    destroy(s);
+    return code;
+  };
+  if (cudaGetDevice(&s->device) != cudaSuccess) return bail(fail(H2G_CUDA_ERROR, "no CUDA device"));
+  cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, s->device);
+  const Geo& g = s->g;
+  const size_t nb = sizeof(double) * (size_t)g.n;
+#define AL(ptr, bytes)                                                                     \
+  do {                                                                                     \
+    if (cudaMalloc((void**)&(ptr), (bytes)) != cudaSuccess || cudaMemset((ptr), 0, (bytes)) != cudaSuccess) \
+      return bail(fail(H2G_CUDA_ERROR, "cudaMalloc of %zu bytes failed", (size_t)(bytes)));                \
+  } while (0)
+  AL(s->th, nb);
+  AL(s->b, nb);
+  AL(s->th_snap, nb);
+  AL(s->key, (size_t)g.n);
+  const size_t kvb = s->elem * (size_t)g.n;
+  for (int i = 0; i < 8; ++i) AL(s->kv[i], kvb);
+  if (precision == H2G_MIXED) {
+    AL(s->kv[KE], kvb);
+    AL(s->r64, nb);
+  }
+  for (int i = 0; i < 4; ++i) AL(s->stage[i], sizeof(double) * (size_t)s->nfort());
+  AL(s->st, sizeof(SolverState));
+  AL(s->st_in, sizeof(SolverState));
+  s->partials_cap = partials_needed(s);
+  AL(s->partials, sizeof(double) * s->partials_cap);
+  AL(s->slots, sizeof(unsigned long long) * kHashSlots);
+  AL(s->slot_index, sizeof(int) * kHashSlots);
+  AL(s->flags, sizeof(int));
+#undef AL
+  if (cudaMallocHost(&s->st_host, sizeof(SolverState)) != cudaSuccess)
+    return bail(fail(H2G_CUDA_ERROR, "cudaMallocHost failed"));
+  if (cudaStreamCreateWithFlags(&s->cap, cudaStreamNonBlocking) != cudaSuccess)
+    return bail(fail(H2G_CUDA_ERROR, "cudaStreamCreate failed"));
+  (void)rc;
+  *out = s;
+  return H2G_OK;
+}
+
+static int set_grid(Solver* s, const double* ZC, const double* dZ, double dx, double dy, double dt, const double* HC,
+                    int is_steady) {
+  if (!ZC || !dZ || !HC) return fail(H2G_BAD_ARG, "null ZC/dZ/HC");
+  if (!(dx > 0) || !(dy > 0) || !std::isfinite(dx) || !std::isfinite(dy)) return fail(H2G_BAD_ARG, "bad dx/dy");
+  if (!is_steady && !(dt > 0 && std::isfinite(dt))) return fail(H2G_BAD_ARG, "bad dt");
+  const int MZ = s->g.MZ;
+  for (int k = 0; k < MZ; ++k)
+    if (!std::isfinite(ZC[k]) || !std::isfinite(dZ[k])) return fail(H2G_NONFINITE, "non-finite ZC/dZ");
+  for (int f = 0; f < 6; ++f)
+    if (!std::isfinite(HC[f])) return fail(H2G_NONFINITE, "non-finite HC");
+  s->ZC.assign(ZC, ZC + MZ);
+  s->dZ.assign(dZ, dZ + MZ);
+  s->dx = dx;
+  s->dy = dy;
+  s->dt = is_steady ? (dt > 0 ? dt : 1.0) : dt;
+  memcpy(s->HC, HC, sizeof s->HC);
+  const int was_steady = s->steady;
+  s->steady = is_steady ? 1 : 0;
+  s->grid_set = true;
+  if (s->fields_set && !s->steady && (was_steady || !s->rc_valid))
+    return fail(H2G_BAD_ARG, "switching to a transient grid needs h2g_set_fields with rho and cp");
+  return build_tables(s);
+}
+
+static int set_fields(Solver* s, const double* lam, const double* mask, const double* rho, const double* cp) {
+  if (!lam || !mask) return fail(H2G_BAD_ARG, "null lambda/mask");
+  if ((rho == nullptr) != (cp == nullptr)) return fail(H2G_BAD_ARG, "rho and cp must both be given or both be NULL");
+  if (s->grid_set && !s->steady && !rho) return fail(H2G_BAD_ARG, "transient grid needs rho and cp");
+  const Geo& g = s->g;
+  const size_t nf = sizeof(double) * (size_t)s->nfort();
+  CK(cudaMemcpyAsync(s->stage[0], lam, nf, cudaMemcpyHostToDevice, s->stream));
+  CK(cudaMemcpyAsync(s->stage[1], mask, nf, cudaMemcpyHostToDevice, s->stream));
+  if (rho) {
+    CK(cudaMemcpyAsync(s->stage[2], rho, nf, cudaMemcpyHostToDevice, s->stream));
+    CK(cudaMemcpyAsync(s->stage[3], cp, nf, cudaMemcpyHostToDevice, s->stream));
+  }
+  CK(cudaMemsetAsync(s->slots, 0xff, sizeof(unsigned long long) * kHashSlots, s->stream));
+  CK(cudaMemsetAsync(s->flags, 0, sizeof(int), s->stream));
+  k_collect_keys<<<s->num_sms * 4, 256, 0, s->stream>>>(g, s->stage[0], s->stage[1], rho ? s->stage[2] : nullptr,
+                                                         rho ? s->stage[3] : nullptr, s->slots, s->flags);
+  CKL();
+  unsigned long long slots[kHashSlots];
+  int flags = 0;
+  CK(cudaMemcpyAsync(slots, s->slots, sizeof slots, cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaMemcpyAsync(&flags, s->flags, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  if (flags & kFlagNonFinite) return fail(H2G_NONFINITE, "non-finite value in lambda, mask, rho or cp");
+  if (flags & kFlagMaskValue) return fail(H2G_UNSUPPORTED, "mask values must be 0 or 1");
+  std::vector<unsigned long long> vals;
+  for (auto v : slots)
+    if (v != ~0ull) vals.push_back(v);
+  if ((flags & kFlagTooMany) || (int)vals.size() > kMaxKeys)
+    return fail(H2G_UNSUPPORTED, "more than %d distinct conductivity values", kMaxKeys);
+  std::sort(vals.begin(), vals.end());
+  int index[kHashSlots];
+  for (int h = 0; h < kHashSlots; ++h) {
+    index[h] = 0;
+    if (slots[h] != ~0ull) index[h] = (int)(std::lower_bound(vals.begin(), vals.end(), slots[h]) - vals.begin());
+  }
+  s->P = (int)vals.size();
+  s->lam_values.resize(vals.size());
+  for (size_t i = 0; i < vals.size(); ++i) memcpy(&s->lam_values[i], &vals[i], sizeof(double));
+  CK(cudaMemcpyAsync(s->slot_index, index, sizeof index, cudaMemcpyHostToDevice, s->stream));
+  // rho*cp per cell for transient grids
+  if (rho) {
+    if (!s->t64.rc) CK(cudaMalloc(&s->t64.rc, sizeof(double) * (size_t)g.n));
+    if (s->precision == H2G_MIXED && !s->t32.rc) CK(cudaMalloc(&s->t32.rc, sizeof(float) * (size_t)g.n));
+    CK(cudaMemsetAsync(s->t64.rc, 0, sizeof(double) * (size_t)g.n, s->stream));
+  }
+  dim3 grid((g.MX + 127) / 128, g.MY, g.MZ);
+  k_make_keys<double><<<grid, 128, 0, s->stream>>>(g, s->stage[0], s->stage[1], rho ? s->stage[2] : nullptr,
+                                                   rho ? s->stage[3] : nullptr, s->slots, s->slot_index, s->key,
+                                                   rho ? s->t64.rc : nullptr);
+  CKL();
+  if (rho && s->precision == H2G_MIXED) {
+    k_make_keys<float><<<grid, 128, 0, s->stream>>>(g, s->stage[0], s->stage[1], s->stage[2], s->stage[3], s->slots,
+                                                    s->slot_index, s->key, s->t32.rc);
+    CKL();
+  }
+  s->rc_valid = rho != nullptr;
+  s->fields_set = true;
+  CK(cudaStreamSynchronize(s->stream));
+  return build_tables(s);
+}
+
+}  // namespace h2g
+
+// ==========================================================================================
+// C ABI
+// ==========================================================================================
+using h2g::Solver;
+using h2g::fail;
+
+static Solver* S(h2g_solver* h) { return static_cast<Solver*>(h); }
+
+// ---- single-kernel helpers ---------------------------------------------------------------
+template <typename T>
+static int calcax_t(Solver* s, const double* x, double* ax, const h2g::OpParams<T>& op) {
+  using namespace h2g;
+  T* xd = kvec<T>(s, KPH);
+  T* yd = kvec<T>(s, KQ);
+  int rc;
+  if ((rc = upload<T>(s, x, xd))) return rc;
+  k_ax<T, 0><<<ax_grid(s->g), dim3(kBX, kBY), 0, s->stream>>>(op, yd, xd, nullptr, nullptr, nullptr, nullptr, 0);
+  CKL();
+  return download<T>(s, yd, ax);
+}
+
+template <typename T>
+static int rbsor_t(Solver* s, double* x, const double* b, int color, double omega, const h2g::OpParams<T>& op) {
+  using namespace h2g;
+  T* xd = kvec<T>(s, KPH);
+  T* bd = kvec<T>(s, KP);
+  int rc;
+  if ((rc = upload<T>(s, x, xd, 0))) return rc;
+  if ((rc = upload<T>(s, b, bd, 1))) return rc;
+  k_rb_pass<T><<<rb_grid(s->g), dim3(kBX, kBY), 0, s->stream>>>(op, xd, bd, color, (T)omega, nullptr);
+  CKL();
+  return download<T>(s, xd, x);
+}
+
+template <typename T>
+static int precond_t(Solver* s, const double* bb, double* xx, int smoother, const h2g::OpParams<T>& op) {
+  using namespace h2g;
+  T* xd = kvec<T>(s, KPH);
+  T* bd = kvec<T>(s, KP);
+  int rc;
+  if ((rc = upload<T>(s, bb, bd, 1))) return rc;
+  const dim3 rg = rb_grid(s->g), blk(kBX, kBY);
+  const int none = smoother == H2G_SMOOTHER_NONE;
+  k_rb_first<T, 0><<<rg, blk, 0, s->stream>>>(op, xd, bd, nullptr, nullptr, nullptr, none);
+  if (!none)
+    for (int pass = 1; pass < 2 * kSweeps; ++pass) k_rb_pass<T><<<rg, blk, 0, s->stream>>>(op, xd, bd, pass & 1, T(1), nullptr);
+  CKL();
+  return download<T>(s, xd, xx);
+}
+
+template <typename T>
+static int bench_t(Solver* s, int kind, int reps, int* launches, const h2g::OpParams<T>& op) {
+  using namespace h2g;
+  const dim3 rg = rb_grid(s->g), ag = ax_grid(s->g), blk(kBX, kBY);
+  int n = 0;
+  for (int r = 0; r < reps; ++r) {
+    if (kind == 0) {
+      k_rb_pass<T><<<rg, blk, 0, s->stream>>>(op, kvec<T>(s, KPH), kvec<T>(s, KP), 0, T(1), nullptr);
+      k_rb_pass<T><<<rg, blk, 0, s->stream>>>(op, kvec<T>(s, KPH), kvec<T>(s, KP), 1, T(1), nullptr);
+      n += 2;
+    } else {
+      k_ax<T, 0><<<ag, blk, 0, s->stream>>>(op, kvec<T>(s, KQ), kvec<T>(s, KPH), nullptr, nullptr, nullptr, nullptr, 0);
+      n += 1;
+    }
+  }
+  CKL();
+  if (launches) *launches = n;
+  return H2G_OK;
+}
+
+extern "C" {
+
+const char* h2g_version(void) { return "h2g 0.1 (sm_100a)"; }
+
+const char* h2g_status_string(int status) {
+  switch (status) {
+    case H2G_OK: return "ok";
+    case H2G_NOT_CONVERGED: return "not converged";
+    case H2G_BREAKDOWN: return "breakdown";
+    case H2G_NONFINITE: return "non-finite value";
+    case H2G_BAD_ARG: return "bad argument";
+    case H2G_CUDA_ERROR: return "CUDA error";
+    case H2G_TIMEOUT: return "timeout";
+    case H2G_UNSUPPORTED: return "unsupported";
+    default: return "unknown status";
+  }
+}
+
+const char* h2g_last_error(void) { return h2g::g_err.c_str(); }
+
+int h2g_create(int MX, int MY, int MZ, int precision, h2g_solver** out) {
+  if (!out) return fail(H2G_BAD_ARG, "null output pointer");
+  *out = nullptr;
+  Solver* s = nullptr;
+  int rc = h2g::create(MX, MY, MZ, precision, &s);
+  if (rc) return rc;
+  *out = static_cast<h2g_solver*>(s);
+  return H2G_OK;
+}
+
+int h2g_destroy(h2g_solver* h) {
+  if (!h) return H2G_OK;
+  h2g::destroy(S(h));
+  return H2G_OK;
+}
+
+int h2g_set_stream(h2g_solver* h, void* stream) {
+  if (int rc = h2g::check_handle(h)) return rc;
+  S(h)->stream = (cudaStream_t)stream;
+  return H2G_OK;
+}
+
+int h2g_set_grid(h2g_solver* h, const double* ZC, const double* dZ, double dx, double dy, double dt, const double* HC,
+                 int is_steady) {
+  if (int rc = h2g::check_handle(h)) return rc;
+  return h2g::set_grid(S(h), ZC, dZ, dx, dy, dt, HC, is_steady);
+}
+
+int h2g_set_fields(h2g_solver* h, const double* lambda, const double* mask, const double* rho, const double* cp) {
+  if (int rc = h2g::check_handle(h)) return rc;
+  return h2g::set_fields(S(h), lambda, mask, rho, cp);
+}
+
+int h2g_set_rhs(h2g_solver* h, const double* b) {
+  if (int rc = h2g::check_handle(h)) return rc;
+  return h2g::upload<double>(S(h), b, S(h)->b);
+}
+
+int h2g_get_rhs(h2g_solver* h, double* b) {
+  if (int rc = h2g::check_handle(h)) return rc;
+  return h2g::download<double>(S(h), S(h)->b, b);
+}
+
+int h2g_set_theta(h2g_solver* h, const double* theta) {
+  if (int rc = h2g::check_handle(h)) return rc;
+  return h2g::upload<double>(S(h), theta, S(h)->th);
+}
+
+int h2g_get_theta(h2g_solver* h, double* theta) {
+  if (int rc = h2g::check_handle(h)) return rc;
+  return h2g::download<double>(S(h), S(h)->th, theta);
+}
+
+int h2g_theta_snapshot(h2g_solver* h, int op) {
+  if (int rc = h2g::check_handle(h)) return rc;
+  Solver* s = S(h);
+  const size_t nb = sizeof(double) * (size_t)s->g.n;
+  if (op == 0) {
+    if (cudaMemcpyAsync(s->th_snap, s->th, nb, cudaMemcpyDeviceToDevice, s->stream) != cudaSuccess)
+      return fail(H2G_CUDA_ERROR, "snapshot copy failed");
+  } else if (op == 1) {
+    if (cudaMemcpyAsync(s->th, s->th_snap, nb, cudaMemcpyDeviceToDevice, s->stream) != cudaSuccess)
+      return fail(H2G_CUDA_ERROR, "snapshot copy failed");
+  } else {
+    return fail(H2G_BAD_ARG, "snapshot op must be 0 (save) or 1 (restore)");
+  }
+  return H2G_OK;
+}
+
+int h2g_set_mixed_params(h2g_solver* h, double inner_tol, int max_outer) {
+  if (int rc = h2g::check_handle(h)) return rc;
+  if (!(inner_tol > 0 && inner_tol < 1) || max_outer < 1) return fail(H2G_BAD_ARG, "bad refinement parameters");
+  S(h)->inner_tol = inner_tol;
+  S(h)->max_outer = max_outer;
+  return H2G_OK;
+}
+
+int h2g_pbicgstab(h2g_solver* h, double tol, int maxItr, int smoother, int verbose, double* res_hist,
+                  h2g_result* out) {
+  if (int rc = h2g::check_handle(h)) return rc;
+  return h2g::solve(S(h), false, tol, maxItr, smoother, verbose, res_hist, out);
+}
+
+int h2g_cg(h2g_solver* h, double tol, int maxItr, int smoother, int verbose, double* res_hist, h2g_result* out) {
+  if (int rc = h2g::check_handle(h)) return rc;
+  return h2g::solve(S(h), true, tol, maxItr, smoother, verbose, res_hist, out);
+}
+
+static std::mutex g_cache_mu;
+static h2g_solver* g_cache[2] = {nullptr, nullptr};
+
+static int oneshot(bool cg, int MX, int MY, int MZ, double* theta, const double* b, const double* lambda,
+                   const double* mask, const double* rho, const double* cp, double dx, double dy, double dt,
+                   const double* ZC, const double* dZ, const double* HC, double tol, int maxItr, int smoother,
+                   int verbose, int is_steady, int precision, double* res_hist, h2g_result* out) {
+  if (precision != H2G_FP64 && precision != H2G_MIXED) return fail(H2G_BAD_ARG, "unknown precision %d", precision);
+  if (!theta || !b) return fail(H2G_BAD_ARG, "null theta/b");
+  std::lock_guard<std::mutex> lk(g_cache_mu);
+  h2g_solver*& h = g_cache[precision];
+  if (h && (S(h)->g.MX != MX || S(h)->g.MY != MY || S(h)->g.MZ != MZ)) {
+    h2g_destroy(h);
+    h = nullptr;
+  }
+  int rc;
+  if (!h && (rc = h2g_create(MX, MY, MZ, precision, &h))) return rc;
+  if ((rc = h2g_set_grid(h, ZC, dZ, dx, dy, dt, HC, is_steady))) return rc;
+  if ((rc = h2g_set_fields(h, lambda, mask, is_steady ? nullptr : rho, is_steady ? nullptr : cp))) return rc;
+  if ((rc = h2g_set_rhs(h, b))) return rc;
+  if ((rc = h2g_set_theta(h, theta))) return rc;
+  int st = h2g::solve(S(h), cg, tol, maxItr, smoother, verbose, res_hist, out);
+  if (st == H2G_BAD_ARG || st == H2G_CUDA_ERROR) return st;
+  if ((rc = h2g_get_theta(h, theta))) return rc;
+  return st;
+}
+
+int h2g_PBiCGSTAB(int MX, int MY, int MZ, double* theta, const double* b, const double* lambda, const double* mask,
+                  const double* rho, const double* cp, double dx, double dy, double dt, const double* ZC,
+                  const double* dZ, const double* HC, double tol, int maxItr, int smoother, int verbose,
+                  int is_steady, int precision, double* res_hist, h2g_result* out) {
+  return oneshot(false, MX, MY, MZ, theta, b, lambda, mask, rho, cp, dx, dy, dt, ZC, dZ, HC, tol, maxItr, smoother,
+                 verbose, is_steady, precision, res_hist, out);
+}
+
+int h2g_CG(int MX, int MY, int MZ, double* theta, const double* b, const double* lambda, const double* mask,
+           const double* rho, const double* cp, double dx, double dy, double dt, const double* ZC, const double* dZ,
+           const double* HC, double tol, int maxItr, int smoother, int verbose, int is_steady, int precision,
+           double* res_hist, h2g_result* out) {
+  return oneshot(true, MX, MY, MZ, theta, b, lambda, mask, rho, cp, dx, dy, dt, ZC, dZ, HC, tol, maxItr, smoother,
+                 verbose, is_steady, precision, res_hist, out);
+}
+
+int h2g_release_cached(void) {
+  std::lock_guard<std::mutex> lk(g_cache_mu);
+  for (auto& h : g_cache) {
+    h2g_destroy(h);
+    h = nullptr;
+  }
+  return H2G_OK;
+}
+
+// ---- single kernels ------------------------------------------------------------------------
+
+int h2g_calcax(h2g_solver* h, const double* x, double* ax) {
+  if (int rc = h2g::check_handle(h)) return rc;
+  Solver* s = S(h);
+  if (!s->grid_set || !s->fields_set) return fail(H2G_BAD_ARG, "h2g_set_grid and h2g_set_fields must come first");
+  if (s->precision == H2G_MIXED) return calcax_t<float>(s, x, ax, h2g::op_params<float>(s, s->t32));
+  return calcax_t<double>(s, x, ax, h2g::op_params<double>(s, s->t64));
+}
+
+int h2g_calcrk(h2g_solver* h, double* r, double* res) {
+  using namespace h2g;
+  if (int rc = check_handle(h)) return rc;
+  Solver* s = S(h);
+  if (!s->grid_set || !s->fields_set) return fail(H2G_BAD_ARG, "h2g_set_grid and h2g_set_fields must come first");
+  if (!res) return fail(H2G_BAD_ARG, "null res");
+  OpParams<double> op = op_params<double>(s, s->t64);
+  double* rd = s->precision == H2G_MIXED ? s->r64 : kvec<double>(s, KR);
+  int rc;
+  if ((rc = prime_state(s, s->st, 0.0, 1, nullptr, 0))) return rc;
+  k_rk<double><<<ax_grid(s->g), dim3(kBX, kBY), 0, s->stream>>>(op, rd, nullptr, s->th, s->b, s->st, s->partials,
+                                                                   kStageResid);
+  CKL();
+  CK(cudaMemcpyAsync(s->st_host, s->st, sizeof(SolverState), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  *res = s->st_host->scale;
+  if (r) return download<double>(s, rd, r);
+  return H2G_OK;
+}
+
+
+int h2g_rbsor_pass(h2g_solver* h, double* x, const double* b, int color, double omega) {
+  if (int rc = h2g::check_handle(h)) return rc;
+  Solver* s = S(h);
+  if (!s->grid_set || !s->fields_set) return fail(H2G_BAD_ARG, "h2g_set_grid and h2g_set_fields must come first");
+  if (color != 0 && color != 1) return fail(H2G_BAD_ARG, "color must be 0 or 1");
+  if (!(omega > 0 && omega < 2)) return fail(H2G_BAD_ARG, "omega must be in (0,2)");
+  if (s->precision == H2G_MIXED) return rbsor_t<float>(s, x, b, color, omega, h2g::op_params<float>(s, s->t32));
+  return rbsor_t<double>(s, x, b, color, omega, h2g::op_params<double>(s, s->t64));
+}
+
+
+int h2g_preconditioner(h2g_solver* h, const double* bb, double* xx, int smoother) {
+  if (int rc = h2g::check_handle(h)) return rc;
+  Solver* s = S(h);
+  if (!s->grid_set || !s->fields_set) return fail(H2G_BAD_ARG, "h2g_set_grid and h2g_set_fields must come first");
+  if (smoother != H2G_SMOOTHER_NONE && smoother != H2G_SMOOTHER_GS)
+    return fail(H2G_BAD_ARG, "Unsupported smoother: %d. Use none (0) or gs (1)", smoother);
+  if (s->precision == H2G_MIXED) return precond_t<float>(s, bb, xx, smoother, h2g::op_params<float>(s, s->t32));
+  return precond_t<double>(s, bb, xx, smoother, h2g::op_params<double>(s, s->t64));
+}
+
+
+int h2g_bench_kernel(h2g_solver* h, int kind, int reps, int* launches) {
+  if (int rc = h2g::check_handle(h)) return rc;
+  Solver* s = S(h);
+  if (!s->grid_set || !s->fields_set) return fail(H2G_BAD_ARG, "h2g_set_grid and h2g_set_fields must come first");
+  if (kind != 0 && kind != 1) return fail(H2G_BAD_ARG, "kind must be 0 (RB-GS sweep) or 1 (CalcAX)");
+  if (reps < 1) return fail(H2G_BAD_ARG, "reps must be positive");
+  if (s->precision == H2G_MIXED) return bench_t<float>(s, kind, reps, launches, h2g::op_params<float>(s, s->t32));
+  return bench_t<double>(s, kind, reps, launches, h2g::op_params<double>(s, s->t64));
+}
+
+}  // extern "C"

@@ -1,0 +1,169 @@
+/*
+ * h2g.h -- C ABI of the B200 (sm_100a) solver library for the Heat3ds linear-solver path.
+ *
+ * The library replaces the Julia module NonUniform (src/NonUniform.jl) for par="gpu":
+ * the matrix-free 7-point finite-volume operator, the 5-sweep red-black Gauss-Seidel
+ * preconditioner and the PBiCGSTAB / CG drivers.  It is called with the reference's own
+ * arrays: Float64, column-major (i fastest), shape (MX, MY, MZ) = (NX+2, NY+2, NZ+2)
+ * including one guard layer on each side (src/common.jl:49-89).  Element (i,j,k) of the
+ * Julia array (1-based) is host element (i-1) + MX*((j-1) + MY*(k-1)).
+ *
+ * Conventions
+ *  - Every entry returns an int status (H2G_OK = 0 or one of the codes below); nothing
+ *    aborts or exits.  h2g_last_error() gives a one-line message for the last failure
+ *    on the calling thread.
+ *  - Host pointers are copied in and out; device memory is owned by the solver handle.
+ *  - A handle is not thread-safe: use one handle per host thread / Julia task.
+ *  - Calls are synchronous with respect to the host unless they say otherwise; they run
+ *    on the stream given to h2g_set_stream (default: the legacy default stream).
+ */
+#ifndef H2G_H
+#define H2G_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------------------ */
+#define H2G_OK 0              /* converged / done */
+#define H2G_NOT_CONVERGED 1   /* maxItr reached (reference: isconverged=false, NonUniform.jl:225,349) */
+#define H2G_BREAKDOWN 2       /* |rho|, (p,q) or (t,t) below FloatMin=1e-37 (NonUniform.jl:169-173, 291-294, 321-324) */
+#define H2G_NONFINITE 3       /* NaN/Inf in an input array or in the iteration */
+#define H2G_BAD_ARG 4         /* rejected on the host before any launch */
+#define H2G_CUDA_ERROR 5      /* a CUDA runtime call failed */
+#define H2G_TIMEOUT 6         /* a bounded device wait ran out */
+#define H2G_UNSUPPORTED 7     /* input outside what this build implements (message says what) */
+
+/* ---- precision ---------------------------------------------------------------------- */
+#define H2G_FP64 0  /* FP64 throughout, same arithmetic as the reference */
+#define H2G_MIXED 1 /* FP32 operator/smoother/Krylov vectors inside FP64 iterative refinement */
+
+/* ---- smoother (NonUniform.jl:36-41: :none, :gs) -------------------------------------- */
+#define H2G_SMOOTHER_NONE 0
+#define H2G_SMOOTHER_GS 1
+
+/* ---- boundary types (src/common.jl:20-24) -------------------------------------------- */
+#define H2G_ISOTHERMAL 0
+#define H2G_HEAT_FLUX 1
+#define H2G_CONVECTION 2
+
+/* BoundaryCondition (src/boundary_conditions.jl:15-21); faces ordered x-, x+, y-, y+, z-, z+
+ * (BoundaryConditionSet, boundary_conditions.jl:24-31). */
+typedef struct h2g_bc {
+  int type;
+  double temperature;
+  double heat_flux;
+  double htc;
+  double ambient;
+} h2g_bc;
+
+/* The (isconverged, itr, res0) tuple returned by PBiCGSTAB!/CG! (NonUniform.jl:225, 349),
+ * plus what the GPU path adds. */
+typedef struct h2g_result {
+  int isconverged; /* 1 if ||r_k|| / ||r_0|| < tol */
+  int itr;         /* iterations: PBiCGSTAB/CG iterations (FP64) or all inner iterations (mixed) */
+  int outer;       /* iterative-refinement passes (mixed), 0 for FP64 */
+  int status;      /* same value the call returns */
+  double res0;     /* initial residual ||b - A theta||_2 (NonUniform.jl:263) */
+  double res;      /* final relative residual ||r|| / res0 */
+  long long launches; /* kernels this call launched on the device (graph iterations included) */
+} h2g_result;
+
+typedef struct h2g_solver h2g_solver;
+
+/* ---- library ------------------------------------------------------------------------ */
+const char *h2g_version(void);
+const char *h2g_status_string(int status);
+const char *h2g_last_error(void);
+
+/* ---- handle lifecycle ----------------------------------------------------------------
+ * Allocates the device copies of WorkBuffers (src/common.jl:71-89) for an (MX,MY,MZ)
+ * grid on the current CUDA device. */
+int h2g_create(int MX, int MY, int MZ, int precision, h2g_solver **out);
+int h2g_destroy(h2g_solver *h);
+/* stream: a cudaStream_t (NULL = legacy default stream). */
+int h2g_set_stream(h2g_solver *h, void *stream);
+
+/* Grid and coefficients of the operator (the Δh, Δt, ZC, ΔZ, HC, is_steady arguments of
+ * CalcAX!/CalcRK!/rbsor_core!, NonUniform.jl:372-386, 454-466, 848-862).  ZC and dZ have
+ * MZ entries (genZ!, src/Zcoord.jl:133-166); HC has 6 (set_BC_coef, boundary_conditions.jl:360-394). */
+int h2g_set_grid(h2g_solver *h, const double *ZC, const double *dZ, double dx, double dy, double dt,
+                 const double *HC, int is_steady);
+/* wk.λ, wk.mask, wk.ρ, wk.cp (src/common.jl:52-55), guard layers included.  ρ and cp may be
+ * NULL for a steady grid.  Masks must be 0 or 1. */
+int h2g_set_fields(h2g_solver *h, const double *lambda, const double *mask, const double *rho,
+                   const double *cp);
+/* wk.b and wk.θ (src/common.jl:50-51). */
+int h2g_set_rhs(h2g_solver *h, const double *b);
+int h2g_get_rhs(h2g_solver *h, double *b);
+int h2g_set_theta(h2g_solver *h, const double *theta);
+int h2g_get_theta(h2g_solver *h, double *theta);
+/* Device-side copy of θ: op 0 saves the current θ, op 1 restores it (repeat a solve from
+ * the same start without a host copy). */
+int h2g_theta_snapshot(h2g_solver *h, int op);
+
+/* Iterative-refinement settings for H2G_MIXED: inner relative tolerance of each FP32 solve
+ * and the cap on refinement passes (defaults 1e-4 and 40). */
+int h2g_set_mixed_params(h2g_solver *h, double inner_tol, int max_outer);
+
+/* ---- solvers -------------------------------------------------------------------------
+ * PBiCGSTAB!(wk, Δh, Δt, ZC, ΔZ, HC; tol, maxItr, smoother, par, verbose, is_steady)
+ *   (src/NonUniform.jl:248-350) on the handle's θ, b and fields; θ is updated on the device
+ *   (fetch it with h2g_get_theta).  res_hist (nullable, maxItr doubles) receives the relative
+ *   residual of every iteration; verbose prints the reference's "%10d %24.14E" lines to stdout.
+ *   Returns H2G_OK when converged. */
+int h2g_pbicgstab(h2g_solver *h, double tol, int maxItr, int smoother, int verbose, double *res_hist,
+                  h2g_result *out);
+/* CG!(...) (src/NonUniform.jl:115-226), same conventions. */
+int h2g_cg(h2g_solver *h, double tol, int maxItr, int smoother, int verbose, double *res_hist, h2g_result *out);
+
+/* One-call drop-in for PBiCGSTAB!/CG! with the reference's arrays (heat3ds.jl:133-141):
+ * uploads θ, b, λ, mask, ρ, cp and the grid, solves, and writes θ back.  A handle for the
+ * grid size is kept between calls (not thread-safe). */
+int h2g_PBiCGSTAB(int MX, int MY, int MZ, double *theta, const double *b, const double *lambda,
+                  const double *mask, const double *rho, const double *cp, double dx, double dy, double dt,
+                  const double *ZC, const double *dZ, const double *HC, double tol, int maxItr, int smoother,
+                  int verbose, int is_steady, int precision, double *res_hist, h2g_result *out);
+int h2g_CG(int MX, int MY, int MZ, double *theta, const double *b, const double *lambda, const double *mask,
+           const double *rho, const double *cp, double dx, double dy, double dt, const double *ZC,
+           const double *dZ, const double *HC, double tol, int maxItr, int smoother, int verbose, int is_steady,
+           int precision, double *res_hist, h2g_result *out);
+/* Release the handles kept by h2g_PBiCGSTAB / h2g_CG. */
+int h2g_release_cached(void);
+
+/* ---- kernels of the path, callable one at a time (host arrays in and out) ---------------
+ * CalcAX! (NonUniform.jl:454-511): ax = A x over the interior; guard cells of ax are 0. */
+int h2g_calcax(h2g_solver *h, const double *x, double *ax);
+/* CalcRK! (NonUniform.jl:372-434): r = b - A θ with the handle's θ and b; *res = ||r||_2. */
+int h2g_calcrk(h2g_solver *h, double *r, double *res);
+/* rbsor_core! (NonUniform.jl:848-915): one colour pass (color 0 or 1) of RB-SOR with
+ * relaxation omega on x (in/out) with right-hand side b. */
+int h2g_rbsor_pass(h2g_solver *h, double *x, const double *b, int color, double omega);
+/* Preconditioner! (NonUniform.jl:531-559): xx = M^-1 bb, xx starting from zero. */
+int h2g_preconditioner(h2g_solver *h, const double *bb, double *xx, int smoother);
+
+/* ---- device-resident timing hooks (for benchmarks) --------------------------------------
+ * Run `reps` back-to-back launches of one kernel class on the handle's resident data, on the
+ * handle's stream, without synchronising: kind 0 = one RB-GS sweep (both colours) of the
+ * preconditioner, kind 1 = CalcAX.  Returns the number of kernel launches issued in *launches. */
+int h2g_bench_kernel(h2g_solver *h, int kind, int reps, int *launches);
+
+/* ---- the reference's problem set-up (what q3d does before the solve) ---------------------
+ * genZ! (src/Zcoord.jl:133-166) for NZ = 30*m: Z (NZ+3 faces with extrapolated guards), ZC and dZ
+ * (NZ+2 each).  m > 1 splits each of the 30 Zcase2! cells (Zcoord.jl:88-124) into m equal
+ * sub-cells; the reference itself only supports NZ = 30. */
+int h2g_model_zgrid(int NZ, double *Z, double *ZC, double *dZ);
+/* dx = round(1.2e-3/N, digits=8) (src/heat3ds.jl:197-200). */
+double h2g_model_pitch(int N);
+/* fillID! (src/modelA.jl:545-556) on the GPU: the uint8 material-ID field of the IC stack for an
+ * (NX+2, NY+2, NZ+2) grid, written to the host array ID (column-major); bit-identical to the
+ * reference's 50^3-sample volume tests. */
+int h2g_model_fill_id(int NX, int NY, int NZ, uint8_t *ID);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* H2G_H */

@@ -1,0 +1,70 @@
+"""The C-ABI library without a GPU: it loads, exports every symbol include/h2g.h declares,
+and rejects bad arguments on the host before any launch.  The Python host interface raises the
+reference's errors (unknown smoother, unknown par) and fails loudly without the library."""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+
+import h2_b200
+from h2_b200 import _lib as L
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from h2_b200 import build
+    build.build()
+    return L.load()
+
+
+def test_exports_every_declared_symbol(lib):
+    names = L.header_functions()
+    assert len(names) >= 24
+    raw = C.CDLL(L.LIB_PATH)
+    missing = [n for n in names if not hasattr(raw, n)]
+    assert not missing, missing
+    # every declared function has a ctypes signature in the binding
+    assert set(names) == set(L._SIGS), set(names) ^ set(L._SIGS)
+
+
+def test_status_strings(lib):
+    assert lib.h2g_status_string(L.H2G_OK) == b"ok"
+    assert lib.h2g_status_string(L.H2G_BREAKDOWN) == b"breakdown"
+    assert b"sm_100a" in lib.h2g_version()
+
+
+def test_bad_arguments_rejected_on_host(lib):
+    h = C.c_void_p()
+    assert lib.h2g_create(1, 5, 5, 0, C.byref(h)) == L.H2G_BAD_ARG
+    assert lib.h2g_create(5, 5, 5, 7, C.byref(h)) == L.H2G_BAD_ARG
+    assert lib.h2g_create(5, 5, 5, 0, None) == L.H2G_BAD_ARG
+    res = L.Result()
+    assert lib.h2g_pbicgstab(None, 1e-6, 10, 1, 0, None, C.byref(res)) == L.H2G_BAD_ARG
+    assert lib.h2g_cg(None, 1e-6, 10, 1, 0, None, C.byref(res)) == L.H2G_BAD_ARG
+    assert b"null" in lib.h2g_last_error()
+    assert lib.h2g_destroy(None) == L.H2G_OK
+
+
+def test_smoother_selector_errors():
+    assert h2_b200.smoother_selector("gs") == L.H2G_SMOOTHER_GS
+    assert h2_b200.smoother_selector(":none") == L.H2G_SMOOTHER_NONE
+    with pytest.raises(ValueError, match="Unsupported smoother"):
+        h2_b200.smoother_selector("jacobi")
+
+
+def test_par_must_be_gpu():
+    wk = h2_b200.WorkBuffers.allocate(6, 6, 6)
+    with pytest.raises(ValueError, match="parallel mode"):
+        h2_b200.PBiCGSTAB(wk, (1e-5, 1e-5, 1.0), 1.0, np.zeros(6), np.zeros(6), np.zeros(6), par="thread")
+
+
+def test_missing_library_fails_loudly(tmp_path):
+    with pytest.raises(h2_b200.H2GLibraryError):
+        L.load(str(tmp_path / "libh2g.so"))
+
+
+def test_workbuffers_layout():
+    wk = h2_b200.WorkBuffers.allocate(7, 6, 5)
+    assert wk.theta.flags.f_contiguous and wk.theta.shape == (7, 6, 5)
+    assert wk.mask.min() == 1.0 and wk.lam.min() == 1.0 and wk.cp.min() == 1.0 and wk.rho.max() == 0.0

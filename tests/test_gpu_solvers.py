@@ -1,0 +1,205 @@
+"""GPU PBiCGSTAB!/CG! against the oracle (theta within 1e-3 K,
+FP64 iteration counts within 10 %), through the C ABI, plus the status/edge cases of the
+reference's control flow (res0 == 0, maxItr, breakdown, non-finite input)."""
+import numpy as np
+import pytest
+
+import h2_b200
+from conftest import golden, mode3_model
+from test_gpu_kernels import make_solver
+
+pytestmark = pytest.mark.gpu
+
+THETA_TOL_K = 1e-3
+
+
+def sample(theta, ijk):
+    ijk = np.asarray(ijk)
+    return theta[ijk[:, 0], ijk[:, 1], ijk[:, 2]]
+
+
+@pytest.mark.parametrize("method", ["pbicgstab", "cg"])
+@pytest.mark.parametrize("smoother", ["gs", "none"])
+def test_small_fp64_matches_oracle(oracle, method, smoother):
+    prob = mode3_model(oracle, 40, symmetric=(method == "cg"))
+    ref = mode3_model(oracle, 40, symmetric=(method == "cg"))
+    fn = oracle.pbicgstab if method == "pbicgstab" else oracle.cg
+    conv_r, itr_r, res0_r, hist_r = fn(ref, tol=1e-6, maxItr=20000, smoother=smoother)
+    s = make_solver(prob)
+    hist = np.zeros(20000)
+    st, res = s.solve(method, tol=1e-6, maxItr=20000, smoother=smoother, hist=hist)
+    assert st == 0 and res.isconverged and conv_r
+    assert abs(res.itr - itr_r) <= max(1, 0.1 * itr_r)
+    assert abs(res.res0 - res0_r) <= 1e-13 * res0_r
+    th = s.get_theta()
+    assert np.abs(th - ref.wk["theta"]).max() <= THETA_TOL_K
+    # the first iterations agree to rounding of the reductions
+    n = min(5, res.itr)
+    assert np.allclose(hist[:n], hist_r[:n], rtol=1e-9, atol=0)
+    s.close()
+
+
+def test_readme_case_fp64(oracle):
+    """The README's q3d(240,240,30,"pbicgstab","gs"; epsilon=1e-4): 208 iterations."""
+    g = golden("oracle_240_1e-4.json")
+    prob = mode3_model(oracle, 240)
+    s = make_solver(prob)
+    hist = np.zeros(20000)
+    st, res = s.solve("pbicgstab", tol=1e-4, maxItr=20000, smoother="gs", hist=hist)
+    assert st == 0 and res.isconverged
+    assert abs(res.itr - g["itr"]) <= 0.1 * g["itr"]
+    assert abs(res.res0 - g["res0"]) <= 1e-13 * g["res0"]
+    th = s.get_theta()
+    assert np.abs(sample(th, g["sample_ijk"]) - np.array(g["sample_theta"])).max() <= THETA_TOL_K
+    assert abs(th[1:-1, 1:-1, 1:-1].max() - g["theta_max"]) <= THETA_TOL_K
+    assert np.allclose(hist[:3], g["hist"][:3], rtol=1e-9)
+    s.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_240_to_1e8(oracle, precision):
+    """Default case, relative residual 1e-8: FP64 and FP32-inner/FP64-refinement both within
+    1e-3 K of the FP64 oracle."""
+    g = golden("oracle_240_1e-8.json")
+    prob = mode3_model(oracle, 240)
+    s = make_solver(prob, precision=precision)
+    st, res = s.solve("pbicgstab", tol=1e-8, maxItr=20000, smoother="gs")
+    assert st == 0 and res.isconverged and res.res < 1e-8
+    if precision == "fp64":
+        assert abs(res.itr - g["itr"]) <= 0.1 * g["itr"]
+    th = s.get_theta()
+    err = np.abs(sample(th, g["sample_ijk"]) - np.array(g["sample_theta"])).max()
+    assert err <= THETA_TOL_K, err
+    # the true FP64 residual of the returned field
+    s2 = make_solver(prob)
+    s2.set_theta(th)
+    _, r = s2.calc_rk()
+    assert r / res.res0 < 1e-8 * 1.01
+    s.close()
+    s2.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_cg_symmetric_variant(oracle, precision):
+    g = golden("oracle_240_cg_sym.json")
+    prob = mode3_model(oracle, 240, symmetric=True)
+    s = make_solver(prob, precision=precision)
+    st, res = s.solve("cg", tol=1e-8, maxItr=20000, smoother="gs")
+    assert st == 0 and res.isconverged
+    if precision == "fp64":
+        assert abs(res.itr - g["itr"]) <= 0.1 * g["itr"]
+    th = s.get_theta()
+    err = np.abs(sample(th, g["sample_ijk"]) - np.array(g["sample_theta"])).max()
+    assert err <= THETA_TOL_K, err
+    s.close()
+
+
+def test_transient_step(oracle):
+    prob = mode3_model(oracle, 40, is_steady=False, dt=1e-4)
+    ref = mode3_model(oracle, 40, is_steady=False, dt=1e-4)
+    conv_r, itr_r, _, _ = oracle.pbicgstab(ref, tol=1e-8, smoother="gs")
+    s = make_solver(prob)
+    st, res = s.solve("pbicgstab", tol=1e-8, smoother="gs")
+    assert st == 0 and abs(res.itr - itr_r) <= max(1, 0.1 * itr_r)
+    assert np.abs(s.get_theta() - ref.wk["theta"]).max() <= THETA_TOL_K
+    s.close()
+
+
+def test_oneshot_dropin_matches_handle(oracle):
+    """h2g_PBiCGSTAB with the reference's WorkBuffers (PBiCGSTAB! signature)."""
+    prob = mode3_model(oracle, 40)
+    w = prob.wk
+    wk = h2_b200.WorkBuffers.allocate(*prob.shape)
+    for src, dst in [("theta", "theta"), ("b", "b"), ("mask", "mask"), ("rho", "rho"), ("lam", "lam"),
+                     ("cp", "cp"), ("hsrc", "hsrc")]:
+        getattr(wk, dst)[...] = w[src]
+    conv, itr, res0 = h2_b200.PBiCGSTAB(wk, (prob.dx, prob.dy, 1.0), prob.dt, prob.ZC, prob.dZ, prob.HC, tol=1e-6,
+                                        smoother="gs", par="gpu", is_steady=True)
+    conv_r, itr_r, res0_r, _ = oracle.pbicgstab(prob, tol=1e-6, smoother="gs")
+    assert conv and abs(itr - itr_r) <= max(1, 0.1 * itr_r)
+    assert np.abs(wk.theta - prob.wk["theta"]).max() <= THETA_TOL_K
+    # a second call on the cached handle (theta is now the solution: converges at once or soon)
+    conv2, itr2, res02 = h2_b200.PBiCGSTAB(wk, (prob.dx, prob.dy, 1.0), prob.dt, prob.ZC, prob.dZ, prob.HC, tol=1e-6,
+                                           smoother="gs", par="gpu", is_steady=True)
+    assert conv2 and res02 < 1e-5 * res0
+    h2_b200.load().h2g_release_cached()
+
+
+def test_zero_initial_residual(oracle):
+    """res0 == 0 returns (true, 0, res0) (NonUniform.jl:270-272)."""
+    prob = mode3_model(oracle, 20)
+    prob.wk["b"][...] = 0.0
+    prob.wk["theta"][1:-1, 1:-1, 1:-1] = 0.0
+    s = make_solver(prob)
+    for method in ("pbicgstab", "cg"):
+        st, res = s.solve(method, tol=1e-6, smoother="gs")
+        assert st == 0 and res.isconverged and res.itr == 0 and res.res0 == 0.0
+    s.close()
+
+
+def test_max_iterations(oracle):
+    prob = mode3_model(oracle, 20)
+    s = make_solver(prob)
+    s.snapshot()
+    st, res = s.solve("pbicgstab", tol=1e-12, maxItr=3, smoother="gs")
+    assert st == 1 and not res.isconverged and res.itr == 3
+    s.snapshot(restore=True)
+    st, res = s.solve("cg", tol=1e-12, maxItr=3, smoother="gs")
+    assert st == 1 and not res.isconverged and res.itr == 3
+    s.close()
+
+
+def test_maxitr_matches_oracle_state(oracle):
+    """After maxItr iterations the field equals the oracle's after the same iterations."""
+    prob = mode3_model(oracle, 30)
+    ref = mode3_model(oracle, 30)
+    oracle.pbicgstab(ref, tol=1e-30, maxItr=7, smoother="gs")
+    s = make_solver(prob)
+    st, res = s.solve("pbicgstab", tol=1e-30, maxItr=7, smoother="gs")
+    assert res.itr == 7
+    assert np.abs(s.get_theta() - ref.wk["theta"]).max() <= 1e-9
+
+
+def test_breakdown_on_tiny_rho(oracle):
+    """|rho| < FloatMin = 1e-37 at the top of iteration 1 (NonUniform.jl:291-294): a residual of
+    norm 1e-25 gives rho = 1e-50.  PBiCGSTAB stops with itr = 1, not converged; CG (which has no
+    initial rho check) breaks down on (p, q) < FloatMin (NonUniform.jl:169-173) at itr = 1."""
+    prob = mode3_model(oracle, 20)
+    prob.wk["theta"][...] = 0.0
+    prob.wk["b"][...] = 0.0
+    prob.wk["b"][5, 6, 7] = 1e-25
+    ref = mode3_model(oracle, 20)
+    ref.wk["theta"][...] = 0.0
+    ref.wk["b"][...] = 0.0
+    ref.wk["b"][5, 6, 7] = 1e-25
+    conv_r, itr_r, res0_r, _ = oracle.pbicgstab(ref, tol=1e-6, smoother="gs")
+    assert (conv_r, itr_r) == (False, 1)
+    s = make_solver(prob)
+    s.snapshot()
+    st, res = s.solve("pbicgstab", tol=1e-6, smoother="gs")
+    assert st == 2 and not res.isconverged and res.itr == 1 and res.res0 == res0_r
+    s.snapshot(restore=True)
+    conv_c, itr_c, _, _ = oracle.cg(ref, tol=1e-6, smoother="gs")
+    st, res = s.solve("cg", tol=1e-6, smoother="gs")
+    assert st == 2 and not res.isconverged and (res.itr, conv_c) == (itr_c, False)
+    s.close()
+
+
+def test_nonfinite_rhs_reports_nonfinite(oracle):
+    prob = mode3_model(oracle, 20)
+    prob.wk["b"][4, 4, 4] = np.inf
+    s = make_solver(prob)
+    st, res = s.solve("pbicgstab", tol=1e-6, smoother="gs")
+    assert st == 3 and not res.isconverged
+    s.close()
+
+
+def test_verbose_log_format(oracle, capfd):
+    prob = mode3_model(oracle, 20)
+    s = make_solver(prob)
+    st, res = s.solve("pbicgstab", tol=1e-4, smoother="gs", verbose=True)
+    out = capfd.readouterr().out.splitlines()
+    assert out[0].startswith("Initial residual = ")
+    assert out[1] == "%10d %24.14E" % (1, float(out[1].split()[1]))
+    assert out[-1] == f"Converged at {res.itr}"
+    s.close()
