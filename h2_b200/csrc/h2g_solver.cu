@@ -73,7 +73,6 @@ struct OpTables {
   T* tz = nullptr;
   T* conv = nullptr;
   T* dzk = nullptr;
-  T* rc = nullptr;
   int pcap = 0;
 };
 
@@ -98,6 +97,9 @@ struct Solver {
   int* flags = nullptr;
   OpTables<double> t64;
   OpTables<float> t32;
+  // rho*cp per cell (device layout) for transient grids; independent of the key tables
+  double* rc64 = nullptr;
+  float* rc32 = nullptr;
   bool rc_valid = false;
   // FP64 state vectors (device layout)
   double* th = nullptr;
@@ -161,7 +163,14 @@ static T* kvec(Solver* s, int i) {
 enum { KR = 0, KR0 = 1, KP = 2, KPH = 3, KQ = 4, KS = 5, KSH = 6, KT = 7, KE = 8 };
 
 template <typename T>
-static OpParams<T> op_params(const Solver* s, const OpTables<T>& t) {
+static OpParams<T> op_params(const Solver* s, const OpTables<T>& t);
+template <>
+OpParams<double> op_params<double>(const Solver* s, const OpTables<double>& t);
+template <>
+OpParams<float> op_params<float>(const Solver* s, const OpTables<float>& t);
+
+template <typename T>
+static OpParams<T> op_params_rc(const Solver* s, const OpTables<T>& t, const T* rc) {
   OpParams<T> op;
   op.g = s->g;
   op.key = s->key;
@@ -169,7 +178,7 @@ static OpParams<T> op_params(const Solver* s, const OpTables<T>& t) {
   op.ty = t.ty;
   op.tz = t.tz;
   op.conv = t.conv;
-  op.rc = t.rc;
+  op.rc = rc;
   op.dzk = t.dzk;
   const double dx0 = s->dx, dy0 = s->dy;
   op.czm = (T)((s->HC[4] * dx0) * dy0);
@@ -181,13 +190,21 @@ static OpParams<T> op_params(const Solver* s, const OpTables<T>& t) {
   op.steady = s->steady;
   return op;
 }
+template <>
+OpParams<double> op_params<double>(const Solver* s, const OpTables<double>& t) {
+  return op_params_rc<double>(s, t, s->rc64);
+}
+template <>
+OpParams<float> op_params<float>(const Solver* s, const OpTables<float>& t) {
+  return op_params_rc<float>(s, t, s->rc32);
+}
 
 static void free_tables64(OpTables<double>& t) {
-  cudaFree(t.tx); cudaFree(t.ty); cudaFree(t.tz); cudaFree(t.conv); cudaFree(t.dzk); cudaFree(t.rc);
+  cudaFree(t.tx); cudaFree(t.ty); cudaFree(t.tz); cudaFree(t.conv); cudaFree(t.dzk);
   t = OpTables<double>();
 }
 static void free_tables32(OpTables<float>& t) {
-  cudaFree(t.tx); cudaFree(t.ty); cudaFree(t.tz); cudaFree(t.conv); cudaFree(t.dzk); cudaFree(t.rc);
+  cudaFree(t.tx); cudaFree(t.ty); cudaFree(t.tz); cudaFree(t.conv); cudaFree(t.dzk);
   t = OpTables<float>();
 }
 
@@ -199,6 +216,7 @@ static void destroy(Solver* s) {
   cudaFree(s->key); cudaFree(s->slots); cudaFree(s->slot_index); cudaFree(s->flags);
   free_tables64(s->t64);
   free_tables32(s->t32);
+  cudaFree(s->rc64); cudaFree(s->rc32);
   cudaFree(s->th); cudaFree(s->b); cudaFree(s->th_snap); cudaFree(s->r64);
   for (auto& p : s->kv) cudaFree(p);
   for (auto& p : s->stage) cudaFree(p);
@@ -836,18 +854,25 @@ static int set_fields(Solver* s, const double* lam, const double* mask, const do
   CK(cudaMemcpyAsync(s->slot_index, index, sizeof index, cudaMemcpyHostToDevice, s->stream));
   // rho*cp per cell for transient grids
   if (rho) {
-    if (!s->t64.rc) CK(cudaMalloc(&s->t64.rc, sizeof(double) * (size_t)g.n));
-    if (s->precision == H2G_MIXED && !s->t32.rc) CK(cudaMalloc(&s->t32.rc, sizeof(float) * (size_t)g.n));
-    CK(cudaMemsetAsync(s->t64.rc, 0, sizeof(double) * (size_t)g.n, s->stream));
+    if (!s->rc64) {
+      CK(cudaMalloc(&s->rc64, sizeof(double) * (size_t)g.n));
+      invalidate_graphs(s);
+    }
+    if (s->precision == H2G_MIXED && !s->rc32) {
+      CK(cudaMalloc(&s->rc32, sizeof(float) * (size_t)g.n));
+      invalidate_graphs(s);
+    }
+    CK(cudaMemsetAsync(s->rc64, 0, sizeof(double) * (size_t)g.n, s->stream));
+    if (s->rc32) CK(cudaMemsetAsync(s->rc32, 0, sizeof(float) * (size_t)g.n, s->stream));
   }
   dim3 grid((g.MX + 127) / 128, g.MY, g.MZ);
   k_make_keys<double><<<grid, 128, 0, s->stream>>>(g, s->stage[0], s->stage[1], rho ? s->stage[2] : nullptr,
                                                    rho ? s->stage[3] : nullptr, s->slots, s->slot_index, s->key,
-                                                   rho ? s->t64.rc : nullptr);
+                                                   rho ? s->rc64 : nullptr);
   CKL();
   if (rho && s->precision == H2G_MIXED) {
     k_make_keys<float><<<grid, 128, 0, s->stream>>>(g, s->stage[0], s->stage[1], s->stage[2], s->stage[3], s->slots,
-                                                    s->slot_index, s->key, s->t32.rc);
+                                                    s->slot_index, s->key, s->rc32);
     CKL();
   }
   s->rc_valid = rho != nullptr;
