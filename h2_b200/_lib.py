@@ -15,7 +15,7 @@ HEADER = os.path.join(os.path.dirname(HERE), "include", "h2g.h")
 
 H2G_OK, H2G_NOT_CONVERGED, H2G_BREAKDOWN, H2G_NONFINITE = 0, 1, 2, 3
 H2G_BAD_ARG, H2G_CUDA_ERROR, H2G_TIMEOUT, H2G_UNSUPPORTED = 4, 5, 6, 7
-H2G_FP64, H2G_MIXED = 0, 1
+H2G_FP64, H2G_MIXED, H2G_MIXED_IR = 0, 1, 2
 H2G_SMOOTHER_NONE, H2G_SMOOTHER_GS = 0, 1
 H2G_ISOTHERMAL, H2G_HEAT_FLUX, H2G_CONVECTION = 0, 1, 2
 

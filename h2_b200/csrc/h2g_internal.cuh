@@ -30,6 +30,7 @@ struct Geo {
   int NX, NY, NZ;  // interior sizes
   int HP;          // half-row pitch (positions)
   int HI;          // positions that can hold interior cells: (NX >> 1) + 1
+  int HN;          // positions that hold cells (guards included): (MX + 1) / 2
   long long plane; // elements per k plane: MY * 2 * HP
   long long n;     // elements per vector: MZ * plane
   __host__ __device__ __forceinline__ long long row(int c, int j, int k) const {
@@ -47,6 +48,7 @@ inline Geo make_geo(int MX, int MY, int MZ) {
   int half = (MX + 1) / 2;
   g.HP = (half + 31) / 32 * 32;
   g.HI = (g.NX >> 1) + 1;
+  g.HN = half;
   g.plane = (long long)MY * 2 * g.HP;
   g.n = (long long)MZ * g.plane;
   return g;

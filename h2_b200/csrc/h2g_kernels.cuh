@@ -153,12 +153,23 @@ __device__ __forceinline__ void reduce_finish(double (&v)[NV], double* __restric
   __syncthreads();
   if (!am_last) return;
   __threadfence();
+  // fixed-order sum of the partials; eight independent loads in flight per thread
   double acc[NV];
 #pragma unroll
   for (int q = 0; q < NV; ++q) acc[q] = 0.0;
-  for (unsigned b = tid; b < nb; b += nthr)
+  for (unsigned b0 = tid; b0 < nb; b0 += 8u * nthr) {
+    double t[NV][8];
 #pragma unroll
-    for (int q = 0; q < NV; ++q) acc[q] += __ldcg(partials + (size_t)q * nb + b);
+    for (int u = 0; u < 8; ++u) {
+      const unsigned b = b0 + (unsigned)u * nthr;
+#pragma unroll
+      for (int q = 0; q < NV; ++q) t[q][u] = b < nb ? __ldcg(partials + (size_t)q * nb + b) : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+#pragma unroll
+      for (int q = 0; q < NV; ++q) acc[q] += t[q][u];
+  }
   block_sum<NV>(acc, sm, tid, nthr);
   if (tid == 0) {
     st->ticket = 0;
@@ -174,6 +185,7 @@ __device__ __forceinline__ void reduce_finish(double (&v)[NV], double* __restric
 template <typename T>
 struct Coef {
   T cxm, cxp, cym, cyp, czm, czp, dd;
+  T sconv;  // convective terms + a_p0 (FP32 difference form only)
 };
 
 template <typename T>
@@ -218,7 +230,32 @@ __device__ __forceinline__ bool cell_coef(const OpParams<T>& op, int k, uint8_t 
   s = add(s, vzm);
   s = add(s, ap);
   c.dd = add(T(0), s);  // (1 - m0) + (...) * m0 with m0 = 1
+  if constexpr (sizeof(T) == 4) c.sconv = ((((vxp + vxm) + (vyp + vym)) + (vzp + vzm)) + ap);
   return true;
+}
+
+// A x at one cell.  FP64: (ss - dd*x) exactly as CalcAX! (NonUniform.jl:505-509).  FP32: the same
+// operator in difference form, sum c_nb*(x_nb - x) - (conv + a_p0)*x, which cancels first
+// differences instead of ss against dd*x (whose rounding error grows like 1/h^2 in FP32).
+template <typename T>
+__device__ __forceinline__ T apply_a(const Coef<T>& c, T x0, T xp, T xm, T yp, T ym, T zp, T zm) {
+  if constexpr (sizeof(T) == 4) {
+    T s = c.cxp * (xp - x0);
+    s = fmaf(c.cxm, xm - x0, s);
+    s = fmaf(c.cyp, yp - x0, s);
+    s = fmaf(c.cym, ym - x0, s);
+    s = fmaf(c.czp, zp - x0, s);
+    s = fmaf(c.czm, zm - x0, s);
+    return fmaf(-c.sconv, x0, s);
+  } else {
+    T s = mul(c.cxp, xp);
+    s = add(s, mul(c.cxm, xm));
+    s = add(s, mul(c.cyp, yp));
+    s = add(s, mul(c.cym, ym));
+    s = add(s, mul(c.czp, zp));
+    s = add(s, mul(c.czm, zm));
+    return sub(s, mul(c.dd, x0));
+  }
 }
 
 // ss of NonUniform.jl:505-507 (products summed left to right)
@@ -287,24 +324,27 @@ __global__ void __launch_bounds__(kThreads) k_rb_pass(OpParams<T> op, T* __restr
 // (copy_only) xx = bb everywhere (mycopy!, NonUniform.jl:549-551).
 // Grid as k_rb_pass; each thread owns position p of both half-rows of row (j,k).
 // ------------------------------------------------------------------------------------------
-template <typename T, int VM>
-__global__ void __launch_bounds__(kThreads) k_rb_first(OpParams<T> op, T* __restrict__ xx, T* __restrict__ v,
-                                                        const T* __restrict__ r, const T* __restrict__ q,
-                                                        const SolverState* __restrict__ st, int copy_only) {
+template <typename T, typename TV, int VM>
+__global__ void __launch_bounds__(kThreads) k_rb_first(OpParams<T> op, T* __restrict__ xx, TV* __restrict__ v,
+                                                        T* __restrict__ bbT, const TV* __restrict__ r,
+                                                        const TV* __restrict__ q, const SolverState* __restrict__ st,
+                                                        int copy_only) {
+  // T: precision of the smoother (xx, operator tables); TV: precision of the Krylov vectors.
+  // When they differ, bbT receives the smoother's copy of the right-hand side in T.
   if (st && st->stop) return;
   const Geo& g = op.g;
   const int p = blockIdx.x * kBX + threadIdx.x;
   const int j = 1 + blockIdx.y * kBY + threadIdx.y;
   const int k = 1 + blockIdx.z;
   if (j > g.NY) return;
-  T beta = T(0), omg = T(0), alpha = T(0);
+  TV beta = TV(0), omg = TV(0), alpha = TV(0);
   int first = 0;
   if (VM == 1) {
     first = st->first;
-    beta = (T)st->beta;
-    omg = (T)st->omega;
+    beta = (TV)st->beta;
+    omg = (TV)st->omega;
   } else if (VM == 2) {
-    alpha = (T)st->alpha;
+    alpha = (TV)st->alpha;
   }
 #pragma unroll
   for (int col = 0; col < 2; ++col) {
@@ -312,16 +352,18 @@ __global__ void __launch_bounds__(kThreads) k_rb_first(OpParams<T> op, T* __rest
     const int i = 2 * p + e;
     if (i < 1 || i > g.NX) continue;
     const long long ci = g.row(col, j, k) + p;
-    T b;
+    TV bv;
     if (VM == 0) {
-      b = v[ci];
+      bv = v[ci];
     } else if (VM == 1) {
-      b = first ? r[ci] : add(r[ci], mul(beta, sub(v[ci], mul(omg, q[ci]))));
-      v[ci] = b;
+      bv = first ? r[ci] : add(r[ci], mul(beta, sub(v[ci], mul(omg, q[ci]))));
+      v[ci] = bv;
     } else {
-      b = add(mul(-alpha, q[ci]), r[ci]);
-      v[ci] = b;
+      bv = add(mul(-alpha, q[ci]), r[ci]);
+      v[ci] = bv;
     }
+    const T b = (T)bv;
+    if (bbT) bbT[ci] = b;
     T out = T(0);
     if (copy_only) {
       out = b;
@@ -345,8 +387,8 @@ __global__ void __launch_bounds__(kThreads) k_rb_first(OpParams<T> op, T* __rest
 // and the stage finisher.  Grid (ceil(HI/32), ceil(2*NY/8), zc); block (32,8); rows of a block
 // interleave the two colours; each block walks planes k = 1+blockIdx.z, +gridDim.z, ...
 // ------------------------------------------------------------------------------------------
-template <typename T, int NDOT>
-__global__ void __launch_bounds__(kThreads) k_ax(OpParams<T> op, T* __restrict__ y, const T* __restrict__ x,
+template <typename T, int NDOT, typename TI = T>
+__global__ void __launch_bounds__(kThreads) k_ax(OpParams<T> op, T* __restrict__ y, const TI* __restrict__ x,
                                                   const T* __restrict__ u, const T* __restrict__ w,
                                                   SolverState* st, double* __restrict__ partials, int stage) {
   if (st && st->stop) return;
@@ -366,12 +408,10 @@ __global__ void __launch_bounds__(kThreads) k_ax(OpParams<T> op, T* __restrict__
     const uint8_t* key = op.key;
     Coef<T> c;
     T out = T(0);
-    if (cell_coef(op, k, key[n.c], key[n.xm], key[n.xp], key[n.ym], key[n.yp], key[n.zm], key[n.zp], n.c, c)) {
-      const T ss = nb_sum(c, x[n.xp], x[n.xm], x[n.yp], x[n.ym], x[n.zp], x[n.zm]);
-      out = sub(ss, mul(c.dd, x[n.c]));
-    }
+    if (cell_coef(op, k, key[n.c], key[n.xm], key[n.xp], key[n.ym], key[n.yp], key[n.zm], key[n.zp], n.c, c))
+      out = apply_a(c, (T)x[n.c], (T)x[n.xp], (T)x[n.xm], (T)x[n.yp], (T)x[n.ym], (T)x[n.zp], (T)x[n.zm]);
     y[n.c] = out;
-    if (NDOT >= 1) v[0] += (double)out * (double)(u ? u[n.c] : out);
+    if (NDOT >= 1) v[0] += (double)out * (u ? (double)u[n.c] : (double)out);
     if (NDOT >= 2) v[1] += (double)out * (double)w[n.c];
   }
   if constexpr (NDOT > 0) reduce_finish<NDOT>(v, partials, st, stage, 0, 0);
@@ -427,6 +467,23 @@ struct Vec16<float> {
   static constexpr int n = 4;
 };
 
+// V consecutive elements of type TT (V*sizeof(TT) = 8 or 16 bytes), converted to T
+template <typename T, typename TT, int V>
+__device__ __forceinline__ void ldv(const TT* p, T (&a)[V]) {
+  if constexpr (sizeof(TT) * V == 16) {
+    const float4 v = *reinterpret_cast<const float4*>(p);
+    const TT* s = reinterpret_cast<const TT*>(&v);
+#pragma unroll
+    for (int q = 0; q < V; ++q) a[q] = (T)s[q];
+  } else {
+    static_assert(sizeof(TT) * V == 8, "vector width");
+    const float2 v = *reinterpret_cast<const float2*>(p);
+    const TT* s = reinterpret_cast<const TT*>(&v);
+#pragma unroll
+    for (int q = 0; q < V; ++q) a[q] = (T)s[q];
+  }
+}
+
 template <typename T>
 __device__ __forceinline__ void ld16(const T* p, T (&a)[Vec16<T>::n]) {
   const typename Vec16<T>::type v = *reinterpret_cast<const typename Vec16<T>::type*>(p);
@@ -445,9 +502,9 @@ __device__ __forceinline__ void st16(T* p, const T (&a)[Vec16<T>::n]) {
 
 // BICG2! + Triad! + Fdot1/Fdot2 (NonUniform.jl:328-331 and the next 289):
 //   x += alpha*ph + omega*sh;  r = (-omega)*t + s;  d1 = (r,r), d2 = (r,r0) -> kStageUpdate
-template <typename T, typename TX>
-__global__ void __launch_bounds__(256) k_bicg_update(long long n, TX* __restrict__ x, const T* __restrict__ ph,
-                                                      const T* __restrict__ sh, T* __restrict__ r,
+template <typename T, typename TX, typename TP = T>
+__global__ void __launch_bounds__(256) k_bicg_update(long long n, TX* __restrict__ x, const TP* __restrict__ ph,
+                                                      const TP* __restrict__ sh, T* __restrict__ r,
                                                       const T* __restrict__ s, const T* __restrict__ t,
                                                       const T* __restrict__ r0, SolverState* st,
                                                       double* __restrict__ partials, cudaGraphConditionalHandle hc,
@@ -466,8 +523,8 @@ __global__ void __launch_bounds__(256) k_bicg_update(long long n, TX* __restrict
   for (long long b = blockIdx.x * (long long)blockDim.x + threadIdx.x; b < nv; b += (long long)gridDim.x * blockDim.x) {
     const long long o = b * V;
     T a_ph[V], a_sh[V], a_s[V], a_t[V], a_r0[V], a_r[V];
-    ld16(ph + o, a_ph);
-    ld16(sh + o, a_sh);
+    ldv<T, TP, V>(ph + o, a_ph);
+    ldv<T, TP, V>(sh + o, a_sh);
     ld16(s + o, a_s);
     ld16(t + o, a_t);
     ld16(r0 + o, a_r0);
@@ -511,8 +568,8 @@ __global__ void __launch_bounds__(256) k_cg_update(long long n, TX* __restrict__
 }
 
 // d1 = (a,b) with an optional copy dst = b (CG: p = z and rho = (r,z), NonUniform.jl:152-155)
-template <typename T>
-__global__ void __launch_bounds__(256) k_dot(long long n, const T* __restrict__ a, const T* __restrict__ b,
+template <typename T, typename T2 = T>
+__global__ void __launch_bounds__(256) k_dot(long long n, const T* __restrict__ a, const T2* __restrict__ b,
                                               T* __restrict__ dst, SolverState* st, double* __restrict__ partials,
                                               int stage) {
   if (st->stop) return;
@@ -523,7 +580,7 @@ __global__ void __launch_bounds__(256) k_dot(long long n, const T* __restrict__ 
     const long long o = i * V;
     T a_a[V], a_b[V];
     ld16(a + o, a_a);
-    ld16(b + o, a_b);
+    ldv<T, T2, V>(b + o, a_b);
 #pragma unroll
     for (int k = 0; k < V; ++k) v[0] += (double)a_a[k] * (double)a_b[k];
     if (dst) st16(dst + o, a_b);
@@ -532,8 +589,8 @@ __global__ void __launch_bounds__(256) k_dot(long long n, const T* __restrict__ 
 }
 
 // CG! p = z + beta*p (NonUniform.jl:218-220); sets the loop condition.
-template <typename T>
-__global__ void __launch_bounds__(256) k_cg_pupd(long long n, T* __restrict__ p, const T* __restrict__ z,
+template <typename T, typename TP = T>
+__global__ void __launch_bounds__(256) k_cg_pupd(long long n, T* __restrict__ p, const TP* __restrict__ z,
                                                   SolverState* st, cudaGraphConditionalHandle hc, int use_cond) {
   const int stop = st->stop;
   if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -548,7 +605,7 @@ __global__ void __launch_bounds__(256) k_cg_pupd(long long n, T* __restrict__ p,
     const long long o = i * V;
     T a_p[V], a_z[V];
     ld16(p + o, a_p);
-    ld16(z + o, a_z);
+    ldv<T, TP, V>(z + o, a_z);
 #pragma unroll
     for (int k = 0; k < V; ++k) a_p[k] = add(a_z[k], mul(beta, a_p[k]));
     st16(p + o, a_p);

@@ -15,6 +15,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
+#include <type_traits>
 #include <string>
 #include <vector>
 
@@ -64,7 +65,7 @@ struct SolveGraph {
   }
 };
 
-enum GraphKind { kGPbicg64 = 0, kGCg64 = 1, kGPbicg32 = 2, kGCg32 = 3, kGNum = 4 };
+enum GraphKind { kGPbicg64 = 0, kGCg64 = 1, kGPbicg32 = 2, kGCg32 = 3, kGPbicgMx = 4, kGCgMx = 5, kGNum = 6 };
 
 template <typename T>
 struct OpTables {
@@ -107,7 +108,7 @@ struct Solver {
   double* th_snap = nullptr;
   double* r64 = nullptr;
   // Krylov vectors in working precision: r, r0, p, ph, q, s, sh, t (+ e for refinement)
-  void* kv[9] = {nullptr};
+  void* kv[10] = {nullptr};
   size_t elem = 8;
   // column-major staging buffers (MX*MY*MZ doubles each)
   double* stage[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -144,7 +145,7 @@ static dim3 rb_grid(const Geo& g) { return dim3((g.HI + kBX - 1) / kBX, (g.NY + 
 
 static dim3 ax_grid(const Geo& g) {
   const int xt = (g.HI + kBX - 1) / kBX, yt = (2 * g.NY + kBY - 1) / kBY;
-  int zc = (4096 + xt * yt - 1) / (xt * yt);
+  int zc = (2048 + xt * yt - 1) / (xt * yt);
   zc = std::max(1, std::min(zc, g.NZ));
   return dim3(xt, yt, zc);
 }
@@ -160,7 +161,7 @@ template <typename T>
 static T* kvec(Solver* s, int i) {
   return reinterpret_cast<T*>(s->kv[i]);
 }
-enum { KR = 0, KR0 = 1, KP = 2, KPH = 3, KQ = 4, KS = 5, KSH = 6, KT = 7, KE = 8 };
+enum { KR = 0, KR0 = 1, KP = 2, KPH = 3, KQ = 4, KS = 5, KSH = 6, KT = 7, KE = 8, KBB = 9 };
 
 template <typename T>
 static OpParams<T> op_params(const Solver* s, const OpTables<T>& t);
@@ -197,6 +198,10 @@ OpParams<double> op_params<double>(const Solver* s, const OpTables<double>& t) {
 template <>
 OpParams<float> op_params<float>(const Solver* s, const OpTables<float>& t) {
   return op_params_rc<float>(s, t, s->rc32);
+}
+template <typename T>
+static OpParams<T> op_params(const Solver* s, const void* tables) {
+  return op_params<T>(s, *static_cast<const OpTables<T>*>(tables));
 }
 
 static void free_tables64(OpTables<double>& t) {
@@ -309,7 +314,7 @@ static int build_tables(Solver* s) {
     CK(cudaMalloc(&s->t64.conv, sizeof(double) * 4 * g.MZ));
     CK(cudaMalloc(&s->t64.dzk, sizeof(double) * g.MZ));
     s->t64.pcap = pc;
-    if (s->precision == H2G_MIXED) {
+    if (s->precision != H2G_FP64) {
       CK(cudaMalloc(&s->t32.tx, sizeof(float) * bytes_t));
       CK(cudaMalloc(&s->t32.ty, sizeof(float) * bytes_t));
       CK(cudaMalloc(&s->t32.tz, sizeof(float) * bytes_t));
@@ -323,7 +328,7 @@ static int build_tables(Solver* s) {
   CK(cudaMemcpyAsync(s->t64.tz, tz.data(), sizeof(double) * bytes_t, cudaMemcpyHostToDevice, s->stream));
   CK(cudaMemcpyAsync(s->t64.conv, conv.data(), sizeof(double) * 4 * g.MZ, cudaMemcpyHostToDevice, s->stream));
   CK(cudaMemcpyAsync(s->t64.dzk, s->dZ.data(), sizeof(double) * g.MZ, cudaMemcpyHostToDevice, s->stream));
-  if (s->precision == H2G_MIXED) {
+  if (s->precision != H2G_FP64) {
     auto to32 = [](const std::vector<double>& v) {
       std::vector<float> o(v.size());
       for (size_t i = 0; i < v.size(); ++i) o[i] = (float)v[i];
@@ -344,82 +349,102 @@ static int build_tables(Solver* s) {
 // ------------------------------------------------------------------------------------------
 // Graph capture of one Krylov iteration.
 // ------------------------------------------------------------------------------------------
-template <typename T, typename TX>
-static void launch_pbicg_body(Solver* s, cudaStream_t cs, const OpParams<T>& op, TX* x, SolverState* st,
-                              int smoother, cudaGraphConditionalHandle hc, int use_cond) {
+// One Krylov iteration.  T: Krylov vectors, inner products' inputs and the operator applied by
+// CalcAX (opA); TP: the preconditioner's precision (opM) and of its outputs p_, s_ (z for CG).
+// With TP != T the first pass also writes the smoother's copy of its right-hand side (bb32).
+template <typename T, typename TX, typename TP>
+static void launch_pbicg_body(Solver* s, cudaStream_t cs, const OpParams<T>& opA, const OpParams<TP>& opM, TX* x,
+                              SolverState* st, int smoother, cudaGraphConditionalHandle hc, int use_cond) {
   const Geo& g = s->g;
   T* r = kvec<T>(s, KR);
   T* r0 = kvec<T>(s, KR0);
   T* p = kvec<T>(s, KP);
-  T* ph = kvec<T>(s, KPH);
+  TP* ph = kvec<TP>(s, KPH);
   T* q = kvec<T>(s, KQ);
   T* sv = kvec<T>(s, KS);
-  T* sh = kvec<T>(s, KSH);
+  TP* sh = kvec<TP>(s, KSH);
   T* t = kvec<T>(s, KT);
+  TP* bbm = std::is_same<T, TP>::value ? nullptr : kvec<TP>(s, KBB);
   const dim3 rg = rb_grid(g), ag = ax_grid(g), blk(kBX, kBY);
   const int none = smoother == H2G_SMOOTHER_NONE;
   // p = r + beta (p - omega q); p_ = M^-1 p                     NonUniform.jl:296-305
-  k_rb_first<T, 1><<<rg, blk, 0, cs>>>(op, ph, p, r, q, st, none);
+  k_rb_first<TP, T, 1><<<rg, blk, 0, cs>>>(opM, ph, p, bbm, r, q, st, none);
   if (!none)
-    for (int pass = 1; pass < 2 * kSweeps; ++pass) k_rb_pass<T><<<rg, blk, 0, cs>>>(op, ph, p, pass & 1, T(1), st);
+    for (int pass = 1; pass < 2 * kSweeps; ++pass)
+      k_rb_pass<TP><<<rg, blk, 0, cs>>>(opM, ph, bbm ? bbm : reinterpret_cast<TP*>(p), pass & 1, TP(1), st);
   // q = A p_;  alpha = rho / (q, r0)                            NonUniform.jl:307-309
-  k_ax<T, 1><<<ag, blk, 0, cs>>>(op, q, ph, r0, nullptr, st, s->partials, kStageAlpha);
+  k_ax<T, 1, TP><<<ag, blk, 0, cs>>>(opA, q, ph, r0, nullptr, st, s->partials, kStageAlpha);
   // s = r - alpha q; s_ = M^-1 s                                NonUniform.jl:310-315
-  k_rb_first<T, 2><<<rg, blk, 0, cs>>>(op, sh, sv, r, q, st, none);
+  k_rb_first<TP, T, 2><<<rg, blk, 0, cs>>>(opM, sh, sv, bbm, r, q, st, none);
   if (!none)
-    for (int pass = 1; pass < 2 * kSweeps; ++pass) k_rb_pass<T><<<rg, blk, 0, cs>>>(op, sh, sv, pass & 1, T(1), st);
+    for (int pass = 1; pass < 2 * kSweeps; ++pass)
+      k_rb_pass<TP><<<rg, blk, 0, cs>>>(opM, sh, bbm ? bbm : reinterpret_cast<TP*>(sv), pass & 1, TP(1), st);
   // t = A s_; omega = (t,s)/(t,t)                               NonUniform.jl:317-326
-  k_ax<T, 2><<<ag, blk, 0, cs>>>(op, t, sh, nullptr, sv, st, s->partials, kStageOmega);
+  k_ax<T, 2, TP><<<ag, blk, 0, cs>>>(opA, t, sh, nullptr, sv, st, s->partials, kStageOmega);
   // x += alpha p_ + omega s_; r = s - omega t; res; next rho    NonUniform.jl:328-346
-  k_bicg_update<T, TX><<<elementwise_blocks(s), 256, 0, cs>>>(g.n, x, ph, sh, r, sv, t, r0, st, s->partials, hc,
-                                                              use_cond);
+  k_bicg_update<T, TX, TP><<<elementwise_blocks(s), 256, 0, cs>>>(g.n, x, ph, sh, r, sv, t, r0, st, s->partials, hc,
+                                                                  use_cond);
 }
 
-template <typename T, typename TX>
-static void launch_cg_body(Solver* s, cudaStream_t cs, const OpParams<T>& op, TX* x, SolverState* st, int smoother,
-                           cudaGraphConditionalHandle hc, int use_cond) {
+// z = M^-1 r with the first pass reading r (VM 0) and, for TP != T, writing bb32
+template <typename T, typename TP>
+static void launch_precond_r(Solver* s, cudaStream_t cs, const OpParams<TP>& opM, TP* z, T* r, SolverState* st,
+                             int smoother) {
+  const Geo& g = s->g;
+  const dim3 rg = rb_grid(g), blk(kBX, kBY);
+  const int none = smoother == H2G_SMOOTHER_NONE;
+  TP* bbm = std::is_same<T, TP>::value ? nullptr : kvec<TP>(s, KBB);
+  k_rb_first<TP, T, 0><<<rg, blk, 0, cs>>>(opM, z, r, bbm, nullptr, nullptr, st, none);
+  if (!none)
+    for (int pass = 1; pass < 2 * kSweeps; ++pass)
+      k_rb_pass<TP><<<rg, blk, 0, cs>>>(opM, z, bbm ? bbm : reinterpret_cast<TP*>(r), pass & 1, TP(1), st);
+}
+
+template <typename T, typename TX, typename TP>
+static void launch_cg_body(Solver* s, cudaStream_t cs, const OpParams<T>& opA, const OpParams<TP>& opM, TX* x,
+                           SolverState* st, int smoother, cudaGraphConditionalHandle hc, int use_cond) {
   const Geo& g = s->g;
   T* r = kvec<T>(s, KR);
   T* p = kvec<T>(s, KP);
   T* q = kvec<T>(s, KQ);
-  T* z = kvec<T>(s, KS);  // pcg_s holds z (NonUniform.jl:146)
-  const dim3 rg = rb_grid(g), ag = ax_grid(g), blk(kBX, kBY);
-  const int none = smoother == H2G_SMOOTHER_NONE;
+  TP* z = kvec<TP>(s, KS);  // pcg_s holds z (NonUniform.jl:146)
+  const dim3 ag = ax_grid(g), blk(kBX, kBY);
   const int nb = elementwise_blocks(s);
   // q = A p; alpha = rho_old / (p,q)                             NonUniform.jl:164-176
-  k_ax<T, 1><<<ag, blk, 0, cs>>>(op, q, p, p, nullptr, st, s->partials, kStageCgAlpha);
+  k_ax<T, 1, T><<<ag, blk, 0, cs>>>(opA, q, p, p, nullptr, st, s->partials, kStageCgAlpha);
   // x += alpha p; r -= alpha q; res                              NonUniform.jl:179-198
   k_cg_update<T, TX><<<nb, 256, 0, cs>>>(g.n, x, p, r, q, st, s->partials);
   // z = M^-1 r                                                  NonUniform.jl:201-203
-  k_rb_first<T, 0><<<rg, blk, 0, cs>>>(op, z, r, nullptr, nullptr, st, none);
-  if (!none)
-    for (int pass = 1; pass < 2 * kSweeps; ++pass) k_rb_pass<T><<<rg, blk, 0, cs>>>(op, z, r, pass & 1, T(1), st);
+  launch_precond_r<T, TP>(s, cs, opM, z, r, st, smoother);
   // rho_new = (r,z); beta                                       NonUniform.jl:206-215
-  k_dot<T><<<nb, 256, 0, cs>>>(g.n, r, z, nullptr, st, s->partials, kStageCgBeta);
+  k_dot<T, TP><<<nb, 256, 0, cs>>>(g.n, r, z, nullptr, st, s->partials, kStageCgBeta);
   // p = z + beta p                                              NonUniform.jl:218-220
-  k_cg_pupd<T><<<nb, 256, 0, cs>>>(g.n, p, z, st, hc, use_cond);
+  k_cg_pupd<T, TP><<<nb, 256, 0, cs>>>(g.n, p, z, st, hc, use_cond);
 }
 
-template <typename T>
-static std::vector<unsigned char> signature(const OpParams<T>& op, int smoother, const void* x) {
-  std::vector<unsigned char> v(sizeof op + sizeof smoother + sizeof x);
-  memcpy(v.data(), &op, sizeof op);
-  memcpy(v.data() + sizeof op, &smoother, sizeof smoother);
-  memcpy(v.data() + sizeof op + sizeof smoother, &x, sizeof x);
+template <typename T, typename TP>
+static std::vector<unsigned char> signature(const OpParams<T>& opA, const OpParams<TP>& opM, int smoother,
+                                            const void* x) {
+  std::vector<unsigned char> v(sizeof opA + sizeof opM + sizeof smoother + sizeof x);
+  unsigned char* d = v.data();
+  memcpy(d, &opA, sizeof opA);
+  memcpy(d + sizeof opA, &opM, sizeof opM);
+  memcpy(d + sizeof opA + sizeof opM, &smoother, sizeof smoother);
+  memcpy(d + sizeof opA + sizeof opM + sizeof smoother, &x, sizeof x);
   return v;
 }
 
-template <typename T, typename TX>
-static int get_graph(Solver* s, int kind, int smoother, const OpParams<T>& op, TX* x, SolverState* st,
-                     SolveGraph** out) {
+template <typename T, typename TX, typename TP>
+static int get_graph(Solver* s, int kind, int smoother, const OpParams<T>& op, const OpParams<TP>& opM, TX* x,
+                     SolverState* st, SolveGraph** out) {
   SolveGraph& G = s->graphs[kind][smoother ? 1 : 0];
-  std::vector<unsigned char> sig = signature(op, smoother, (const void*)x);
+  std::vector<unsigned char> sig = signature(op, opM, smoother, (const void*)x);
   if (G.exec && G.sig == sig) {
     *out = &G;
     return H2G_OK;
   }
   G.reset();
-  const bool cg = (kind == kGCg64 || kind == kGCg32);
+  const bool cg = (kind == kGCg64 || kind == kGCg32 || kind == kGCgMx);
   bool cond = !s->no_cond;
   if (cond) {
     cudaGraph_t parent = nullptr;
@@ -440,8 +465,8 @@ static int get_graph(Solver* s, int kind, int smoother, const OpParams<T>& op, T
       ok = cudaStreamBeginCaptureToGraph(s->cap, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) ==
            cudaSuccess;
       if (ok) {
-        if (cg) launch_cg_body<T, TX>(s, s->cap, op, x, st, smoother, hc, 1);
-        else launch_pbicg_body<T, TX>(s, s->cap, op, x, st, smoother, hc, 1);
+        if (cg) launch_cg_body<T, TX, TP>(s, s->cap, op, opM, x, st, smoother, hc, 1);
+        else launch_pbicg_body<T, TX, TP>(s, s->cap, op, opM, x, st, smoother, hc, 1);
         cudaGraph_t got = nullptr;
         ok = cudaStreamEndCapture(s->cap, &got) == cudaSuccess;
       }
@@ -462,8 +487,8 @@ static int get_graph(Solver* s, int kind, int smoother, const OpParams<T>& op, T
   if (!cond) {
     // fallback: a graph of one iteration, relaunched by the host until the state says stop
     CK(cudaStreamBeginCapture(s->cap, cudaStreamCaptureModeRelaxed));
-    if (cg) launch_cg_body<T, TX>(s, s->cap, op, x, st, smoother, 0, 0);
-    else launch_pbicg_body<T, TX>(s, s->cap, op, x, st, smoother, 0, 0);
+    if (cg) launch_cg_body<T, TX, TP>(s, s->cap, op, opM, x, st, smoother, 0, 0);
+    else launch_pbicg_body<T, TX, TP>(s, s->cap, op, opM, x, st, smoother, 0, 0);
     CK(cudaStreamEndCapture(s->cap, &G.graph));
     CK(cudaGraphInstantiate(&G.exec, G.graph, 0));
     G.cond = false;
@@ -556,35 +581,36 @@ static long long body_kernels(bool cg, int smoother) {
   return cg ? (1 + 1 + pc + 1 + 1) : (2 * pc + 2 + 1);
 }
 
-// FP64 PBiCGSTAB!/CG!: the same arithmetic as the reference, on the device.
-static int solve_fp64(Solver* s, bool cg, double tol, int maxItr, int smoother, int verbose, double* res_hist,
-                      h2g_result* out) {
+// PBiCGSTAB!/CG! with FP64 Krylov vectors, inner products and operator (the reference's
+// arithmetic).  TP is the precision of the RB-GS preconditioner: double (H2G_FP64, identical to
+// the reference) or float (H2G_MIXED: the 20 colour passes per iteration read and write FP32).
+template <typename TP>
+static int solve_krylov(Solver* s, bool cg, double tol, int maxItr, int smoother, int verbose, double* res_hist,
+                        h2g_result* out) {
   const Geo& g = s->g;
   int rc = ensure_hist(s, maxItr);
   if (rc) return rc;
   OpParams<double> op = op_params<double>(s, s->t64);
+  OpParams<TP> opM = op_params<TP>(s, std::is_same<TP, double>::value ? (const void*)&s->t64 : (const void*)&s->t32);
   SolverState* st = s->st;
   if ((rc = prime_state(s, st, tol, maxItr, s->hist, maxItr))) return rc;
   double* r = kvec<double>(s, KR);
-  const dim3 ag = ax_grid(g), rg = rb_grid(g), blk(kBX, kBY);
+  const dim3 ag = ax_grid(g), blk(kBX, kBY);
   // r = b - A theta, res0 (and r0 = r for PBiCGSTAB)            NonUniform.jl:131-141, 262-274
   k_rk<double><<<ag, blk, 0, s->stream>>>(op, r, cg ? nullptr : kvec<double>(s, KR0), s->th, s->b, st, s->partials,
                                           cg ? kStageInitCg : kStageInit);
   CKL();
   if (cg) {
     // z = M^-1 r; p = z; rho_old = (r,z)                          NonUniform.jl:147-155
-    double* z = kvec<double>(s, KS);
-    const int none = smoother == H2G_SMOOTHER_NONE;
-    k_rb_first<double, 0><<<rg, blk, 0, s->stream>>>(op, z, r, nullptr, nullptr, st, none);
-    if (!none)
-      for (int pass = 1; pass < 2 * kSweeps; ++pass)
-        k_rb_pass<double><<<rg, blk, 0, s->stream>>>(op, z, r, pass & 1, 1.0, st);
-    k_dot<double><<<elementwise_blocks(s), 256, 0, s->stream>>>(g.n, r, z, kvec<double>(s, KP), st, s->partials,
-                                                                 kStageCgInit);
+    TP* z = kvec<TP>(s, KS);
+    launch_precond_r<double, TP>(s, s->stream, opM, z, r, st, smoother);
+    k_dot<double, TP><<<elementwise_blocks(s), 256, 0, s->stream>>>(g.n, r, z, kvec<double>(s, KP), st, s->partials,
+                                                                     kStageCgInit);
     CKL();
   }
   SolveGraph* G = nullptr;
-  if ((rc = get_graph<double, double>(s, cg ? kGCg64 : kGPbicg64, smoother, op, s->th, st, &G))) return rc;
+  const int kind = std::is_same<TP, double>::value ? (cg ? kGCg64 : kGPbicg64) : (cg ? kGCgMx : kGPbicgMx);
+  if ((rc = get_graph<double, double, TP>(s, kind, smoother, op, opM, s->th, st, &G))) return rc;
   // a state that stopped at the start turns every kernel of the body into a no-op and the
   // last one ends the WHILE loop after one pass
   if ((rc = run_graph(s, G, st, maxItr))) return rc;
@@ -614,10 +640,12 @@ static int solve_fp64(Solver* s, bool cg, double tol, int maxItr, int smoother, 
   return status_of(fin);
 }
 
-// Mixed precision: FP32 PBiCGSTAB/CG (operator, smoother, Krylov vectors) inside FP64 iterative
+// H2G_MIXED_IR: FP32 PBiCGSTAB/CG (operator, smoother, Krylov vectors) inside FP64 iterative
 // refinement.  FP64 is kept for the true residual b - A theta, the accumulation of theta and
-// every inner product (the reductions accumulate in FP64).
-static int solve_mixed(Solver* s, bool cg, double tol, int maxItr, int smoother, int verbose, double* res_hist,
+// every inner product (the reductions accumulate in FP64).  On fine grids the FP32 BiCGSTAB
+// recurrences lose accuracy faster than a refinement pass can use (the inner solve can
+// diverge: the solve then reports H2G_NONFINITE); H2G_MIXED keeps the Krylov part in FP64.
+static int solve_ir(Solver* s, bool cg, double tol, int maxItr, int smoother, int verbose, double* res_hist,
                        h2g_result* out) {
   const Geo& g = s->g;
   int rc;
@@ -625,7 +653,7 @@ static int solve_mixed(Solver* s, bool cg, double tol, int maxItr, int smoother,
   OpParams<float> op32 = op_params<float>(s, s->t32);
   SolverState* st = s->st;
   SolverState* si = s->st_in;
-  const dim3 ag = ax_grid(g), rg = rb_grid(g), blk(kBX, kBY);
+  const dim3 ag = ax_grid(g), blk(kBX, kBY);
   const int nb = elementwise_blocks(s);
   if ((rc = prime_state(s, st, tol, maxItr, nullptr, 0))) return rc;
   // true residual r64 = b - A theta, ||r64||
@@ -658,16 +686,13 @@ static int solve_mixed(Solver* s, bool cg, double tol, int maxItr, int smoother,
       CKL();
       if (cg) {
         float* z = kvec<float>(s, KS);
-        const int none = smoother == H2G_SMOOTHER_NONE;
-        k_rb_first<float, 0><<<rg, blk, 0, s->stream>>>(op32, z, kvec<float>(s, KR), nullptr, nullptr, si, none);
-        if (!none)
-          for (int pass = 1; pass < 2 * kSweeps; ++pass)
-            k_rb_pass<float><<<rg, blk, 0, s->stream>>>(op32, z, kvec<float>(s, KR), pass & 1, 1.0f, si);
+        launch_precond_r<float, float>(s, s->stream, op32, z, kvec<float>(s, KR), si, smoother);
         k_dot<float><<<nb, 256, 0, s->stream>>>(g.n, kvec<float>(s, KR), z, kvec<float>(s, KP), si, s->partials,
                                                  kStageCgInit);
         CKL();
       }
-      if ((rc = get_graph<float, float>(s, cg ? kGCg32 : kGPbicg32, smoother, op32, e, si, &G))) return rc;
+      if ((rc = get_graph<float, float, float>(s, cg ? kGCg32 : kGPbicg32, smoother, op32, op32, e, si, &G)))
+        return rc;
       if ((rc = run_graph(s, G, si, cap))) return rc;
       // theta += ||r64|| e ; r64 = b - A theta
       k_ir_apply<<<nb, 256, 0, s->stream>>>(g.n, s->th, e, st);
@@ -728,8 +753,9 @@ static int solve(Solver* s, bool cg, double tol, int maxItr, int smoother, int v
     return fail(H2G_BAD_ARG, "Unsupported smoother: %d. Use none (0) or gs (1)", smoother);
   if (!(tol >= 0.0) || !std::isfinite(tol)) return fail(H2G_BAD_ARG, "bad tolerance");
   CK(cudaSetDevice(s->device));
-  if (s->precision == H2G_MIXED) return solve_mixed(s, cg, tol, maxItr, smoother, verbose, res_hist, out);
-  return solve_fp64(s, cg, tol, maxItr, smoother, verbose, res_hist, out);
+  if (s->precision == H2G_MIXED_IR) return solve_ir(s, cg, tol, maxItr, smoother, verbose, res_hist, out);
+  if (s->precision == H2G_MIXED) return solve_krylov<float>(s, cg, tol, maxItr, smoother, verbose, res_hist, out);
+  return solve_krylov<double>(s, cg, tol, maxItr, smoother, verbose, res_hist, out);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -740,11 +766,12 @@ static int create(int MX, int MY, int MZ, int precision, Solver** out) {
   *out = nullptr;
   if (MX < 3 || MY < 3 || MZ < 3) return fail(H2G_BAD_ARG, "grid too small: (%d,%d,%d)", MX, MY, MZ);
   if ((long long)MX * MY * MZ > (1ll << 31)) return fail(H2G_BAD_ARG, "grid too large");
-  if (precision != H2G_FP64 && precision != H2G_MIXED) return fail(H2G_BAD_ARG, "unknown precision %d", precision);
+  if (precision != H2G_FP64 && precision != H2G_MIXED && precision != H2G_MIXED_IR)
+    return fail(H2G_BAD_ARG, "unknown precision %d", precision);
   Solver* s = new h2g_solver();
   s->g = make_geo(MX, MY, MZ);
   s->precision = precision;
-  s->elem = precision == H2G_MIXED ? 4 : 8;
+  s->elem = precision == H2G_MIXED_IR ? 4 : 8;
   const char* nc = getenv("H2G_NO_COND");
   s->no_cond = nc && nc[0] == '1';
   int rc = H2G_OK;
@@ -767,7 +794,8 @@ static int create(int MX, int MY, int MZ, int precision, Solver** out) {
   AL(s->key, (size_t)g.n);
   const size_t kvb = s->elem * (size_t)g.n;
   for (int i = 0; i < 8; ++i) AL(s->kv[i], kvb);
-  if (precision == H2G_MIXED) {
+  if (precision == H2G_MIXED) AL(s->kv[KBB], sizeof(float) * (size_t)g.n);
+  if (precision == H2G_MIXED_IR) {
     AL(s->kv[KE], kvb);
     AL(s->r64, nb);
   }
@@ -858,7 +886,7 @@ static int set_fields(Solver* s, const double* lam, const double* mask, const do
       CK(cudaMalloc(&s->rc64, sizeof(double) * (size_t)g.n));
       invalidate_graphs(s);
     }
-    if (s->precision == H2G_MIXED && !s->rc32) {
+    if (s->precision != H2G_FP64 && !s->rc32) {
       CK(cudaMalloc(&s->rc32, sizeof(float) * (size_t)g.n));
       invalidate_graphs(s);
     }
@@ -870,7 +898,7 @@ static int set_fields(Solver* s, const double* lam, const double* mask, const do
                                                    rho ? s->stage[3] : nullptr, s->slots, s->slot_index, s->key,
                                                    rho ? s->rc64 : nullptr);
   CKL();
-  if (rho && s->precision == H2G_MIXED) {
+  if (rho && s->precision != H2G_FP64) {
     k_make_keys<float><<<grid, 128, 0, s->stream>>>(g, s->stage[0], s->stage[1], s->stage[2], s->stage[3], s->slots,
                                                     s->slot_index, s->key, s->rc32);
     CKL();
@@ -926,7 +954,7 @@ static int precond_t(Solver* s, const double* bb, double* xx, int smoother, cons
   if ((rc = upload<T>(s, bb, bd, 1))) return rc;
   const dim3 rg = rb_grid(s->g), blk(kBX, kBY);
   const int none = smoother == H2G_SMOOTHER_NONE;
-  k_rb_first<T, 0><<<rg, blk, 0, s->stream>>>(op, xd, bd, nullptr, nullptr, nullptr, none);
+  k_rb_first<T, T, 0><<<rg, blk, 0, s->stream>>>(op, xd, bd, nullptr, nullptr, nullptr, nullptr, none);
   if (!none)
     for (int pass = 1; pass < 2 * kSweeps; ++pass) k_rb_pass<T><<<rg, blk, 0, s->stream>>>(op, xd, bd, pass & 1, T(1), nullptr);
   CKL();
@@ -1062,13 +1090,13 @@ int h2g_cg(h2g_solver* h, double tol, int maxItr, int smoother, int verbose, dou
 }
 
 static std::mutex g_cache_mu;
-static h2g_solver* g_cache[2] = {nullptr, nullptr};
+static h2g_solver* g_cache[3] = {nullptr, nullptr, nullptr};
 
 static int oneshot(bool cg, int MX, int MY, int MZ, double* theta, const double* b, const double* lambda,
                    const double* mask, const double* rho, const double* cp, double dx, double dy, double dt,
                    const double* ZC, const double* dZ, const double* HC, double tol, int maxItr, int smoother,
                    int verbose, int is_steady, int precision, double* res_hist, h2g_result* out) {
-  if (precision != H2G_FP64 && precision != H2G_MIXED) return fail(H2G_BAD_ARG, "unknown precision %d", precision);
+  if (precision < H2G_FP64 || precision > H2G_MIXED_IR) return fail(H2G_BAD_ARG, "unknown precision %d", precision);
   if (!theta || !b) return fail(H2G_BAD_ARG, "null theta/b");
   std::lock_guard<std::mutex> lk(g_cache_mu);
   h2g_solver*& h = g_cache[precision];
@@ -1119,7 +1147,7 @@ int h2g_calcax(h2g_solver* h, const double* x, double* ax) {
   if (int rc = h2g::check_handle(h)) return rc;
   Solver* s = S(h);
   if (!s->grid_set || !s->fields_set) return fail(H2G_BAD_ARG, "h2g_set_grid and h2g_set_fields must come first");
-  if (s->precision == H2G_MIXED) return calcax_t<float>(s, x, ax, h2g::op_params<float>(s, s->t32));
+  if (s->precision == H2G_MIXED_IR) return calcax_t<float>(s, x, ax, h2g::op_params<float>(s, s->t32));
   return calcax_t<double>(s, x, ax, h2g::op_params<double>(s, s->t64));
 }
 
@@ -1130,7 +1158,7 @@ int h2g_calcrk(h2g_solver* h, double* r, double* res) {
   if (!s->grid_set || !s->fields_set) return fail(H2G_BAD_ARG, "h2g_set_grid and h2g_set_fields must come first");
   if (!res) return fail(H2G_BAD_ARG, "null res");
   OpParams<double> op = op_params<double>(s, s->t64);
-  double* rd = s->precision == H2G_MIXED ? s->r64 : kvec<double>(s, KR);
+  double* rd = s->precision == H2G_MIXED_IR ? s->r64 : kvec<double>(s, KR);
   int rc;
   if ((rc = prime_state(s, s->st, 0.0, 1, nullptr, 0))) return rc;
   k_rk<double><<<ax_grid(s->g), dim3(kBX, kBY), 0, s->stream>>>(op, rd, nullptr, s->th, s->b, s->st, s->partials,
@@ -1150,7 +1178,7 @@ int h2g_rbsor_pass(h2g_solver* h, double* x, const double* b, int color, double 
   if (!s->grid_set || !s->fields_set) return fail(H2G_BAD_ARG, "h2g_set_grid and h2g_set_fields must come first");
   if (color != 0 && color != 1) return fail(H2G_BAD_ARG, "color must be 0 or 1");
   if (!(omega > 0 && omega < 2)) return fail(H2G_BAD_ARG, "omega must be in (0,2)");
-  if (s->precision == H2G_MIXED) return rbsor_t<float>(s, x, b, color, omega, h2g::op_params<float>(s, s->t32));
+  if (s->precision != H2G_FP64) return rbsor_t<float>(s, x, b, color, omega, h2g::op_params<float>(s, s->t32));
   return rbsor_t<double>(s, x, b, color, omega, h2g::op_params<double>(s, s->t64));
 }
 
@@ -1161,7 +1189,7 @@ int h2g_preconditioner(h2g_solver* h, const double* bb, double* xx, int smoother
   if (!s->grid_set || !s->fields_set) return fail(H2G_BAD_ARG, "h2g_set_grid and h2g_set_fields must come first");
   if (smoother != H2G_SMOOTHER_NONE && smoother != H2G_SMOOTHER_GS)
     return fail(H2G_BAD_ARG, "Unsupported smoother: %d. Use none (0) or gs (1)", smoother);
-  if (s->precision == H2G_MIXED) return precond_t<float>(s, bb, xx, smoother, h2g::op_params<float>(s, s->t32));
+  if (s->precision != H2G_FP64) return precond_t<float>(s, bb, xx, smoother, h2g::op_params<float>(s, s->t32));
   return precond_t<double>(s, bb, xx, smoother, h2g::op_params<double>(s, s->t64));
 }
 
@@ -1172,7 +1200,9 @@ int h2g_bench_kernel(h2g_solver* h, int kind, int reps, int* launches) {
   if (!s->grid_set || !s->fields_set) return fail(H2G_BAD_ARG, "h2g_set_grid and h2g_set_fields must come first");
   if (kind != 0 && kind != 1) return fail(H2G_BAD_ARG, "kind must be 0 (RB-GS sweep) or 1 (CalcAX)");
   if (reps < 1) return fail(H2G_BAD_ARG, "reps must be positive");
-  if (s->precision == H2G_MIXED) return bench_t<float>(s, kind, reps, launches, h2g::op_params<float>(s, s->t32));
+  // the sweep runs in the preconditioner's precision, CalcAX in the Krylov solver's
+  const bool fp32 = kind == 0 ? s->precision != H2G_FP64 : s->precision == H2G_MIXED_IR;
+  if (fp32) return bench_t<float>(s, kind, reps, launches, h2g::op_params<float>(s, s->t32));
   return bench_t<double>(s, kind, reps, launches, h2g::op_params<double>(s, s->t64));
 }
 

@@ -17,7 +17,7 @@ import numpy as np
 from . import _lib as L
 
 _SMOOTHERS = {"none": L.H2G_SMOOTHER_NONE, "gs": L.H2G_SMOOTHER_GS}
-_PRECISION = {"fp64": L.H2G_FP64, "mixed": L.H2G_MIXED}
+_PRECISION = {"fp64": L.H2G_FP64, "mixed": L.H2G_MIXED, "mixed_ir": L.H2G_MIXED_IR}
 
 
 def _f64(a: np.ndarray, name: str) -> np.ndarray:

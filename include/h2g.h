@@ -38,8 +38,12 @@ extern "C" {
 #define H2G_UNSUPPORTED 7     /* input outside what this build implements (message says what) */
 
 /* ---- precision ---------------------------------------------------------------------- */
-#define H2G_FP64 0  /* FP64 throughout, same arithmetic as the reference */
-#define H2G_MIXED 1 /* FP32 operator/smoother/Krylov vectors inside FP64 iterative refinement */
+#define H2G_FP64 0     /* FP64 throughout, same arithmetic as the reference */
+#define H2G_MIXED 1    /* FP32 RB-GS preconditioner (operator tables, smoother vectors) inside FP64
+                          PBiCGSTAB/CG: FP64 Krylov vectors, inner products, CalcAX and solution */
+#define H2G_MIXED_IR 2 /* FP32 operator, smoother and Krylov vectors inside FP64 iterative
+                          refinement (FP64 true residual, solution accumulation, inner products);
+                          its FP32 BiCGSTAB can diverge on fine grids (reported as H2G_NONFINITE) */
 
 /* ---- smoother (NonUniform.jl:36-41: :none, :gs) -------------------------------------- */
 #define H2G_SMOOTHER_NONE 0
@@ -64,8 +68,8 @@ typedef struct h2g_bc {
  * plus what the GPU path adds. */
 typedef struct h2g_result {
   int isconverged; /* 1 if ||r_k|| / ||r_0|| < tol */
-  int itr;         /* iterations: PBiCGSTAB/CG iterations (FP64) or all inner iterations (mixed) */
-  int outer;       /* iterative-refinement passes (mixed), 0 for FP64 */
+  int itr;         /* PBiCGSTAB/CG iterations (all inner iterations for H2G_MIXED_IR) */
+  int outer;       /* iterative-refinement passes (H2G_MIXED_IR), 0 otherwise */
   int status;      /* same value the call returns */
   double res0;     /* initial residual ||b - A theta||_2 (NonUniform.jl:263) */
   double res;      /* final relative residual ||r|| / res0 */
@@ -105,7 +109,7 @@ int h2g_get_theta(h2g_solver *h, double *theta);
  * the same start without a host copy). */
 int h2g_theta_snapshot(h2g_solver *h, int op);
 
-/* Iterative-refinement settings for H2G_MIXED: inner relative tolerance of each FP32 solve
+/* Iterative-refinement settings for H2G_MIXED_IR: inner relative tolerance of each FP32 solve
  * and the cap on refinement passes (defaults 1e-4 and 40). */
 int h2g_set_mixed_params(h2g_solver *h, double inner_tol, int max_outer);
 

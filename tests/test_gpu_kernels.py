@@ -99,13 +99,17 @@ def test_preconditioner_bit_exact(oracle, case):
 
 
 def test_fp32_kernels_close_to_fp64(oracle):
+    """FP32 operator (difference form, H2G_MIXED_IR) and FP32 preconditioner (H2G_MIXED) vs the
+    FP64 oracle; H2G_MIXED applies CalcAX in FP64, bit-identical to the reference."""
     prob = mode3_model(oracle, 40)
-    s = make_solver(prob, precision="mixed")
     x = random_interior(prob.shape, 3)
     ref = oracle.calc_ax(prob, x)[1:-1, 1:-1, 1:-1]
-    got = s.calc_ax(x)[1:-1, 1:-1, 1:-1]
-    scale = np.abs(ref).max()
-    assert np.abs(got - ref).max() <= 2e-6 * scale
+    s_ir = make_solver(prob, precision="mixed_ir")
+    got = s_ir.calc_ax(x)[1:-1, 1:-1, 1:-1]
+    assert np.abs(got - ref).max() <= 2e-6 * np.abs(ref).max()
+    s_ir.close()
+    s = make_solver(prob, precision="mixed")
+    assert np.array_equal(s.calc_ax(x)[1:-1, 1:-1, 1:-1], ref)
     bb = random_interior(prob.shape, 4)
     pref = oracle.preconditioner(prob, bb, "gs")
     pgot = s.preconditioner(bb, "gs")
