@@ -33,10 +33,9 @@ struct Geo {
   int HN;          // positions that hold cells (guards included): (MX + 1) / 2
   long long plane; // elements per k plane: MY * 2 * HP
   long long n;     // elements per vector: MZ * plane
-  __host__ __device__ __forceinline__ long long row(int c, int j, int k) const {
-    return ((long long)k * MY + j) * 2 * HP + (long long)c * HP;
-  }
-  __host__ __device__ __forceinline__ long long off(int i, int j, int k) const {
+  // offsets fit in 32 bits (h2g_create rejects grids with n >= 2^31)
+  __host__ __device__ __forceinline__ int row(int c, int j, int k) const { return ((k * MY + j) * 2 + c) * HP; }
+  __host__ __device__ __forceinline__ int off(int i, int j, int k) const {
     return row(((i + j + k) & 1) ^ 1, j, k) + (i >> 1);
   }
 };
@@ -104,9 +103,9 @@ template <typename T>
 struct OpParams {
   Geo g;
   const uint8_t* key;  // per cell: material index (bits 0-6) | mask (bit 7), device layout
-  const T* tx;         // [MZ][2][P][P] x-face conductances of plane k (fac 1, fac 2)
-  const T* ty;         // [MZ][2][P][P] y-face conductances
-  const T* tz;         // [MZ][2][P][P] z-face between planes k-1 and k
+  const T* tx;         // [MZ][P][256] x-face conductance of plane k: [k][key0 & 0x7f][neighbour key]
+  const T* ty;         // [MZ][P][256] y-face conductances
+  const T* tz;         // [MZ][P][256] z-face between planes k-1 and k
   const T* conv;       // [MZ][4] convective terms of x-, x+, y-, y+ faces at plane k
   const T* rc;         // rho*cp per cell (device layout), transient only
   const T* dzk;        // [MZ] dZ

@@ -44,6 +44,14 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double (*sm)[NV], int
   __syncthreads();
 }
 
+// Programmatic dependent launch: wait until the preceding kernel's writes are visible, then let
+// the next kernel of the stream start launching its blocks (they wait the same way).  Both are
+// no-ops for a kernel launched without the programmatic-serialization attribute.
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 __device__ __forceinline__ void set_cond(cudaGraphConditionalHandle h, int use_cond, int value) {
   if (use_cond) cudaGraphSetConditional(h, value ? 1u : 0u);
 }
@@ -188,26 +196,21 @@ struct Coef {
   T sconv;  // convective terms + a_p0 (FP32 difference form only)
 };
 
-template <typename T>
-__device__ __forceinline__ T face(const T* __restrict__ tab, int lvl, int P, int a0, uint8_t kn) {
-  const int f = (kn & 0x80) ? 0 : 1;  // fac = 2 - div(ma+mb,2): 1 if both unmasked, else 2
-  return __ldg(tab + (((size_t)lvl * 2 + f) * P + (kn & 0x7f)) * P + a0);
-}
-
-// Returns false for a masked cell (m0 = 0).  Order of the additions of dd follows
-// NonUniform.jl:501-502 exactly.
+// Coefficients of one unmasked cell (key k0) at plane k from its neighbours' keys.  The tables
+// are indexed by the neighbour's whole key byte: its mask bit selects lambda_f's factor
+// 2 - div(ma+mb, 2) (1 if the neighbour is unmasked, 2 if it is a masked guard).  The order of
+// the additions of dd follows NonUniform.jl:501-502 exactly.
 template <typename T>
 __device__ __forceinline__ bool cell_coef(const OpParams<T>& op, int k, uint8_t k0, uint8_t kxm, uint8_t kxp,
-                                          uint8_t kym, uint8_t kyp, uint8_t kzm, uint8_t kzp, long long ci,
-                                          Coef<T>& c) {
+                                          uint8_t kym, uint8_t kyp, uint8_t kzm, uint8_t kzp, int ci, Coef<T>& c) {
   if (!(k0 & 0x80)) return false;
-  const int P = op.P, a0 = k0 & 0x7f;
-  c.cxm = face(op.tx, k, P, a0, kxm);
-  c.cxp = face(op.tx, k, P, a0, kxp);
-  c.cym = face(op.ty, k, P, a0, kym);
-  c.cyp = face(op.ty, k, P, a0, kyp);
-  c.czm = face(op.tz, k, P, a0, kzm);
-  c.czp = face(op.tz, k + 1, P, a0, kzp);
+  const int bx = (k * op.P + (k0 & 0x7f)) << 8;
+  c.cxm = __ldg(op.tx + (bx | kxm));
+  c.cxp = __ldg(op.tx + (bx | kxp));
+  c.cym = __ldg(op.ty + (bx | kym));
+  c.cyp = __ldg(op.ty + (bx | kyp));
+  c.czm = __ldg(op.tz + (bx | kzm));
+  c.czp = __ldg(op.tz + ((bx + (op.P << 8)) | kzp));
   const T* cv = op.conv + 4 * k;
   const T vxm = (kxm & 0x80) ? T(0) : __ldg(cv + 0);
   const T vxp = (kxp & 0x80) ? T(0) : __ldg(cv + 1);
@@ -234,6 +237,23 @@ __device__ __forceinline__ bool cell_coef(const OpParams<T>& op, int k, uint8_t 
   return true;
 }
 
+// ss of NonUniform.jl:505-507 (products summed left to right)
+template <typename T>
+__device__ __forceinline__ T nb_sum(const Coef<T>& c, T xp, T xm, T yp, T ym, T zp, T zm) {
+  T s = mul(c.cxp, xp);
+  s = add(s, mul(c.cxm, xm));
+  s = add(s, mul(c.cyp, yp));
+  s = add(s, mul(c.cym, ym));
+  s = add(s, mul(c.czp, zp));
+  s = add(s, mul(c.czm, zm));
+  return s;
+}
+
+// Gauss-Seidel update of one cell: (ss - b)/dd, correctly rounded in both precisions (an
+// approximate FP32 division weakens the FP32 preconditioner enough to multiply the iterations).
+__device__ __forceinline__ double gs_div(double a, double b) { return __ddiv_rn(a, b); }
+__device__ __forceinline__ float gs_div(float a, float b) { return a / b; }
+
 // A x at one cell.  FP64: (ss - dd*x) exactly as CalcAX! (NonUniform.jl:505-509).  FP32: the same
 // operator in difference form, sum c_nb*(x_nb - x) - (conv + a_p0)*x, which cancels first
 // differences instead of ss against dd*x (whose rounding error grows like 1/h^2 in FP32).
@@ -258,60 +278,122 @@ __device__ __forceinline__ T apply_a(const Coef<T>& c, T x0, T xp, T xm, T yp, T
   }
 }
 
-// ss of NonUniform.jl:505-507 (products summed left to right)
+// ------------------------------------------------------------------------------------------
+// Stencil kernels.
+//
+// A block is 32 threads along the half-row (positions p) x kBY rows (j); warps run along p.  For
+// a cell of colour c at (p, j, k) every neighbour has colour o = 1-c: the z-neighbours and one
+// x-neighbour are the o-colour column at (p, j) (planes k-1, k+1 and k), the other x-neighbour
+// is the o-colour value at p-1 or p+1 -- the same column of the adjacent lane, taken with a
+// warp shuffle (the warp's edge lanes load it) -- and the y-neighbours are the o-colour columns
+// (p, j+-1).  Each thread updates two cells that share most of these loads: the RB pass takes
+// the colour-c cells of its column at planes k and k+1; CalcAX/CalcRK and the first pass take
+// both colours of its column at plane k.  All loads of a thread are issued before its first
+// store.  Offsets are 32-bit.
+// ------------------------------------------------------------------------------------------
+constexpr unsigned kFull = 0xffffffffu;
+
 template <typename T>
-__device__ __forceinline__ T nb_sum(const Coef<T>& c, T xp, T xm, T yp, T ym, T zp, T zm) {
-  T s = mul(c.cxp, xp);
-  s = add(s, mul(c.cxm, xm));
-  s = add(s, mul(c.cyp, yp));
-  s = add(s, mul(c.cym, ym));
-  s = add(s, mul(c.czp, zp));
-  s = add(s, mul(c.czm, zm));
-  return s;
-}
+__device__ __forceinline__ T ldro(const T* p) { return __ldg(p); }
 
-// Offsets of a cell and its six neighbours in the device layout.
-struct Nbr {
-  long long c, xm, xp, ym, yp, zm, zp;
-};
-
-__device__ __forceinline__ Nbr neighbours(const Geo& g, int p, int col, int j, int k, int e) {
-  Nbr n;
-  const long long ro = g.row(col ^ 1, j, k);
-  n.c = g.row(col, j, k) + p;
-  n.xm = ro + p - 1 + e;
-  n.xp = ro + p + e;
-  n.ym = ro - 2 * g.HP + p;
-  n.yp = ro + 2 * g.HP + p;
-  n.zm = ro - g.plane + p;
-  n.zp = ro + g.plane + p;
-  return n;
+// x-neighbours of a colour-c cell at position p with parity e (x-1 = o[p-1+e], x+1 = o[p+e]),
+// given the o-colour value and key of this lane's column at that plane.  All lanes must call it.
+template <typename T, bool VAL, typename TI = T>
+__device__ __forceinline__ void x_nbrs(T oc, int okc, int e, int lane, int p, int HN, const TI* x,
+                                       const uint8_t* key, int rowo, T& xm, T& xp, int& kxm, int& kxp) {
+  T left = T(0), right = T(0);
+  if (VAL) {
+    left = __shfl_up_sync(kFull, oc, 1);
+    right = __shfl_down_sync(kFull, oc, 1);
+  }
+  int kl = __shfl_up_sync(kFull, okc, 1), kr = __shfl_down_sync(kFull, okc, 1);
+  if (lane == 0 && !e && p >= 1) {
+    if (VAL) left = (T)ldro(x + rowo + p - 1);
+    kl = key[rowo + p - 1];
+  }
+  if (lane == 31 && e && p + 1 < HN) {
+    if (VAL) right = (T)ldro(x + rowo + p + 1);
+    kr = key[rowo + p + 1];
+  }
+  if (e) {
+    xm = oc; kxm = okc; xp = right; kxp = kr;
+  } else {
+    xm = left; kxm = kl; xp = oc; kxp = okc;
+  }
 }
 
 // ------------------------------------------------------------------------------------------
 // rbsor_core! (NonUniform.jl:848-915): one colour pass of RB-SOR on x with rhs bb.
-// Grid (ceil(HI/32), ceil(NY/8), NZ); one thread per cell of the colour.
+// Grid (ceil(HN/32), ceil(NY/kBY), ceil(NZ/2)); thread = colour-c cells of column (p,j) at
+// planes k0, k0+1.
 // ------------------------------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(kThreads) k_rb_pass(OpParams<T> op, T* __restrict__ x, const T* __restrict__ bb,
-                                                       int color, T omega, const SolverState* __restrict__ st) {
+__global__ void __launch_bounds__(kThreads) k_rb_pass(OpParams<T> op, T* x, const T* __restrict__ bb, int color,
+                                                       T omega, const SolverState* __restrict__ st) {
+  pdl_enter();
   if (st && st->stop) return;
   const Geo& g = op.g;
-  const int p = blockIdx.x * kBX + threadIdx.x;
+  const int lane = threadIdx.x, p = blockIdx.x * kBX + lane;
   const int j = 1 + blockIdx.y * kBY + threadIdx.y;
-  const int k = 1 + blockIdx.z;
-  if (j > g.NY) return;
-  const int e = (1 + color + j + k) & 1;
-  const int i = 2 * p + e;
-  if (i < 1 || i > g.NX) return;
-  const Nbr n = neighbours(g, p, color, j, k, e);
+  const int k0 = 1 + 2 * blockIdx.z;
+  if (j > g.NY) return;  // uniform per warp
+  const int o = color ^ 1;
+  const bool pok = p < g.HN;
   const uint8_t* key = op.key;
-  Coef<T> c;
-  if (!cell_coef(op, k, key[n.c], key[n.xm], key[n.xp], key[n.ym], key[n.yp], key[n.zm], key[n.zp], n.c, c)) return;
-  const T pp = x[n.c];
-  const T ss = nb_sum(c, x[n.xp], x[n.xm], x[n.yp], x[n.ym], x[n.zp], x[n.zm]);
-  const T dp = sub(dvd(sub(ss, bb[n.c]), c.dd), pp);  // * m0 (= 1)
-  x[n.c] = add(pp, mul(omega, dp));
+  const int HP2 = 2 * g.HP, PL = (int)g.plane;
+  const int ro0 = g.row(o, j, k0), rc0 = g.row(color, j, k0);
+  // o-colour column at (p, j), planes k0-1 .. k0+2
+  T col[4];
+  int kcol[4];
+#pragma unroll
+  for (int t = 0; t < 4; ++t) {
+    col[t] = T(0);
+    kcol[t] = 0;
+    if (pok && k0 - 1 + t <= g.MZ - 1) {
+      const int a = ro0 + (t - 1) * PL + p;
+      col[t] = ldro(x + a);
+      kcol[t] = key[a];
+    }
+  }
+  T ym[2], yp[2], pp[2], bv[2];
+  int kym[2], kyp[2], kc[2];
+  bool ok[2];
+#pragma unroll
+  for (int u = 0; u < 2; ++u) {
+    const int k = k0 + u, e = (1 + color + j + k) & 1, i = 2 * p + e;
+    ok[u] = pok && k <= g.NZ && i >= 1 && i <= g.NX;
+    ym[u] = yp[u] = pp[u] = bv[u] = T(0);
+    kym[u] = kyp[u] = kc[u] = 0;
+    if (ok[u]) {
+      const int ao = ro0 + u * PL + p, ac = rc0 + u * PL + p;
+      ym[u] = ldro(x + ao - HP2);
+      yp[u] = ldro(x + ao + HP2);
+      kym[u] = key[ao - HP2];
+      kyp[u] = key[ao + HP2];
+      kc[u] = key[ac];
+      pp[u] = x[ac];
+      bv[u] = bb[ac];
+    }
+  }
+  T xm[2], xp[2];
+  int kxm[2], kxp[2];
+#pragma unroll
+  for (int u = 0; u < 2; ++u) {
+    const int e = (1 + color + j + k0 + u) & 1;
+    x_nbrs<T, true>(col[u + 1], kcol[u + 1], e, lane, p, g.HN, x, key, ro0 + u * PL, xm[u], xp[u], kxm[u], kxp[u]);
+  }
+#pragma unroll
+  for (int u = 0; u < 2; ++u) {
+    if (!ok[u]) continue;
+    const int ac = rc0 + u * PL + p;
+    Coef<T> c;
+    if (!cell_coef(op, k0 + u, (uint8_t)kc[u], (uint8_t)kxm[u], (uint8_t)kxp[u], (uint8_t)kym[u], (uint8_t)kyp[u],
+                   (uint8_t)kcol[u], (uint8_t)kcol[u + 2], ac, c))
+      continue;
+    const T ss = nb_sum(c, xp[u], xm[u], yp[u], ym[u], col[u + 2], col[u]);
+    const T dp = sub(gs_div(sub(ss, bv[u]), c.dd), pp[u]);  // * m0 (= 1)
+    x[ac] = add(pp[u], mul(omega, dp));
+  }
 }
 
 // ------------------------------------------------------------------------------------------
@@ -321,22 +403,26 @@ __global__ void __launch_bounds__(kThreads) k_rb_pass(OpParams<T> op, T* __restr
 //   VM 1: p = r (first iteration) or p = r + beta*(p - omega*q)    BiCG1!, NonUniform.jl:296-301
 //   VM 2: s = (-alpha)*q + r                                         Triad!, NonUniform.jl:310-311
 // Colour-0 cells get xx = ((0 - bb)/dd - 0)*m0; colour-1 cells get 0.  With smoother :none
-// (copy_only) xx = bb everywhere (mycopy!, NonUniform.jl:549-551).
-// Grid as k_rb_pass; each thread owns position p of both half-rows of row (j,k).
+// (copy_only) xx = bb everywhere (mycopy!, NonUniform.jl:549-551).  T: precision of the smoother
+// (xx, operator tables); TV: precision of the Krylov vectors; when they differ, bbT receives the
+// smoother's copy of the right-hand side in T.  Thread = both colours of column (p,j) at plane k.
 // ------------------------------------------------------------------------------------------
 template <typename T, typename TV, int VM>
 __global__ void __launch_bounds__(kThreads) k_rb_first(OpParams<T> op, T* __restrict__ xx, TV* __restrict__ v,
                                                         T* __restrict__ bbT, const TV* __restrict__ r,
                                                         const TV* __restrict__ q, const SolverState* __restrict__ st,
                                                         int copy_only) {
-  // T: precision of the smoother (xx, operator tables); TV: precision of the Krylov vectors.
-  // When they differ, bbT receives the smoother's copy of the right-hand side in T.
+  pdl_enter();
   if (st && st->stop) return;
   const Geo& g = op.g;
-  const int p = blockIdx.x * kBX + threadIdx.x;
+  const int lane = threadIdx.x, p = blockIdx.x * kBX + lane;
   const int j = 1 + blockIdx.y * kBY + threadIdx.y;
   const int k = 1 + blockIdx.z;
   if (j > g.NY) return;
+  const bool pok = p < g.HN;
+  const uint8_t* key = op.key;
+  const int HP2 = 2 * g.HP, PL = (int)g.plane;
+  const int r0 = g.row(0, j, k), r1 = r0 + g.HP;
   TV beta = TV(0), omg = TV(0), alpha = TV(0);
   int first = 0;
   if (VM == 1) {
@@ -346,34 +432,55 @@ __global__ void __launch_bounds__(kThreads) k_rb_first(OpParams<T> op, T* __rest
   } else if (VM == 2) {
     alpha = (TV)st->alpha;
   }
+  const int e0 = (1 + j + k) & 1;
+  bool ok[2];
+  TV bvv[2];
 #pragma unroll
   for (int col = 0; col < 2; ++col) {
-    const int e = (1 + col + j + k) & 1;
-    const int i = 2 * p + e;
-    if (i < 1 || i > g.NX) continue;
-    const long long ci = g.row(col, j, k) + p;
-    TV bv;
-    if (VM == 0) {
-      bv = v[ci];
-    } else if (VM == 1) {
-      bv = first ? r[ci] : add(r[ci], mul(beta, sub(v[ci], mul(omg, q[ci]))));
-      v[ci] = bv;
-    } else {
-      bv = add(mul(-alpha, q[ci]), r[ci]);
-      v[ci] = bv;
+    const int i = 2 * p + (e0 ^ col);
+    ok[col] = pok && i >= 1 && i <= g.NX;
+    bvv[col] = TV(0);
+    if (!ok[col]) continue;
+    const int ci = (col ? r1 : r0) + p;
+    if (VM == 0) bvv[col] = v[ci];
+    else if (VM == 1) bvv[col] = first ? r[ci] : add(r[ci], mul(beta, sub(v[ci], mul(omg, q[ci]))));
+    else bvv[col] = add(mul(-alpha, q[ci]), r[ci]);
+  }
+  // keys for the colour-0 cell: its own and its colour-1 neighbours
+  int k1c = 0, k1m = 0, k1p = 0, kym = 0, kyp = 0, k0c = 0;
+  if (!copy_only && pok) {
+    const int a1 = r1 + p;
+    k1c = key[a1];
+    if (ok[0]) {
+      k1m = key[a1 - PL];
+      k1p = key[a1 + PL];
+      kym = key[a1 - HP2];
+      kyp = key[a1 + HP2];
+      k0c = key[r0 + p];
     }
-    const T b = (T)bv;
+  }
+  int kxm = 0, kxp = 0;
+  if (!copy_only) {
+    T dm, dp_;
+    x_nbrs<T, false>(T(0), k1c, e0, lane, p, g.HN, (const T*)nullptr, key, r1, dm, dp_, kxm, kxp);
+  }
+#pragma unroll
+  for (int col = 0; col < 2; ++col) {
+    if (!ok[col]) continue;
+    const int ci = (col ? r1 : r0) + p;
+    const TV bvx = bvv[col];
+    if (VM != 0) v[ci] = bvx;
+    const T b = (T)bvx;
     if (bbT) bbT[ci] = b;
     T out = T(0);
     if (copy_only) {
       out = b;
     } else if (col == 0) {
-      const Nbr n = neighbours(g, p, col, j, k, e);
-      const uint8_t* key = op.key;
       Coef<T> c;
-      if (cell_coef(op, k, key[n.c], key[n.xm], key[n.xp], key[n.ym], key[n.yp], key[n.zm], key[n.zp], n.c, c)) {
+      if (cell_coef(op, k, (uint8_t)k0c, (uint8_t)kxm, (uint8_t)kxp, (uint8_t)kym, (uint8_t)kyp, (uint8_t)k1m,
+                    (uint8_t)k1p, ci, c)) {
         const T ss = T(0);
-        const T dp = sub(dvd(sub(ss, b), c.dd), T(0));
+        const T dp = sub(gs_div(sub(ss, b), c.dd), T(0));
         out = add(T(0), dp);  // pp + omega*dp with pp = 0, omega = 1
       }
     }
@@ -381,38 +488,110 @@ __global__ void __launch_bounds__(kThreads) k_rb_first(OpParams<T> op, T* __rest
   }
 }
 
+// Both colours of column (p, j) at plane k: the values (centre and z-neighbours) and keys of the
+// two columns, and the y-neighbour values and keys of each colour.
+template <typename T, typename TI>
+struct Pair {
+  T c0[3], c1[3];  // colour 0 / 1 column at planes k-1, k, k+1
+  int kc0[3], kc1[3];
+  T y0m, y0p, y1m, y1p;
+  int ky0m, ky0p, ky1m, ky1p;
+};
+
+template <typename T, typename TI>
+__device__ __forceinline__ void load_pair(const Geo& g, const TI* x, const uint8_t* key, int r0, int p, bool pok,
+                                          Pair<T, TI>& P) {
+  const int r1 = r0 + g.HP, PL = (int)g.plane, HP2 = 2 * g.HP;
+#pragma unroll
+  for (int t = 0; t < 3; ++t) {
+    P.c0[t] = P.c1[t] = T(0);
+    P.kc0[t] = P.kc1[t] = 0;
+  }
+  P.y0m = P.y0p = P.y1m = P.y1p = T(0);
+  P.ky0m = P.ky0p = P.ky1m = P.ky1p = 0;
+  if (!pok) return;
+#pragma unroll
+  for (int t = 0; t < 3; ++t) {
+    const int a0 = r0 + (t - 1) * PL + p, a1 = r1 + (t - 1) * PL + p;
+    P.c0[t] = (T)ldro(x + a0);
+    P.c1[t] = (T)ldro(x + a1);
+    P.kc0[t] = key[a0];
+    P.kc1[t] = key[a1];
+  }
+  P.y0m = (T)ldro(x + r0 + p - HP2);
+  P.y0p = (T)ldro(x + r0 + p + HP2);
+  P.y1m = (T)ldro(x + r1 + p - HP2);
+  P.y1p = (T)ldro(x + r1 + p + HP2);
+  P.ky0m = key[r0 + p - HP2];
+  P.ky0p = key[r0 + p + HP2];
+  P.ky1m = key[r1 + p - HP2];
+  P.ky1p = key[r1 + p + HP2];
+}
+
 // ------------------------------------------------------------------------------------------
 // CalcAX! (NonUniform.jl:454-511): y = A x, fused with up to two dot products
 //   d1 = sum y*u (u == nullptr: y*y),  d2 = sum y*w
-// and the stage finisher.  Grid (ceil(HI/32), ceil(2*NY/8), zc); block (32,8); rows of a block
-// interleave the two colours; each block walks planes k = 1+blockIdx.z, +gridDim.z, ...
+// and the stage finisher.  TI: type of x (the preconditioner output may be FP32 while A is
+// applied in FP64).  Grid (ceil(HN/32), ceil(NY/kBY), NZ).
 // ------------------------------------------------------------------------------------------
 template <typename T, int NDOT, typename TI = T>
 __global__ void __launch_bounds__(kThreads) k_ax(OpParams<T> op, T* __restrict__ y, const TI* __restrict__ x,
                                                   const T* __restrict__ u, const T* __restrict__ w,
                                                   SolverState* st, double* __restrict__ partials, int stage) {
+  pdl_enter();
   if (st && st->stop) return;
   const Geo& g = op.g;
-  const int p = blockIdx.x * kBX + threadIdx.x;
-  const int rr = blockIdx.y * kBY + threadIdx.y;
-  const int j = 1 + (rr >> 1), col = rr & 1;
+  const int lane = threadIdx.x, p = blockIdx.x * kBX + lane;
+  const int j = 1 + blockIdx.y * kBY + threadIdx.y;
+  const int k = 1 + blockIdx.z;
   double v[NDOT > 0 ? NDOT : 1];
 #pragma unroll
   for (int q = 0; q < (NDOT > 0 ? NDOT : 1); ++q) v[q] = 0.0;
-  const int e0 = (1 + col + j) & 1;
-  for (int k = 1 + blockIdx.z; k <= g.NZ; k += gridDim.z) {
-    const int e = e0 ^ (k & 1);
-    const int i = 2 * p + e;
-    if (j > g.NY || i < 1 || i > g.NX) continue;
-    const Nbr n = neighbours(g, p, col, j, k, e);
+  if (j <= g.NY) {  // uniform per warp
+    const bool pok = p < g.HN;
     const uint8_t* key = op.key;
-    Coef<T> c;
-    T out = T(0);
-    if (cell_coef(op, k, key[n.c], key[n.xm], key[n.xp], key[n.ym], key[n.yp], key[n.zm], key[n.zp], n.c, c))
-      out = apply_a(c, (T)x[n.c], (T)x[n.xp], (T)x[n.xm], (T)x[n.yp], (T)x[n.ym], (T)x[n.zp], (T)x[n.zm]);
-    y[n.c] = out;
-    if (NDOT >= 1) v[0] += (double)out * (u ? (double)u[n.c] : (double)out);
-    if (NDOT >= 2) v[1] += (double)out * (double)w[n.c];
+    const int r0 = g.row(0, j, k), r1 = r0 + g.HP;
+    const int e0 = (1 + j + k) & 1;
+    bool ok[2];
+    T uu[2] = {T(0), T(0)}, ww[2] = {T(0), T(0)};
+#pragma unroll
+    for (int col = 0; col < 2; ++col) {
+      const int i = 2 * p + (e0 ^ col);
+      ok[col] = pok && i >= 1 && i <= g.NX;
+      if (ok[col]) {
+        const int ci = (col ? r1 : r0) + p;
+        if (NDOT >= 1 && u) uu[col] = u[ci];
+        if (NDOT >= 2) ww[col] = w[ci];
+      }
+    }
+    Pair<T, TI> P;
+    load_pair<T, TI>(g, x, key, r0, p, pok, P);
+    T xm0, xp0, xm1, xp1;
+    int kxm0, kxp0, kxm1, kxp1;
+    // colour-0 cell: neighbours of colour 1; colour-1 cell: neighbours of colour 0
+    x_nbrs<T, true, TI>(P.c1[1], P.kc1[1], e0, lane, p, g.HN, x, key, r1, xm0, xp0, kxm0, kxp0);
+    x_nbrs<T, true, TI>(P.c0[1], P.kc0[1], e0 ^ 1, lane, p, g.HN, x, key, r0, xm1, xp1, kxm1, kxp1);
+#pragma unroll
+    for (int col = 0; col < 2; ++col) {
+      if (!ok[col]) continue;
+      const int ci = (col ? r1 : r0) + p;
+      Coef<T> c;
+      T out = T(0);
+      bool has;
+      if (col == 0)
+        has = cell_coef(op, k, (uint8_t)P.kc0[1], (uint8_t)kxm0, (uint8_t)kxp0, (uint8_t)P.ky1m, (uint8_t)P.ky1p,
+                        (uint8_t)P.kc1[0], (uint8_t)P.kc1[2], ci, c);
+      else
+        has = cell_coef(op, k, (uint8_t)P.kc1[1], (uint8_t)kxm1, (uint8_t)kxp1, (uint8_t)P.ky0m, (uint8_t)P.ky0p,
+                        (uint8_t)P.kc0[0], (uint8_t)P.kc0[2], ci, c);
+      if (has) {
+        if (col == 0) out = apply_a(c, P.c0[1], xp0, xm0, P.y1p, P.y1m, P.c1[2], P.c1[0]);
+        else out = apply_a(c, P.c1[1], xp1, xm1, P.y0p, P.y0m, P.c0[2], P.c0[0]);
+      }
+      y[ci] = out;
+      if (NDOT >= 1) v[0] += (double)out * (u ? (double)uu[col] : (double)out);
+      if (NDOT >= 2) v[NDOT - 1] += (double)out * (double)ww[col];
+    }
   }
   if constexpr (NDOT > 0) reduce_finish<NDOT>(v, partials, st, stage, 0, 0);
 }
@@ -422,30 +601,56 @@ __global__ void __launch_bounds__(kThreads) k_ax(OpParams<T> op, T* __restrict__
 // Optional copy r0 = r (PBiCGSTAB's mycopy!, NonUniform.jl:274).  th and b are FP64; r is T.
 // ------------------------------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(kThreads) k_rk(OpParams<double> op, T* __restrict__ r, T* __restrict__ r0,
+__global__ void __launch_bounds__(kThreads) k_rk(OpParams<double> op, T* __restrict__ r, T* __restrict__ r0c,
                                                   const double* __restrict__ th, const double* __restrict__ b,
                                                   SolverState* st, double* __restrict__ partials, int stage) {
+  pdl_enter();
   const Geo& g = op.g;
-  const int p = blockIdx.x * kBX + threadIdx.x;
-  const int rr = blockIdx.y * kBY + threadIdx.y;
-  const int j = 1 + (rr >> 1), col = rr & 1;
+  const int lane = threadIdx.x, p = blockIdx.x * kBX + lane;
+  const int j = 1 + blockIdx.y * kBY + threadIdx.y;
+  const int k = 1 + blockIdx.z;
   double v[1] = {0.0};
-  const int e0 = (1 + col + j) & 1;
-  for (int k = 1 + blockIdx.z; k <= g.NZ; k += gridDim.z) {
-    const int e = e0 ^ (k & 1);
-    const int i = 2 * p + e;
-    if (j > g.NY || i < 1 || i > g.NX) continue;
-    const Nbr n = neighbours(g, p, col, j, k, e);
+  if (j <= g.NY) {
+    const bool pok = p < g.HN;
     const uint8_t* key = op.key;
-    Coef<double> c;
-    double rs = 0.0;
-    if (cell_coef(op, k, key[n.c], key[n.xm], key[n.xp], key[n.ym], key[n.yp], key[n.zm], key[n.zp], n.c, c)) {
-      const double ss = nb_sum(c, th[n.xp], th[n.xm], th[n.yp], th[n.ym], th[n.zp], th[n.zm]);
-      rs = sub(b[n.c], sub(ss, mul(c.dd, th[n.c])));
+    const int r0 = g.row(0, j, k), r1 = r0 + g.HP;
+    const int e0 = (1 + j + k) & 1;
+    bool ok[2];
+    double bb[2] = {0.0, 0.0};
+#pragma unroll
+    for (int col = 0; col < 2; ++col) {
+      const int i = 2 * p + (e0 ^ col);
+      ok[col] = pok && i >= 1 && i <= g.NX;
+      if (ok[col]) bb[col] = b[(col ? r1 : r0) + p];
     }
-    r[n.c] = (T)rs;
-    if (r0) r0[n.c] = (T)rs;
-    v[0] += rs * rs;
+    Pair<double, double> P;
+    load_pair<double, double>(g, th, key, r0, p, pok, P);
+    double xm0, xp0, xm1, xp1;
+    int kxm0, kxp0, kxm1, kxp1;
+    x_nbrs<double, true>(P.c1[1], P.kc1[1], e0, lane, p, g.HN, th, key, r1, xm0, xp0, kxm0, kxp0);
+    x_nbrs<double, true>(P.c0[1], P.kc0[1], e0 ^ 1, lane, p, g.HN, th, key, r0, xm1, xp1, kxm1, kxp1);
+#pragma unroll
+    for (int col = 0; col < 2; ++col) {
+      if (!ok[col]) continue;
+      const int ci = (col ? r1 : r0) + p;
+      Coef<double> c;
+      double rs = 0.0;
+      bool has;
+      if (col == 0)
+        has = cell_coef(op, k, (uint8_t)P.kc0[1], (uint8_t)kxm0, (uint8_t)kxp0, (uint8_t)P.ky1m, (uint8_t)P.ky1p,
+                        (uint8_t)P.kc1[0], (uint8_t)P.kc1[2], ci, c);
+      else
+        has = cell_coef(op, k, (uint8_t)P.kc1[1], (uint8_t)kxm1, (uint8_t)kxp1, (uint8_t)P.ky0m, (uint8_t)P.ky0p,
+                        (uint8_t)P.kc0[0], (uint8_t)P.kc0[2], ci, c);
+      if (has) {
+        const double ss = col == 0 ? nb_sum(c, xp0, xm0, P.y1p, P.y1m, P.c1[2], P.c1[0])
+                                   : nb_sum(c, xp1, xm1, P.y0p, P.y0m, P.c0[2], P.c0[0]);
+        rs = sub(bb[col], sub(ss, mul(c.dd, col == 0 ? P.c0[1] : P.c1[1])));
+      }
+      r[ci] = (T)rs;
+      if (r0c) r0c[ci] = (T)rs;
+      v[0] += rs * rs;
+    }
   }
   reduce_finish<1>(v, partials, st, stage, 0, 0);
 }
@@ -509,6 +714,7 @@ __global__ void __launch_bounds__(256) k_bicg_update(long long n, TX* __restrict
                                                       const T* __restrict__ r0, SolverState* st,
                                                       double* __restrict__ partials, cudaGraphConditionalHandle hc,
                                                       int use_cond) {
+  pdl_enter();
   // Fail-safe loop bound: block 0 counts the pass and ends the loop provisionally; only the
   // finisher of this kernel (which runs after block 0 has arrived) can continue it.
   if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -545,6 +751,7 @@ template <typename T, typename TX>
 __global__ void __launch_bounds__(256) k_cg_update(long long n, TX* __restrict__ x, const T* __restrict__ p,
                                                     T* __restrict__ r, const T* __restrict__ q, SolverState* st,
                                                     double* __restrict__ partials) {
+  pdl_enter();
   if (st->stop) return;
   constexpr int V = Vec16<T>::n;
   const T alpha = (T)st->alpha;
@@ -572,6 +779,7 @@ template <typename T, typename T2 = T>
 __global__ void __launch_bounds__(256) k_dot(long long n, const T* __restrict__ a, const T2* __restrict__ b,
                                               T* __restrict__ dst, SolverState* st, double* __restrict__ partials,
                                               int stage) {
+  pdl_enter();
   if (st->stop) return;
   constexpr int V = Vec16<T>::n;
   double v[1] = {0.0};
@@ -592,6 +800,7 @@ __global__ void __launch_bounds__(256) k_dot(long long n, const T* __restrict__ 
 template <typename T, typename TP = T>
 __global__ void __launch_bounds__(256) k_cg_pupd(long long n, T* __restrict__ p, const TP* __restrict__ z,
                                                   SolverState* st, cudaGraphConditionalHandle hc, int use_cond) {
+  pdl_enter();
   const int stop = st->stop;
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     st->passes += 1;
@@ -618,6 +827,7 @@ __global__ void __launch_bounds__(256) k_ir_prep(long long n, const double* __re
                                                   float* __restrict__ r0, float* __restrict__ e,
                                                   const SolverState* __restrict__ outer, SolverState* inner,
                                                   double* __restrict__ partials, int stage) {
+  pdl_enter();
   const double inv = 1.0 / outer->scale;
   double v[1] = {0.0};
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
@@ -632,6 +842,7 @@ __global__ void __launch_bounds__(256) k_ir_prep(long long n, const double* __re
 
 // Host-controlled fields of a state: tolerance, iteration cap and residual history.
 __global__ void k_prime(SolverState* st, double tol, int maxItr, double* hist, int hist_len) {
+  pdl_enter();
   st->tol = tol;
   st->maxItr = maxItr;
   st->hist = hist;
@@ -644,6 +855,7 @@ __global__ void k_prime(SolverState* st, double tol, int maxItr, double* hist, i
 // Iterative refinement: th += ||r64|| * e (FP64 accumulation of the FP32 correction).
 __global__ void __launch_bounds__(256) k_ir_apply(long long n, double* __restrict__ th, const float* __restrict__ e,
                                                    const SolverState* __restrict__ outer) {
+  pdl_enter();
   const double sc = outer->scale;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     th[i] += sc * (double)e[i];

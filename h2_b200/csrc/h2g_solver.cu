@@ -16,6 +16,7 @@
 #include <cstring>
 #include <mutex>
 #include <type_traits>
+#include <utility>
 #include <string>
 #include <vector>
 
@@ -109,6 +110,7 @@ struct Solver {
   double* r64 = nullptr;
   // Krylov vectors in working precision: r, r0, p, ph, q, s, sh, t (+ e for refinement)
   void* kv[10] = {nullptr};
+  void* hook[2] = {nullptr, nullptr};  // scratch of the single-kernel entry points (never a Krylov vector)
   size_t elem = 8;
   // column-major staging buffers (MX*MY*MZ doubles each)
   double* stage[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -125,6 +127,7 @@ struct Solver {
   double inner_tol = 1e-4;
   int max_outer = 40;
   bool no_cond = false;
+  bool pdl = true;  // programmatic dependent launch of the solver kernels
 
   long long nfort() const { return (long long)g.MX * g.MY * g.MZ; }
 };
@@ -139,16 +142,31 @@ namespace h2g {
 // ------------------------------------------------------------------------------------------
 // helpers
 // ------------------------------------------------------------------------------------------
+// Kernel launch with programmatic stream serialization: inside the captured iteration graph the
+// edges become programmatic, so each kernel's launch overlaps the tail of the one before it
+// (the kernels wait for their predecessor with griddepcontrol.wait).
+template <typename... KArgs, typename... Args>
+static void launch(const Solver* s, void (*kern)(KArgs...), dim3 grid, dim3 block, cudaStream_t stream,
+                   Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = s->pdl ? 1 : 0;
+  cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
+}
 static int elementwise_blocks(const Solver* s) { return s->num_sms * 4; }
 
-static dim3 rb_grid(const Geo& g) { return dim3((g.HI + kBX - 1) / kBX, (g.NY + kBY - 1) / kBY, g.NZ); }
-
-static dim3 ax_grid(const Geo& g) {
-  const int xt = (g.HI + kBX - 1) / kBX, yt = (2 * g.NY + kBY - 1) / kBY;
-  int zc = (2048 + xt * yt - 1) / (xt * yt);
-  zc = std::max(1, std::min(zc, g.NZ));
-  return dim3(xt, yt, zc);
-}
+// Grids of the stencil kernels: columns (p, j) in 32 x kBY blocks; the RB passes take two planes
+// per thread, CalcAX / CalcRK / the first pass one plane (both colours).
+static dim3 rb_grid(const Geo& g) { return dim3((g.HN + kBX - 1) / kBX, (g.NY + kBY - 1) / kBY, (g.NZ + 1) / 2); }
+static dim3 ax_grid(const Geo& g) { return dim3((g.HN + kBX - 1) / kBX, (g.NY + kBY - 1) / kBY, g.NZ); }
+static dim3 first_grid(const Geo& g) { return ax_grid(g); }
 
 static size_t partials_needed(const Solver* s) {
   dim3 a = ax_grid(s->g);
@@ -224,6 +242,7 @@ static void destroy(Solver* s) {
   cudaFree(s->rc64); cudaFree(s->rc32);
   cudaFree(s->th); cudaFree(s->b); cudaFree(s->th_snap); cudaFree(s->r64);
   for (auto& p : s->kv) cudaFree(p);
+  for (auto& p : s->hook) cudaFree(p);
   for (auto& p : s->stage) cudaFree(p);
   cudaFree(s->st); cudaFree(s->st_in); cudaFree(s->partials); cudaFree(s->hist);
   if (s->st_host) cudaFreeHost(s->st_host);
@@ -282,21 +301,23 @@ static int build_tables(Solver* s) {
       const double la = s->lam_values[a], lb = s->lam_values[b];
       LP[(size_t)a * pc + b] = 2.0 * la * lb / (la + lb);  // lambda_f without the mask factor, common.jl:35
     }
-  const size_t lvl = (size_t)2 * pc * pc;
+  // tables [k][a0][neighbour key byte]: bit 7 of the neighbour key is its mask; a masked
+  // neighbour doubles lambda_f (2 - div(ma+mb, 2) = 2), an unmasked one keeps it (= 1)
+  const size_t lvl = (size_t)pc * 256;
   std::vector<double> tx(lvl * g.MZ, 0.0), ty(lvl * g.MZ, 0.0), tz(lvl * g.MZ, 0.0), conv(4 * (size_t)g.MZ, 0.0);
   for (int k = 0; k < g.MZ; ++k) {
     const double dz_k = s->dZ[k];
-    for (int f = 0; f < 2; ++f) {
-      const double fac = f == 0 ? 1.0 : 2.0;  // 2 - div(ma+mb, 2)
-      for (int a = 0; a < P; ++a)
-        for (int b = 0; b < P; ++b) {
-          const double lf = LP[(size_t)a * pc + b] * fac;
-          const size_t o = (size_t)k * lvl + (size_t)f * pc * pc + (size_t)a * pc + b;
-          tx[o] = lf * dy0 * dz_k * ddx;  // NonUniform.jl:482-483
-          ty[o] = lf * dx0 * dz_k * ddy;  // NonUniform.jl:484-485
-          if (k >= 1) tz[o] = lf * dx0 * dy0 / (s->ZC[k] - s->ZC[k - 1]);  // NonUniform.jl:486
-        }
-    }
+    for (int a = 0; a < P; ++a)
+      for (int kn = 0; kn < 256; ++kn) {
+        const int b = kn & 0x7f;
+        if (b >= P) continue;
+        const double fac = (kn & 0x80) ? 1.0 : 2.0;
+        const double lf = LP[(size_t)a * pc + b] * fac;
+        const size_t o = (size_t)k * lvl + (size_t)a * 256 + kn;
+        tx[o] = lf * dy0 * dz_k * ddx;  // NonUniform.jl:482-483
+        ty[o] = lf * dx0 * dz_k * ddy;  // NonUniform.jl:484-485
+        if (k >= 1) tz[o] = lf * dx0 * dy0 / (s->ZC[k] - s->ZC[k - 1]);  // NonUniform.jl:486
+      }
     conv[4 * k + 0] = s->HC[0] * dy0 * dz_k;  // NonUniform.jl:490-493
     conv[4 * k + 1] = s->HC[1] * dy0 * dz_k;
     conv[4 * k + 2] = s->HC[2] * dx0 * dz_k;
@@ -368,21 +389,21 @@ static void launch_pbicg_body(Solver* s, cudaStream_t cs, const OpParams<T>& opA
   const dim3 rg = rb_grid(g), ag = ax_grid(g), blk(kBX, kBY);
   const int none = smoother == H2G_SMOOTHER_NONE;
   // p = r + beta (p - omega q); p_ = M^-1 p                     NonUniform.jl:296-305
-  k_rb_first<TP, T, 1><<<rg, blk, 0, cs>>>(opM, ph, p, bbm, r, q, st, none);
+  launch(s, k_rb_first<TP, T, 1>, first_grid(g), blk, cs, opM, ph, p, bbm, r, q, st, none);
   if (!none)
     for (int pass = 1; pass < 2 * kSweeps; ++pass)
-      k_rb_pass<TP><<<rg, blk, 0, cs>>>(opM, ph, bbm ? bbm : reinterpret_cast<TP*>(p), pass & 1, TP(1), st);
+      launch(s, k_rb_pass<TP>, rg, blk, cs, opM, ph, bbm ? bbm : reinterpret_cast<TP*>(p), pass & 1, TP(1), st);
   // q = A p_;  alpha = rho / (q, r0)                            NonUniform.jl:307-309
-  k_ax<T, 1, TP><<<ag, blk, 0, cs>>>(opA, q, ph, r0, nullptr, st, s->partials, kStageAlpha);
+  launch(s, k_ax<T, 1, TP>, ag, blk, cs, opA, q, ph, r0, nullptr, st, s->partials, kStageAlpha);
   // s = r - alpha q; s_ = M^-1 s                                NonUniform.jl:310-315
-  k_rb_first<TP, T, 2><<<rg, blk, 0, cs>>>(opM, sh, sv, bbm, r, q, st, none);
+  launch(s, k_rb_first<TP, T, 2>, first_grid(g), blk, cs, opM, sh, sv, bbm, r, q, st, none);
   if (!none)
     for (int pass = 1; pass < 2 * kSweeps; ++pass)
-      k_rb_pass<TP><<<rg, blk, 0, cs>>>(opM, sh, bbm ? bbm : reinterpret_cast<TP*>(sv), pass & 1, TP(1), st);
+      launch(s, k_rb_pass<TP>, rg, blk, cs, opM, sh, bbm ? bbm : reinterpret_cast<TP*>(sv), pass & 1, TP(1), st);
   // t = A s_; omega = (t,s)/(t,t)                               NonUniform.jl:317-326
-  k_ax<T, 2, TP><<<ag, blk, 0, cs>>>(opA, t, sh, nullptr, sv, st, s->partials, kStageOmega);
+  launch(s, k_ax<T, 2, TP>, ag, blk, cs, opA, t, sh, nullptr, sv, st, s->partials, kStageOmega);
   // x += alpha p_ + omega s_; r = s - omega t; res; next rho    NonUniform.jl:328-346
-  k_bicg_update<T, TX, TP><<<elementwise_blocks(s), 256, 0, cs>>>(g.n, x, ph, sh, r, sv, t, r0, st, s->partials, hc,
+  launch(s, k_bicg_update<T, TX, TP>, elementwise_blocks(s), 256, cs, g.n, x, ph, sh, r, sv, t, r0, st, s->partials, hc,
                                                                   use_cond);
 }
 
@@ -394,10 +415,10 @@ static void launch_precond_r(Solver* s, cudaStream_t cs, const OpParams<TP>& opM
   const dim3 rg = rb_grid(g), blk(kBX, kBY);
   const int none = smoother == H2G_SMOOTHER_NONE;
   TP* bbm = std::is_same<T, TP>::value ? nullptr : kvec<TP>(s, KBB);
-  k_rb_first<TP, T, 0><<<rg, blk, 0, cs>>>(opM, z, r, bbm, nullptr, nullptr, st, none);
+  launch(s, k_rb_first<TP, T, 0>, first_grid(g), blk, cs, opM, z, r, bbm, nullptr, nullptr, st, none);
   if (!none)
     for (int pass = 1; pass < 2 * kSweeps; ++pass)
-      k_rb_pass<TP><<<rg, blk, 0, cs>>>(opM, z, bbm ? bbm : reinterpret_cast<TP*>(r), pass & 1, TP(1), st);
+      launch(s, k_rb_pass<TP>, rg, blk, cs, opM, z, bbm ? bbm : reinterpret_cast<TP*>(r), pass & 1, TP(1), st);
 }
 
 template <typename T, typename TX, typename TP>
@@ -407,19 +428,19 @@ static void launch_cg_body(Solver* s, cudaStream_t cs, const OpParams<T>& opA, c
   T* r = kvec<T>(s, KR);
   T* p = kvec<T>(s, KP);
   T* q = kvec<T>(s, KQ);
-  TP* z = kvec<TP>(s, KS);  // pcg_s holds z (NonUniform.jl:146)
+  TP* z = kvec<TP>(s, KPH);  // z (pcg_s in NonUniform.jl:146) in the preconditioner-output buffer
   const dim3 ag = ax_grid(g), blk(kBX, kBY);
   const int nb = elementwise_blocks(s);
   // q = A p; alpha = rho_old / (p,q)                             NonUniform.jl:164-176
-  k_ax<T, 1, T><<<ag, blk, 0, cs>>>(opA, q, p, p, nullptr, st, s->partials, kStageCgAlpha);
+  launch(s, k_ax<T, 1, T>, ag, blk, cs, opA, q, p, p, nullptr, st, s->partials, kStageCgAlpha);
   // x += alpha p; r -= alpha q; res                              NonUniform.jl:179-198
-  k_cg_update<T, TX><<<nb, 256, 0, cs>>>(g.n, x, p, r, q, st, s->partials);
+  launch(s, k_cg_update<T, TX>, nb, 256, cs, g.n, x, p, r, q, st, s->partials);
   // z = M^-1 r                                                  NonUniform.jl:201-203
   launch_precond_r<T, TP>(s, cs, opM, z, r, st, smoother);
   // rho_new = (r,z); beta                                       NonUniform.jl:206-215
-  k_dot<T, TP><<<nb, 256, 0, cs>>>(g.n, r, z, nullptr, st, s->partials, kStageCgBeta);
+  launch(s, k_dot<T, TP>, nb, 256, cs, g.n, r, z, nullptr, st, s->partials, kStageCgBeta);
   // p = z + beta p                                              NonUniform.jl:218-220
-  k_cg_pupd<T, TP><<<nb, 256, 0, cs>>>(g.n, p, z, st, hc, use_cond);
+  launch(s, k_cg_pupd<T, TP>, nb, 256, cs, g.n, p, z, st, hc, use_cond);
 }
 
 template <typename T, typename TP>
@@ -518,7 +539,7 @@ static int run_graph(Solver* s, SolveGraph* G, SolverState* st, int maxItr) {
 
 // Set the host-controlled fields of a device state (tolerance, iteration cap, history).
 static int prime_state(Solver* s, SolverState* st, double tol, int maxItr, double* hist, int hist_len) {
-  k_prime<<<1, 1, 0, s->stream>>>(st, tol, maxItr, hist, hist_len);
+  launch(s, k_prime, 1, 1, s->stream, st, tol, maxItr, hist, hist_len);
   CKL();
   return H2G_OK;
 }
@@ -597,14 +618,14 @@ static int solve_krylov(Solver* s, bool cg, double tol, int maxItr, int smoother
   double* r = kvec<double>(s, KR);
   const dim3 ag = ax_grid(g), blk(kBX, kBY);
   // r = b - A theta, res0 (and r0 = r for PBiCGSTAB)            NonUniform.jl:131-141, 262-274
-  k_rk<double><<<ag, blk, 0, s->stream>>>(op, r, cg ? nullptr : kvec<double>(s, KR0), s->th, s->b, st, s->partials,
+  launch(s, k_rk<double>, ag, blk, s->stream, op, r, cg ? nullptr : kvec<double>(s, KR0), s->th, s->b, st, s->partials,
                                           cg ? kStageInitCg : kStageInit);
   CKL();
   if (cg) {
     // z = M^-1 r; p = z; rho_old = (r,z)                          NonUniform.jl:147-155
-    TP* z = kvec<TP>(s, KS);
+    TP* z = kvec<TP>(s, KPH);
     launch_precond_r<double, TP>(s, s->stream, opM, z, r, st, smoother);
-    k_dot<double, TP><<<elementwise_blocks(s), 256, 0, s->stream>>>(g.n, r, z, kvec<double>(s, KP), st, s->partials,
+    launch(s, k_dot<double, TP>, elementwise_blocks(s), 256, s->stream, g.n, r, z, kvec<double>(s, KP), st, s->partials,
                                                                      kStageCgInit);
     CKL();
   }
@@ -657,7 +678,7 @@ static int solve_ir(Solver* s, bool cg, double tol, int maxItr, int smoother, in
   const int nb = elementwise_blocks(s);
   if ((rc = prime_state(s, st, tol, maxItr, nullptr, 0))) return rc;
   // true residual r64 = b - A theta, ||r64||
-  k_rk<double><<<ag, blk, 0, s->stream>>>(op64, s->r64, nullptr, s->th, s->b, st, s->partials, kStageResid);
+  launch(s, k_rk<double>, ag, blk, s->stream, op64, s->r64, nullptr, s->th, s->b, st, s->partials, kStageResid);
   CKL();
   CK(cudaMemcpyAsync(s->st_host, st, sizeof(SolverState), cudaMemcpyDeviceToHost, s->stream));
   CK(cudaStreamSynchronize(s->stream));
@@ -681,13 +702,13 @@ static int solve_ir(Solver* s, bool cg, double tol, int maxItr, int smoother, in
       const int cap = maxItr - total;
       if ((rc = prime_state(s, si, s->inner_tol, cap, s->hist, cap))) return rc;
       // inner right-hand side r = r64/||r64||, e = 0, inner res0 and rho
-      k_ir_prep<<<nb, 256, 0, s->stream>>>(g.n, s->r64, kvec<float>(s, KR), kvec<float>(s, KR0), e, st, si,
+      launch(s, k_ir_prep, nb, 256, s->stream, g.n, s->r64, kvec<float>(s, KR), kvec<float>(s, KR0), e, st, si,
                                            s->partials, cg ? kStageInitCg : kStageInit);
       CKL();
       if (cg) {
-        float* z = kvec<float>(s, KS);
+        float* z = kvec<float>(s, KPH);
         launch_precond_r<float, float>(s, s->stream, op32, z, kvec<float>(s, KR), si, smoother);
-        k_dot<float><<<nb, 256, 0, s->stream>>>(g.n, kvec<float>(s, KR), z, kvec<float>(s, KP), si, s->partials,
+        launch(s, k_dot<float>, nb, 256, s->stream, g.n, kvec<float>(s, KR), z, kvec<float>(s, KP), si, s->partials,
                                                  kStageCgInit);
         CKL();
       }
@@ -695,8 +716,8 @@ static int solve_ir(Solver* s, bool cg, double tol, int maxItr, int smoother, in
         return rc;
       if ((rc = run_graph(s, G, si, cap))) return rc;
       // theta += ||r64|| e ; r64 = b - A theta
-      k_ir_apply<<<nb, 256, 0, s->stream>>>(g.n, s->th, e, st);
-      k_rk<double><<<ag, blk, 0, s->stream>>>(op64, s->r64, nullptr, s->th, s->b, st, s->partials, kStageResid);
+      launch(s, k_ir_apply, nb, 256, s->stream, g.n, s->th, e, st);
+      launch(s, k_rk<double>, ag, blk, s->stream, op64, s->r64, nullptr, s->th, s->b, st, s->partials, kStageResid);
       CKL();
       SolverState inner;
       CK(cudaMemcpyAsync(s->st_host, si, sizeof(SolverState), cudaMemcpyDeviceToHost, s->stream));
@@ -745,6 +766,62 @@ static int solve_ir(Solver* s, bool cg, double tol, int maxItr, int smoother, in
   return status;
 }
 
+// ||b - A theta|| in FP64 on the device (into the r vector, which every solve recomputes).
+static int true_residual(Solver* s, double* res) {
+  OpParams<double> op = op_params<double>(s, s->t64);
+  int rc;
+  if ((rc = prime_state(s, s->st, 0.0, 1, nullptr, 0))) return rc;
+  launch(s, k_rk<double>, ax_grid(s->g), dim3(kBX, kBY), s->stream, op, kvec<double>(s, KR), (double*)nullptr, s->th,
+         s->b, s->st, s->partials, (int)kStageResid);
+  CKL();
+  CK(cudaMemcpyAsync(s->st_host, s->st, sizeof(SolverState), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  *res = s->st_host->scale;
+  return H2G_OK;
+}
+
+// H2G_MIXED: FP64 Krylov with the FP32 preconditioner.  The preconditioner's rounding makes the
+// recursively updated residual drift from the true one, so convergence is confirmed with the
+// FP64 true residual and the solve restarts from the current theta until the true residual
+// meets the tolerance.
+static int solve_mixed(Solver* s, bool cg, double tol, int maxItr, int smoother, int verbose, double* res_hist,
+                       h2g_result* out) {
+  int total = 0, status = H2G_NOT_CONVERGED, converged = 0, passes = 0;
+  long long launches = 0;
+  double res0 = 0.0, res = 1.0, tol_cur = tol;
+  for (int restart = 0; restart < 16 && total < maxItr; ++restart) {
+    h2g_result r;
+    memset(&r, 0, sizeof r);
+    const int st = solve_krylov<float>(s, cg, tol_cur, maxItr - total, smoother, verbose && restart == 0,
+                                       res_hist ? res_hist + total : nullptr, &r);
+    if (st == H2G_BAD_ARG || st == H2G_CUDA_ERROR) return st;
+    ++passes;
+    launches += r.launches + 2;
+    total += r.itr;
+    if (restart == 0) res0 = r.res0;
+    if (res0 == 0.0) { status = H2G_OK; converged = 1; res = 0.0; break; }
+    double tr;
+    int rc;
+    if ((rc = true_residual(s, &tr))) return rc;
+    res = tr / res0;
+    if (!std::isfinite(res)) { status = H2G_NONFINITE; break; }
+    if (res < tol) { status = H2G_OK; converged = 1; break; }
+    if (st != H2G_OK && st != H2G_NOT_CONVERGED) { status = st; break; }
+    if (r.itr == 0) break;
+    tol_cur = tol / res;  // relative to the restart's initial residual
+  }
+  if (out) {
+    out->isconverged = converged;
+    out->itr = total;
+    out->outer = passes;
+    out->status = status;
+    out->res0 = res0;
+    out->res = res;
+    out->launches = launches;
+  }
+  return status;
+}
+
 static int solve(Solver* s, bool cg, double tol, int maxItr, int smoother, int verbose, double* res_hist,
                  h2g_result* out) {
   if (!s->grid_set || !s->fields_set) return fail(H2G_BAD_ARG, "h2g_set_grid and h2g_set_fields must come first");
@@ -754,7 +831,7 @@ static int solve(Solver* s, bool cg, double tol, int maxItr, int smoother, int v
   if (!(tol >= 0.0) || !std::isfinite(tol)) return fail(H2G_BAD_ARG, "bad tolerance");
   CK(cudaSetDevice(s->device));
   if (s->precision == H2G_MIXED_IR) return solve_ir(s, cg, tol, maxItr, smoother, verbose, res_hist, out);
-  if (s->precision == H2G_MIXED) return solve_krylov<float>(s, cg, tol, maxItr, smoother, verbose, res_hist, out);
+  if (s->precision == H2G_MIXED) return solve_mixed(s, cg, tol, maxItr, smoother, verbose, res_hist, out);
   return solve_krylov<double>(s, cg, tol, maxItr, smoother, verbose, res_hist, out);
 }
 
@@ -766,6 +843,7 @@ static int create(int MX, int MY, int MZ, int precision, Solver** out) {
   *out = nullptr;
   if (MX < 3 || MY < 3 || MZ < 3) return fail(H2G_BAD_ARG, "grid too small: (%d,%d,%d)", MX, MY, MZ);
   if ((long long)MX * MY * MZ > (1ll << 31)) return fail(H2G_BAD_ARG, "grid too large");
+  if (make_geo(MX, MY, MZ).n >= (1ll << 31) - 1) return fail(H2G_BAD_ARG, "grid too large for 32-bit offsets");
   if (precision != H2G_FP64 && precision != H2G_MIXED && precision != H2G_MIXED_IR)
     return fail(H2G_BAD_ARG, "unknown precision %d", precision);
   Solver* s = new h2g_solver();
@@ -774,6 +852,8 @@ static int create(int MX, int MY, int MZ, int precision, Solver** out) {
   s->elem = precision == H2G_MIXED_IR ? 4 : 8;
   const char* nc = getenv("H2G_NO_COND");
   s->no_cond = nc && nc[0] == '1';
+  const char* np = getenv("H2G_NO_PDL");
+  s->pdl = !(np && np[0] == '1');
   int rc = H2G_OK;
   auto bail = [&](int code) {
     destroy(s);
@@ -920,14 +1000,30 @@ using h2g::fail;
 static Solver* S(h2g_solver* h) { return static_cast<Solver*>(h); }
 
 // ---- single-kernel helpers ---------------------------------------------------------------
+// The single-kernel entry points use their own two buffers, cleared before every call, so the
+// guard and padding entries they rely on are zero whatever precision used them last, and the
+// Krylov vectors of the solvers are never touched.
+static int hook_buffers(Solver* s, void** a, void** b) {
+  const size_t bytes = sizeof(double) * (size_t)s->g.n;
+  for (auto& p : s->hook)
+    if (!p) CK(cudaMalloc(&p, bytes));
+  CK(cudaMemsetAsync(s->hook[0], 0, bytes, s->stream));
+  CK(cudaMemsetAsync(s->hook[1], 0, bytes, s->stream));
+  *a = s->hook[0];
+  *b = s->hook[1];
+  return H2G_OK;
+}
+
 template <typename T>
 static int calcax_t(Solver* s, const double* x, double* ax, const h2g::OpParams<T>& op) {
   using namespace h2g;
-  T* xd = kvec<T>(s, KPH);
-  T* yd = kvec<T>(s, KQ);
+  void *ha, *hb;
   int rc;
+  if ((rc = hook_buffers(s, &ha, &hb))) return rc;
+  T* xd = static_cast<T*>(ha);
+  T* yd = static_cast<T*>(hb);
   if ((rc = upload<T>(s, x, xd))) return rc;
-  k_ax<T, 0><<<ax_grid(s->g), dim3(kBX, kBY), 0, s->stream>>>(op, yd, xd, nullptr, nullptr, nullptr, nullptr, 0);
+  launch(s, k_ax<T, 0>, ax_grid(s->g), dim3(kBX, kBY), s->stream, op, yd, xd, nullptr, nullptr, nullptr, nullptr, 0);
   CKL();
   return download<T>(s, yd, ax);
 }
@@ -935,12 +1031,14 @@ static int calcax_t(Solver* s, const double* x, double* ax, const h2g::OpParams<
 template <typename T>
 static int rbsor_t(Solver* s, double* x, const double* b, int color, double omega, const h2g::OpParams<T>& op) {
   using namespace h2g;
-  T* xd = kvec<T>(s, KPH);
-  T* bd = kvec<T>(s, KP);
+  void *ha, *hb;
   int rc;
+  if ((rc = hook_buffers(s, &ha, &hb))) return rc;
+  T* xd = static_cast<T*>(ha);
+  T* bd = static_cast<T*>(hb);
   if ((rc = upload<T>(s, x, xd, 0))) return rc;
   if ((rc = upload<T>(s, b, bd, 1))) return rc;
-  k_rb_pass<T><<<rb_grid(s->g), dim3(kBX, kBY), 0, s->stream>>>(op, xd, bd, color, (T)omega, nullptr);
+  launch(s, k_rb_pass<T>, rb_grid(s->g), dim3(kBX, kBY), s->stream, op, xd, bd, color, (T)omega, nullptr);
   CKL();
   return download<T>(s, xd, x);
 }
@@ -948,15 +1046,17 @@ static int rbsor_t(Solver* s, double* x, const double* b, int color, double omeg
 template <typename T>
 static int precond_t(Solver* s, const double* bb, double* xx, int smoother, const h2g::OpParams<T>& op) {
   using namespace h2g;
-  T* xd = kvec<T>(s, KPH);
-  T* bd = kvec<T>(s, KP);
+  void *ha, *hb;
   int rc;
+  if ((rc = hook_buffers(s, &ha, &hb))) return rc;
+  T* xd = static_cast<T*>(ha);
+  T* bd = static_cast<T*>(hb);
   if ((rc = upload<T>(s, bb, bd, 1))) return rc;
   const dim3 rg = rb_grid(s->g), blk(kBX, kBY);
   const int none = smoother == H2G_SMOOTHER_NONE;
-  k_rb_first<T, T, 0><<<rg, blk, 0, s->stream>>>(op, xd, bd, nullptr, nullptr, nullptr, nullptr, none);
+  launch(s, k_rb_first<T, T, 0>, first_grid(s->g), blk, s->stream, op, xd, bd, nullptr, nullptr, nullptr, nullptr, none);
   if (!none)
-    for (int pass = 1; pass < 2 * kSweeps; ++pass) k_rb_pass<T><<<rg, blk, 0, s->stream>>>(op, xd, bd, pass & 1, T(1), nullptr);
+    for (int pass = 1; pass < 2 * kSweeps; ++pass) launch(s, k_rb_pass<T>, rg, blk, s->stream, op, xd, bd, pass & 1, T(1), nullptr);
   CKL();
   return download<T>(s, xd, xx);
 }
@@ -964,15 +1064,24 @@ static int precond_t(Solver* s, const double* bb, double* xx, int smoother, cons
 template <typename T>
 static int bench_t(Solver* s, int kind, int reps, int* launches, const h2g::OpParams<T>& op) {
   using namespace h2g;
+  // the hook buffers (zeroed when allocated; values are irrelevant for timing)
+  const size_t bytes = sizeof(double) * (size_t)s->g.n;
+  for (auto& p : s->hook)
+    if (!p) {
+      CK(cudaMalloc(&p, bytes));
+      CK(cudaMemset(p, 0, bytes));
+    }
+  T* xa = static_cast<T*>(s->hook[0]);
+  T* xb = static_cast<T*>(s->hook[1]);
   const dim3 rg = rb_grid(s->g), ag = ax_grid(s->g), blk(kBX, kBY);
   int n = 0;
   for (int r = 0; r < reps; ++r) {
     if (kind == 0) {
-      k_rb_pass<T><<<rg, blk, 0, s->stream>>>(op, kvec<T>(s, KPH), kvec<T>(s, KP), 0, T(1), nullptr);
-      k_rb_pass<T><<<rg, blk, 0, s->stream>>>(op, kvec<T>(s, KPH), kvec<T>(s, KP), 1, T(1), nullptr);
+      launch(s, k_rb_pass<T>, rg, blk, s->stream, op, xa, xb, 0, T(1), nullptr);
+      launch(s, k_rb_pass<T>, rg, blk, s->stream, op, xa, xb, 1, T(1), nullptr);
       n += 2;
     } else {
-      k_ax<T, 0><<<ag, blk, 0, s->stream>>>(op, kvec<T>(s, KQ), kvec<T>(s, KPH), nullptr, nullptr, nullptr, nullptr, 0);
+      launch(s, k_ax<T, 0>, ag, blk, s->stream, op, xb, xa, nullptr, nullptr, nullptr, nullptr, 0);
       n += 1;
     }
   }
@@ -1161,7 +1270,7 @@ int h2g_calcrk(h2g_solver* h, double* r, double* res) {
   double* rd = s->precision == H2G_MIXED_IR ? s->r64 : kvec<double>(s, KR);
   int rc;
   if ((rc = prime_state(s, s->st, 0.0, 1, nullptr, 0))) return rc;
-  k_rk<double><<<ax_grid(s->g), dim3(kBX, kBY), 0, s->stream>>>(op, rd, nullptr, s->th, s->b, s->st, s->partials,
+  launch(s, k_rk<double>, ax_grid(s->g), dim3(kBX, kBY), s->stream, op, rd, nullptr, s->th, s->b, s->st, s->partials,
                                                                    kStageResid);
   CKL();
   CK(cudaMemcpyAsync(s->st_host, s->st, sizeof(SolverState), cudaMemcpyDeviceToHost, s->stream));

@@ -40,7 +40,8 @@ extern "C" {
 /* ---- precision ---------------------------------------------------------------------- */
 #define H2G_FP64 0     /* FP64 throughout, same arithmetic as the reference */
 #define H2G_MIXED 1    /* FP32 RB-GS preconditioner (operator tables, smoother vectors) inside FP64
-                          PBiCGSTAB/CG: FP64 Krylov vectors, inner products, CalcAX and solution */
+                          PBiCGSTAB/CG: FP64 Krylov vectors, inner products, CalcAX and solution;
+                          convergence is confirmed on the FP64 true residual (restarts if needed) */
 #define H2G_MIXED_IR 2 /* FP32 operator, smoother and Krylov vectors inside FP64 iterative
                           refinement (FP64 true residual, solution accumulation, inner products);
                           its FP32 BiCGSTAB can diverge on fine grids (reported as H2G_NONFINITE) */
@@ -69,7 +70,7 @@ typedef struct h2g_bc {
 typedef struct h2g_result {
   int isconverged; /* 1 if ||r_k|| / ||r_0|| < tol */
   int itr;         /* PBiCGSTAB/CG iterations (all inner iterations for H2G_MIXED_IR) */
-  int outer;       /* iterative-refinement passes (H2G_MIXED_IR), 0 otherwise */
+  int outer;       /* refinement passes (H2G_MIXED_IR) or true-residual restarts (H2G_MIXED) */
   int status;      /* same value the call returns */
   double res0;     /* initial residual ||b - A theta||_2 (NonUniform.jl:263) */
   double res;      /* final relative residual ||r|| / res0 */
