@@ -74,6 +74,8 @@ _SIGS = {
     "h2g_rbsor_pass": (C.c_int, [_vp, _dp, _dp, C.c_int, C.c_double]),
     "h2g_preconditioner": (C.c_int, [_vp, _dp, _dp, C.c_int]),
     "h2g_bench_kernel": (C.c_int, [_vp, C.c_int, C.c_int, _ip]),
+    "h2g_calcrk_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                                     C.c_double, C.c_double, C.c_double, _dp, C.c_int, _vp, _dp, _vp]),
     "h2g_model_zgrid": (C.c_int, [C.c_int, _dp, _dp, _dp]),
     "h2g_model_pitch": (C.c_double, [C.c_int]),
     "h2g_model_fill_id": (C.c_int, [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_uint8)]),

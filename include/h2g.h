@@ -156,6 +156,25 @@ int h2g_preconditioner(h2g_solver *h, const double *bb, double *xx, int smoother
  * preconditioner, kind 1 = CalcAX.  Returns the number of kernel launches issued in *launches. */
 int h2g_bench_kernel(h2g_solver *h, int kind, int reps, int *launches);
 
+/* ---- CalcRK! without device allocation -------------------------------------------------
+ * No counterpart in the reference.  For callers that cannot allocate device memory: the device
+ * memory belongs to someone else (a Julia program's CUDA.jl pool, a framework's caching
+ * allocator), or the caller runs a time-stepping loop that must not stall on cudaMalloc/cudaFree,
+ * or it is between steps of a CUDA stream capture, where cudaFree is not allowed.  Computes
+ * r = b - A theta over the interior and *res = ||r||_2 exactly as h2g_calcrk, from the
+ * reference's column-major arrays already in device memory (theta, b, lambda, mask, rho, cp: MX*MY*MZ
+ * doubles; ZC, dZ: MZ doubles; rho and cp may be NULL when is_steady) and HC[6] on the host;
+ * r (device, MX*MY*MZ) gets the interior, guard cells are left untouched.  Nothing is allocated:
+ * the reduction uses a 512 KiB device array inside the library that every GPU loading it keeps
+ * until exit, so grids with more than 65536 interior rows (NY*NZ) are rejected (H2G_BAD_ARG).
+ * Calls share that array: calls that overlap on the GPU race and must be serialised.  The first
+ * call on a device looks up the array's address; make it before any stream capture.  stream may
+ * be NULL (legacy default stream); the call returns after *res is on the host. */
+int h2g_calcrk_noalloc(int MX, int MY, int MZ, const double *theta, const double *b, const double *lambda,
+                       const double *mask, const double *rho, const double *cp, const double *ZC, const double *dZ,
+                       double dx, double dy, double dt, const double *HC, int is_steady, double *r, double *res,
+                       void *stream);
+
 /* ---- the reference's problem set-up (what q3d does before the solve) ---------------------
  * genZ! (src/Zcoord.jl:133-166) for NZ = 30*m: Z (NZ+3 faces with extrapolated guards), ZC and dZ
  * (NZ+2 each).  m > 1 splits each of the 30 Zcase2! cells (Zcoord.jl:88-124) into m equal
