@@ -5,7 +5,7 @@ is its Python host interface, mirroring the reference's NonUniform module.
 """
 from ._lib import H2GError, H2GLibraryError, load  # noqa: F401
 from .nonuniform import (CG, CalcAX, CalcRK, PBiCGSTAB, Preconditioner, Solver, WorkBuffers,  # noqa: F401
-                         rbsor_core, smoother_selector)
+                         rbsor_core, smoother_selector, solveSOR)
 
 __all__ = ["CG", "CalcAX", "CalcRK", "PBiCGSTAB", "Preconditioner", "Solver", "WorkBuffers", "rbsor_core",
-           "smoother_selector", "H2GError", "H2GLibraryError", "load"]
+           "smoother_selector", "solveSOR", "H2GError", "H2GLibraryError", "load"]

@@ -68,6 +68,16 @@ _SIGS = {
     "h2g_CG": (C.c_int, [C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, _dp, _dp, _dp, C.c_double, C.c_double,
                          C.c_double, _dp, _dp, _dp, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                          _dp, C.POINTER(Result)]),
+    "h2g_sor": (C.c_int, [_vp, C.c_double, C.c_double, C.c_int, C.c_int, _dp, C.POINTER(Result)]),
+    "h2g_SolveSOR": (C.c_int, [C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, _dp, _dp, _dp, C.c_double, C.c_double,
+                               C.c_double, C.c_double, _dp, _dp, _dp, C.c_double, C.c_int, C.c_int, C.c_int, _dp,
+                               C.POINTER(Result)]),
+    "h2g_set_hsrc": (C.c_int, [_vp, _dp]),
+    "h2g_calrhs": (C.c_int, [_vp, C.POINTER(Bc), C.c_int]),
+    "h2g_transient": (C.c_int, [_vp, C.POINTER(Bc), C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, _dp,
+                                C.POINTER(Result)]),
+    "h2g_batch_solve": (C.c_int, [C.c_int, C.POINTER(C.c_void_p), C.c_int, C.c_double, C.c_int, C.c_int, C.c_int,
+                                  C.POINTER(Result)]),
     "h2g_release_cached": (C.c_int, []),
     "h2g_calcax": (C.c_int, [_vp, _dp, _dp]),
     "h2g_calcrk": (C.c_int, [_vp, _dp, _dp]),

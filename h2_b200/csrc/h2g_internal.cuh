@@ -70,6 +70,9 @@ enum Stage {
   kStageCgBeta = 9,  // s1 = (r,z) -> beta (breakdown), iteration count
   kStageDot = 10,    // store s1, s2 in dot1, dot2
   kStageInitCg = 11, // CG start: s1 = (r,r) -> res0 (no rho check, NonUniform.jl:131-141)
+  kStageSorInit = 12, // SOR start: s1 = resSOR^2 -> res0
+  kStageSorHalf = 13, // s1 = colour-0 sum of r^2 -> dot1
+  kStageSorIter = 14, // s1 = colour-1 sum of r^2 -> res, convergence, iteration count
 };
 
 // Scalars of one Krylov solve, resident in device memory for the whole solve.

@@ -146,6 +146,31 @@ __device__ void finish_stage(int stage, SolverState* st, double s1, double s2) {
       st->dot1 = s1;
       st->dot2 = s2;
       break;
+    case kStageSorInit: {  // solveSOR! NonUniform.jl:1031-1035: res0 (1 if zero)
+      double res0 = sqrt(s1);
+      if (res0 == 0.0) res0 = 1.0;
+      st->res0 = res0;
+      st->res = 1.0;
+      st->itr = 0;
+      st->stop = 0;
+      st->converged = 0;
+      st->reason = kRunning;
+      if (!isfinite(res0)) { st->stop = 1; st->reason = kNonFinite; }
+      break;
+    }
+    case kStageSorHalf:  // colour 0 of rbsor! (NonUniform.jl:952-955)
+      st->dot1 = s1;
+      break;
+    case kStageSorIter: {  // colour 1, then the test of solveSOR! (NonUniform.jl:1038-1048)
+      const double res = __ddiv_rn(sqrt(__dadd_rn(st->dot1, s1)), st->res0);
+      st->itr += 1;
+      if (st->hist && st->itr <= st->hist_len) st->hist[st->itr - 1] = res;
+      st->res = res;
+      if (res < st->tol) { st->stop = 1; st->converged = 1; st->reason = kConverged; break; }
+      if (!isfinite(res)) { st->stop = 1; st->reason = kNonFinite; break; }
+      if (st->itr >= st->maxItr) { st->stop = 1; st->reason = kMaxItr; break; }
+      break;
+    }
     default:
       break;
   }
@@ -337,16 +362,13 @@ __device__ __forceinline__ void x_nbrs(T oc, int okc, int e, int lane, int p, in
 // Grid (ceil(HN/32), ceil(NY/kBY), ceil(NZ/2)); thread = colour-c cells of column (p,j) at
 // planes k0, k0+1.
 // ------------------------------------------------------------------------------------------
-template <typename T>
-__global__ void __launch_bounds__(kThreads, H2G_MINB) k_rb_pass(OpParams<T> op, T* x, const T* __restrict__ bb, int color,
-                                                       T omega, const SolverState* __restrict__ st) {
-  pdl_enter();
-  if (st && st->stop) return;
+// One colour pass over the two planes k0, k0+1 of column (p, j).  RES: also returns the sum of
+// the squared SOR residuals r = (dd + omega*(c_xm + c_ym + c_zm))*dp/omega of the updated cells
+// (rbsor_core!, NonUniform.jl:907-908); the preconditioner discards them and skips the work.
+template <typename T, bool RES>
+__device__ __forceinline__ double rb_pass_column(const OpParams<T>& op, T* x, const T* __restrict__ bb, int color,
+                                                 T omega, int lane, int p, int j, int k0) {
   const Geo& g = op.g;
-  const int lane = threadIdx.x, p = blockIdx.x * kBX + lane;
-  const int j = 1 + blockIdx.y * kBY + threadIdx.y;
-  const int k0 = 1 + 2 * blockIdx.z;
-  if (j > g.NY) return;  // uniform per warp
   const int o = color ^ 1;
   const bool pok = p < g.HN;
   const uint8_t* key = op.key;
@@ -392,6 +414,7 @@ __global__ void __launch_bounds__(kThreads, H2G_MINB) k_rb_pass(OpParams<T> op, 
     const int e = (1 + color + j + k0 + u) & 1;
     x_nbrs<T, true>(col[u + 1], kcol[u + 1], e, lane, p, g.HN, x, key, ro0 + u * PL, xm[u], xp[u], kxm[u], kxp[u]);
   }
+  double acc = 0.0;
 #pragma unroll
   for (int u = 0; u < 2; ++u) {
     if (!ok[u]) continue;
@@ -403,7 +426,46 @@ __global__ void __launch_bounds__(kThreads, H2G_MINB) k_rb_pass(OpParams<T> op, 
     const T ss = nb_sum(c, xp[u], xm[u], yp[u], ym[u], col[u + 2], col[u]);
     const T dp = sub(gs_div(sub(ss, bv[u]), c.dd), pp[u]);  // * m0 (= 1)
     x[ac] = add(pp[u], mul(omega, dp));
+    if constexpr (RES) {
+      const T r = dvd(mul(add(c.dd, mul(omega, add(add(c.cxm, c.cym), c.czm))), dp), omega);
+      acc = add(acc, mul((double)r, (double)r));
+    }
   }
+  return acc;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads, H2G_MINB) k_rb_pass(OpParams<T> op, T* x, const T* __restrict__ bb, int color,
+                                                       T omega, const SolverState* __restrict__ st) {
+  pdl_enter();
+  if (st && st->stop) return;
+  const int lane = threadIdx.x, p = blockIdx.x * kBX + lane;
+  const int j = 1 + blockIdx.y * kBY + threadIdx.y;
+  const int k0 = 1 + 2 * blockIdx.z;
+  if (j > op.g.NY) return;  // uniform per warp
+  rb_pass_column<T, false>(op, x, bb, color, omega, lane, p, j, k0);
+}
+
+// rbsor_core! with its residual (NonUniform.jl:848-915) for solveSOR! (NonUniform.jl:1004-1051):
+// colour `color` updated with relaxation omega, sum of r^2 -> stage (kStageSorHalf after colour
+// 0, kStageSorIter after colour 1).  The colour-1 launch ends a WHILE-body pass: block 0 counts
+// the pass and ends the loop provisionally; only the finisher can continue it.
+__global__ void __launch_bounds__(kThreads) k_sor_pass(OpParams<double> op, double* x,
+                                                       const double* __restrict__ bb, int color, double omega,
+                                                       SolverState* st, double* __restrict__ partials, int stage,
+                                                       cudaGraphConditionalHandle hc, int use_cond) {
+  pdl_enter();
+  if (color == 1 && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.x == 0 && threadIdx.y == 0) {
+    st->passes += 1;
+    set_cond(hc, use_cond, 0);
+  }
+  if (st->stop) return;
+  const int lane = threadIdx.x, p = blockIdx.x * kBX + lane;
+  const int j = 1 + blockIdx.y * kBY + threadIdx.y;
+  const int k0 = 1 + 2 * blockIdx.z;
+  double v[1] = {0.0};
+  if (j <= op.g.NY) v[0] = rb_pass_column<double, true>(op, x, bb, color, omega, lane, p, j, k0);
+  reduce_finish<1>(v, partials, st, stage, hc, color == 1 ? use_cond : 0);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -666,6 +728,62 @@ __global__ void __launch_bounds__(kThreads) k_rk(OpParams<double> op, T* __restr
 }
 
 // ------------------------------------------------------------------------------------------
+// resSOR (NonUniform.jl:680-743): the SOR residual of the current th without updating it,
+//   dp = ((ss - b)/dd - th)*m0,  r = (dd + omega*(c_xm + c_ym + c_zm))*dp/omega,
+// sum r^2 over the interior -> stage.  Both colours of column (p, j) at plane k.
+// ------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(kThreads) k_res_sor(OpParams<double> op, const double* __restrict__ th,
+                                                       const double* __restrict__ b, double omega, SolverState* st,
+                                                       double* __restrict__ partials, int stage) {
+  pdl_enter();
+  const Geo& g = op.g;
+  const int lane = threadIdx.x, p = blockIdx.x * kBX + lane;
+  const int j = 1 + blockIdx.y * kBY + threadIdx.y;
+  const int k = 1 + blockIdx.z;
+  double v[1] = {0.0};
+  if (j <= g.NY) {
+    const bool pok = p < g.HN;
+    const uint8_t* key = op.key;
+    const int r0 = g.row(0, j, k), r1 = r0 + g.HP;
+    const int e0 = (1 + j + k) & 1;
+    bool ok[2];
+    double bb[2] = {0.0, 0.0};
+#pragma unroll
+    for (int col = 0; col < 2; ++col) {
+      const int i = 2 * p + (e0 ^ col);
+      ok[col] = pok && i >= 1 && i <= g.NX;
+      if (ok[col]) bb[col] = b[(col ? r1 : r0) + p];
+    }
+    Pair<double, double> P;
+    load_pair<double, double>(g, th, key, r0, p, pok, P);
+    double xm0, xp0, xm1, xp1;
+    int kxm0, kxp0, kxm1, kxp1;
+    x_nbrs<double, true>(P.c1[1], P.kc1[1], e0, lane, p, g.HN, th, key, r1, xm0, xp0, kxm0, kxp0);
+    x_nbrs<double, true>(P.c0[1], P.kc0[1], e0 ^ 1, lane, p, g.HN, th, key, r0, xm1, xp1, kxm1, kxp1);
+#pragma unroll
+    for (int col = 0; col < 2; ++col) {
+      if (!ok[col]) continue;
+      const int ci = (col ? r1 : r0) + p;
+      Coef<double> c;
+      bool has;
+      if (col == 0)
+        has = cell_coef(op, k, (uint8_t)P.kc0[1], (uint8_t)kxm0, (uint8_t)kxp0, (uint8_t)P.ky1m, (uint8_t)P.ky1p,
+                        (uint8_t)P.kc1[0], (uint8_t)P.kc1[2], ci, c);
+      else
+        has = cell_coef(op, k, (uint8_t)P.kc1[1], (uint8_t)kxm1, (uint8_t)kxp1, (uint8_t)P.ky0m, (uint8_t)P.ky0p,
+                        (uint8_t)P.kc0[0], (uint8_t)P.kc0[2], ci, c);
+      if (!has) continue;
+      const double ss = col == 0 ? nb_sum(c, xp0, xm0, P.y1p, P.y1m, P.c1[2], P.c1[0])
+                                 : nb_sum(c, xp1, xm1, P.y0p, P.y0m, P.c0[2], P.c0[0]);
+      const double dp = sub(gs_div(sub(ss, bb[col]), c.dd), col == 0 ? P.c0[1] : P.c1[1]);
+      const double r = dvd(mul(add(c.dd, mul(omega, add(add(c.cxm, c.cym), c.czm))), dp), omega);
+      v[0] = add(v[0], mul(r, r));
+    }
+  }
+  reduce_finish<1>(v, partials, st, stage, 0, 0);
+}
+
+// ------------------------------------------------------------------------------------------
 // Element-wise kernels over whole vectors.  Guard and padding entries of every Krylov vector
 // are zero and stay zero, so these run linearly over the buffer with 16-byte accesses.
 // ------------------------------------------------------------------------------------------
@@ -888,6 +1006,112 @@ __global__ void k_from_dev(Geo g, const T* __restrict__ src, double* __restrict_
   const int j = blockIdx.y, k = blockIdx.z;
   if (i >= g.MX) return;
   dst[(long long)i + (long long)g.MX * ((long long)j + (long long)g.MY * k)] = (double)src[g.off(i, j, k)];
+}
+
+// ------------------------------------------------------------------------------------------
+// calRHS! (src/NonUniform.jl:57-91) with apply_bc2RHS! (src/RHS.jl:23-192), one thread per
+// interior cell (i fastest).  The boundary faces are applied in the reference's order x-, x+,
+// y-, y+, z-, z+ to the cells next to them, then b = -(a_p0*theta + hsrc*dx*dy*dz + b).
+// ------------------------------------------------------------------------------------------
+struct FaceBC {
+  int type[6];     // 0 isothermal (no RHS term), 1 heat flux, 2 convection
+  double q[6];     // heat flux
+  double h[6];     // heat-transfer coefficient
+  double ta[6];    // ambient temperature
+};
+
+// One face of RHS_heat_flux! / RHS_convection! (RHS.jl:70-186): sign -1 for the minus faces
+// (b += q*area; b -= h*area*(ta - theta)), +1 for the plus faces (b -= q*area; b += ...).
+__device__ __forceinline__ double face_term(const FaceBC& bc, int f, double b, double area, double th, int plus) {
+  if (bc.type[f] == 1) {
+    const double t = __dmul_rn(bc.q[f], area);
+    return plus ? __dsub_rn(b, t) : __dadd_rn(b, t);
+  }
+  if (bc.type[f] == 2) {
+    const double t = __dmul_rn(__dmul_rn(bc.h[f], area), __dsub_rn(bc.ta[f], th));
+    return plus ? __dadd_rn(b, t) : __dsub_rn(b, t);
+  }
+  return b;
+}
+
+__global__ void __launch_bounds__(256) k_calrhs(Geo g, double* __restrict__ b, const double* __restrict__ th,
+                                                 const double* __restrict__ hsrc, const double* __restrict__ rc,
+                                                 const double* __restrict__ dzk, double dx, double dy, double ddt,
+                                                 int steady, FaceBC bc, int zero_b) {
+  const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = 1 + blockIdx.y, k = 1 + blockIdx.z;
+  if (i > g.NX) return;
+  const int o = g.off(i, j, k);
+  const double t = th[o], dz = __ldg(dzk + k);
+  double bv = zero_b ? 0.0 : b[o];
+  const double ax = __dmul_rn(dy, dz), ay = __dmul_rn(dx, dz), az = __dmul_rn(dx, dy);
+  if (i == 1) bv = face_term(bc, 0, bv, ax, t, 0);
+  if (i == g.NX) bv = face_term(bc, 1, bv, ax, t, 1);
+  if (j == 1) bv = face_term(bc, 2, bv, ay, t, 0);
+  if (j == g.NY) bv = face_term(bc, 3, bv, ay, t, 1);
+  if (k == 1) bv = face_term(bc, 4, bv, az, t, 0);
+  if (k == g.NZ) bv = face_term(bc, 5, bv, az, t, 1);
+  const double ap = steady ? 0.0 : __dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(rc[o], dx), dy), dz), ddt);
+  const double hs = __dmul_rn(__dmul_rn(__dmul_rn(hsrc[o], dx), dy), dz);
+  b[o] = -__dadd_rn(__dadd_rn(__dmul_rn(ap, t), hs), bv);
+}
+
+// min, max and sum of squares of theta over the interior (the per-step line of main(),
+// heat3ds.jl:149-151).  Stage 1: one partial triple per block; stage 2 (one block) reduces the
+// partials in block order and writes out[0..2].
+__global__ void __launch_bounds__(256) k_theta_stats1(Geo g, const double* __restrict__ th,
+                                                       double* __restrict__ partials) {
+  double mn = INFINITY, mx = -INFINITY, ss = 0.0;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < g.n;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const int row = (int)(idx / g.HP), p = (int)(idx % g.HP);
+    const int c = row & 1, jk = row >> 1, j = jk % g.MY, k = jk / g.MY;
+    const int i = 2 * p + ((1 + c + j + k) & 1);
+    if (i < 1 || i > g.NX || j < 1 || j > g.NY || k < 1 || k > g.NZ) continue;
+    const double v = th[idx];
+    mn = fmin(mn, v);
+    mx = fmax(mx, v);
+    ss = __dadd_rn(ss, __dmul_rn(v, v));
+  }
+  __shared__ double sm[3][8];
+  for (int o = 16; o > 0; o >>= 1) {
+    mn = fmin(mn, __shfl_down_sync(kFull, mn, o));
+    mx = fmax(mx, __shfl_down_sync(kFull, mx, o));
+    ss += __shfl_down_sync(kFull, ss, o);
+  }
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) { sm[0][w] = mn; sm[1][w] = mx; sm[2][w] = ss; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int q = 1; q < (int)(blockDim.x >> 5); ++q) {
+      mn = fmin(mn, sm[0][q]);
+      mx = fmax(mx, sm[1][q]);
+      ss += sm[2][q];
+    }
+    partials[3 * blockIdx.x] = mn;
+    partials[3 * blockIdx.x + 1] = mx;
+    partials[3 * blockIdx.x + 2] = ss;
+  }
+}
+
+__global__ void __launch_bounds__(32) k_theta_stats2(const double* __restrict__ partials, int nb,
+                                                      double* __restrict__ out) {
+  double mn = INFINITY, mx = -INFINITY, ss = 0.0;
+  for (int q = threadIdx.x; q < nb; q += 32) {
+    mn = fmin(mn, partials[3 * q]);
+    mx = fmax(mx, partials[3 * q + 1]);
+    ss += partials[3 * q + 2];
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    mn = fmin(mn, __shfl_down_sync(kFull, mn, o));
+    mx = fmax(mx, __shfl_down_sync(kFull, mx, o));
+    ss += __shfl_down_sync(kFull, ss, o);
+  }
+  if (threadIdx.x == 0) {
+    out[0] = mn;
+    out[1] = mx;
+    out[2] = sqrt(ss);
+  }
 }
 
 // ------------------------------------------------------------------------------------------

@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -18,6 +19,7 @@
 #include <type_traits>
 #include <utility>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/h2g.h"
@@ -66,7 +68,9 @@ struct SolveGraph {
   }
 };
 
-enum GraphKind { kGPbicg64 = 0, kGCg64 = 1, kGPbicg32 = 2, kGCg32 = 3, kGPbicgMx = 4, kGCgMx = 5, kGNum = 6 };
+enum GraphKind {
+  kGPbicg64 = 0, kGCg64 = 1, kGPbicg32 = 2, kGCg32 = 3, kGPbicgMx = 4, kGCgMx = 5, kGSor = 6, kGNum = 7
+};
 
 template <typename T>
 struct OpTables {
@@ -108,6 +112,9 @@ struct Solver {
   double* b = nullptr;
   double* th_snap = nullptr;
   double* r64 = nullptr;
+  double* hsrc = nullptr;      // heat source per cell (device layout), set by h2g_set_hsrc
+  double* stats = nullptr;     // per-step theta statistics of the transient driver
+  int stats_cap = 0;
   // Krylov vectors in working precision: r, r0, p, ph, q, s, sh, t (+ e for refinement)
   void* kv[10] = {nullptr};
   void* hook[2] = {nullptr, nullptr};  // scratch of the single-kernel entry points (never a Krylov vector)
@@ -241,6 +248,7 @@ static void destroy(Solver* s) {
   free_tables32(s->t32);
   cudaFree(s->rc64); cudaFree(s->rc32);
   cudaFree(s->th); cudaFree(s->b); cudaFree(s->th_snap); cudaFree(s->r64);
+  cudaFree(s->hsrc); cudaFree(s->stats);
   for (auto& p : s->kv) cudaFree(p);
   for (auto& p : s->hook) cudaFree(p);
   for (auto& p : s->stage) cudaFree(p);
@@ -455,17 +463,12 @@ static std::vector<unsigned char> signature(const OpParams<T>& opA, const OpPara
   return v;
 }
 
-template <typename T, typename TX, typename TP>
-static int get_graph(Solver* s, int kind, int smoother, const OpParams<T>& op, const OpParams<TP>& opM, TX* x,
-                     SolverState* st, SolveGraph** out) {
-  SolveGraph& G = s->graphs[kind][smoother ? 1 : 0];
-  std::vector<unsigned char> sig = signature(op, opM, smoother, (const void*)x);
-  if (G.exec && G.sig == sig) {
-    *out = &G;
-    return H2G_OK;
-  }
+// Instantiate the loop of a solve: a conditional WHILE node whose body is one iteration
+// (body(stream, handle, 1) captured into it), or, where conditional nodes are unavailable, a graph
+// of one iteration (body(stream, 0, 0)) that run_graph relaunches from the host.
+template <typename Body>
+static int make_loop_graph(Solver* s, SolveGraph& G, Body body) {
   G.reset();
-  const bool cg = (kind == kGCg64 || kind == kGCg32 || kind == kGCgMx);
   bool cond = !s->no_cond;
   if (cond) {
     cudaGraph_t parent = nullptr;
@@ -482,12 +485,11 @@ static int get_graph(Solver* s, int kind, int smoother, const OpParams<T>& op, c
       ok = cudaGraphAddNode(&node, parent, nullptr, 0, &cp) == cudaSuccess;
     }
     if (ok) {
-      cudaGraph_t body = cp.conditional.phGraph_out[0];
-      ok = cudaStreamBeginCaptureToGraph(s->cap, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) ==
+      cudaGraph_t bodyg = cp.conditional.phGraph_out[0];
+      ok = cudaStreamBeginCaptureToGraph(s->cap, bodyg, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) ==
            cudaSuccess;
       if (ok) {
-        if (cg) launch_cg_body<T, TX, TP>(s, s->cap, op, opM, x, st, smoother, hc, 1);
-        else launch_pbicg_body<T, TX, TP>(s, s->cap, op, opM, x, st, smoother, hc, 1);
+        body(s->cap, hc, 1);
         cudaGraph_t got = nullptr;
         ok = cudaStreamEndCapture(s->cap, &got) == cudaSuccess;
       }
@@ -506,14 +508,30 @@ static int get_graph(Solver* s, int kind, int smoother, const OpParams<T>& op, c
     }
   }
   if (!cond) {
-    // fallback: a graph of one iteration, relaunched by the host until the state says stop
     CK(cudaStreamBeginCapture(s->cap, cudaStreamCaptureModeRelaxed));
-    if (cg) launch_cg_body<T, TX, TP>(s, s->cap, op, opM, x, st, smoother, 0, 0);
-    else launch_pbicg_body<T, TX, TP>(s, s->cap, op, opM, x, st, smoother, 0, 0);
+    body(s->cap, (cudaGraphConditionalHandle)0, 0);
     CK(cudaStreamEndCapture(s->cap, &G.graph));
     CK(cudaGraphInstantiate(&G.exec, G.graph, 0));
     G.cond = false;
   }
+  return H2G_OK;
+}
+
+template <typename T, typename TX, typename TP>
+static int get_graph(Solver* s, int kind, int smoother, const OpParams<T>& op, const OpParams<TP>& opM, TX* x,
+                     SolverState* st, SolveGraph** out) {
+  SolveGraph& G = s->graphs[kind][smoother ? 1 : 0];
+  std::vector<unsigned char> sig = signature(op, opM, smoother, (const void*)x);
+  if (G.exec && G.sig == sig) {
+    *out = &G;
+    return H2G_OK;
+  }
+  const bool cg = (kind == kGCg64 || kind == kGCg32 || kind == kGCgMx);
+  int rc = make_loop_graph(s, G, [&](cudaStream_t cs, cudaGraphConditionalHandle hc, int use_cond) {
+    if (cg) launch_cg_body<T, TX, TP>(s, cs, op, opM, x, st, smoother, hc, use_cond);
+    else launch_pbicg_body<T, TX, TP>(s, cs, op, opM, x, st, smoother, hc, use_cond);
+  });
+  if (rc) return rc;
   G.sig = sig;
   *out = &G;
   return H2G_OK;
@@ -838,6 +856,162 @@ static int solve(Solver* s, bool cg, double tol, int maxItr, int smoother, int v
 // ------------------------------------------------------------------------------------------
 // creation and set-up
 // ------------------------------------------------------------------------------------------
+// solveSOR! (NonUniform.jl:1004-1051): res0 = resSOR, then rbsor! passes (colour 0, colour 1,
+// each with its sum of squared residuals) until sqrt(sum)/res0 < tol.  FP64 on every handle
+// precision.  Deviation: a non-finite residual stops the loop (the reference would run maxItr
+// passes of NaN).
+static int solve_sor(Solver* s, double omega, double tol, int maxItr, int verbose, double* res_hist,
+                     h2g_result* out) {
+  if (!s->grid_set || !s->fields_set) return fail(H2G_BAD_ARG, "h2g_set_grid and h2g_set_fields must come first");
+  if (maxItr < 1) return fail(H2G_BAD_ARG, "maxItr must be >= 1");
+  if (!(omega > 0.0 && omega < 2.0)) return fail(H2G_BAD_ARG, "omega must lie in (0, 2)");
+  const Geo& g = s->g;
+  int rc = ensure_hist(s, maxItr);
+  if (rc) return rc;
+  const OpParams<double> op = op_params<double>(s, s->t64);
+  SolverState* st = s->st;
+  if ((rc = prime_state(s, st, tol, maxItr, s->hist, maxItr))) return rc;
+  const dim3 ag = ax_grid(g), rg = rb_grid(g), blk(kBX, kBY);
+  launch(s, k_res_sor, ag, blk, s->stream, op, (const double*)s->th, (const double*)s->b, omega, st, s->partials,
+         (int)kStageSorInit);
+  CKL();
+  SolveGraph& G = s->graphs[kGSor][0];
+  std::vector<unsigned char> sig(sizeof op + sizeof omega);
+  memcpy(sig.data(), &op, sizeof op);
+  memcpy(sig.data() + sizeof op, &omega, sizeof omega);
+  if (!G.exec || G.sig != sig) {
+    rc = make_loop_graph(s, G, [&](cudaStream_t cs, cudaGraphConditionalHandle hc, int use_cond) {
+      launch(s, k_sor_pass, rg, blk, cs, op, s->th, (const double*)s->b, 0, omega, st, s->partials,
+             (int)kStageSorHalf, hc, 0);
+      launch(s, k_sor_pass, rg, blk, cs, op, s->th, (const double*)s->b, 1, omega, st, s->partials,
+             (int)kStageSorIter, hc, use_cond);
+    });
+    if (rc) return rc;
+    G.sig = sig;
+  }
+  if ((rc = run_graph(s, &G, st, maxItr))) return rc;
+  CK(cudaMemcpyAsync(s->st_host, st, sizeof(SolverState), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  SolverState fin = *s->st_host;
+  const int nh = std::min(std::max(fin.itr, 0), maxItr);
+  std::vector<double> hh(nh);
+  if (nh > 0 && (verbose || res_hist)) {
+    CK(cudaMemcpy(hh.data(), s->hist, sizeof(double) * nh, cudaMemcpyDeviceToHost));
+    if (res_hist) memcpy(res_hist, hh.data(), sizeof(double) * nh);
+  }
+  if (verbose) print_log(fin, hh.data(), nh, fin.converged);
+  if (out) {
+    out->launches = 2 + 2LL * std::max(1, fin.itr);
+    out->isconverged = fin.converged;
+    out->itr = fin.itr;
+    out->outer = 0;
+    out->status = status_of(fin);
+    out->res0 = fin.res0;
+    out->res = fin.res;
+  }
+  return status_of(fin);
+}
+
+// ---- calRHS! and the time loop of main() ----------------------------------------------------
+
+static int face_bc(const h2g_bc* bc, FaceBC& f) {
+  if (!bc) return fail(H2G_BAD_ARG, "null boundary-condition array");
+  for (int q = 0; q < 6; ++q) {
+    const int t = bc[q].type;
+    if (t != H2G_ISOTHERMAL && t != H2G_HEAT_FLUX && t != H2G_CONVECTION)
+      return fail(H2G_BAD_ARG, "face %d: unknown boundary type %d", q, t);
+    f.type[q] = t;
+    f.q[q] = bc[q].heat_flux;
+    f.h[q] = bc[q].htc;
+    f.ta[q] = bc[q].ambient;
+  }
+  return H2G_OK;
+}
+
+static int ensure_hsrc(Solver* s) {
+  if (s->hsrc) return H2G_OK;
+  CK(cudaMalloc(&s->hsrc, sizeof(double) * (size_t)s->g.n));
+  CK(cudaMemsetAsync(s->hsrc, 0, sizeof(double) * (size_t)s->g.n, s->stream));
+  return H2G_OK;
+}
+
+static int calrhs(Solver* s, const FaceBC& f, int zero_b) {
+  if (!s->grid_set || !s->fields_set) return fail(H2G_BAD_ARG, "h2g_set_grid and h2g_set_fields must come first");
+  if (!s->steady && !s->rc64) return fail(H2G_BAD_ARG, "a transient grid needs rho and cp (h2g_set_fields)");
+  int rc = ensure_hsrc(s);
+  if (rc) return rc;
+  const Geo& g = s->g;
+  dim3 grid((g.NX + 127) / 128, g.NY, g.NZ);
+  k_calrhs<<<grid, 128, 0, s->stream>>>(g, s->b, s->th, s->hsrc, s->rc64, s->t64.dzk, s->dx, s->dy,
+                                         s->steady ? 0.0 : 1.0 / s->dt, s->steady, f, zero_b);
+  CKL();
+  return H2G_OK;
+}
+
+// main()'s time loop (heat3ds.jl:123-151) with theta resident on the device: per step calRHS!
+// (b cleared first: the reference accumulates b across steps), the Krylov solve from the previous
+// step's theta, and the interior min / max / L2 norm of theta.
+static int transient(Solver* s, const FaceBC& f, int nt, int method, double tol, int maxItr, int smoother,
+                     int verbose, double* step_stats, h2g_result* out) {
+  if (nt < 1) return fail(H2G_BAD_ARG, "nt must be >= 1");
+  if (method != 0 && method != 1) return fail(H2G_BAD_ARG, "method must be 0 (PBiCGSTAB) or 1 (CG)");
+  const int nb1 = s->num_sms * 2;
+  if (s->stats_cap < nt) {
+    cudaFree(s->stats);
+    s->stats = nullptr;
+    s->stats_cap = 0;
+    CK(cudaMalloc(&s->stats, sizeof(double) * (3 * (size_t)nt + 3 * (size_t)nb1)));
+    s->stats_cap = nt;
+  }
+  double* part = s->stats + 3 * (size_t)nt;
+  std::vector<int> itrs(nt, 0);
+  std::vector<double> ress(nt, 0.0);
+  long long launches = 0;
+  int all_conv = 1, last = H2G_OK, done = 0;
+  h2g_result r{};
+  for (int step = 0; step < nt; ++step) {
+    int rc = calrhs(s, f, 1);
+    if (rc) return rc;
+    const int st = solve(s, method == 1, tol, maxItr, smoother, verbose, nullptr, &r);
+    if (st == H2G_BAD_ARG || st == H2G_CUDA_ERROR) return st;
+    k_theta_stats1<<<nb1, 256, 0, s->stream>>>(s->g, s->th, part);
+    k_theta_stats2<<<1, 32, 0, s->stream>>>(part, nb1, s->stats + 3 * (size_t)step);
+    CKL();
+    itrs[step] = r.itr;
+    ress[step] = r.res;
+    launches += r.launches + 3;
+    all_conv &= r.isconverged;
+    if (st != H2G_OK) last = st;
+    ++done;
+    if (st == H2G_NONFINITE) break;
+  }
+  if (step_stats) {
+    std::vector<double> hs(3 * (size_t)done);
+    CK(cudaMemcpyAsync(hs.data(), s->stats, sizeof(double) * hs.size(), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    for (int q = 0; q < done; ++q) {
+      step_stats[5 * q + 0] = hs[3 * q + 0];
+      step_stats[5 * q + 1] = hs[3 * q + 1];
+      step_stats[5 * q + 2] = hs[3 * q + 2];
+      step_stats[5 * q + 3] = itrs[q];
+      step_stats[5 * q + 4] = ress[q];
+    }
+  }
+  CK(cudaStreamSynchronize(s->stream));
+  if (out) {
+    long long tot = 0;
+    for (int q = 0; q < done; ++q) tot += itrs[q];
+    out->isconverged = all_conv;
+    out->itr = (int)std::min<long long>(tot, 2147483647LL);
+    out->outer = done;
+    out->status = last;
+    out->res0 = r.res0;
+    out->res = r.res;
+    out->launches = launches;
+  }
+  return last;
+}
+
 static int create(int MX, int MY, int MZ, int precision, Solver** out) {
   if (!out) return fail(H2G_BAD_ARG, "null output pointer");
   *out = nullptr;
@@ -1201,10 +1375,11 @@ int h2g_cg(h2g_solver* h, double tol, int maxItr, int smoother, int verbose, dou
 static std::mutex g_cache_mu;
 static h2g_solver* g_cache[3] = {nullptr, nullptr, nullptr};
 
-static int oneshot(bool cg, int MX, int MY, int MZ, double* theta, const double* b, const double* lambda,
+// method 0: PBiCGSTAB, 1: CG, 2: SOR (omega used only by SOR)
+static int oneshot(int method, int MX, int MY, int MZ, double* theta, const double* b, const double* lambda,
                    const double* mask, const double* rho, const double* cp, double dx, double dy, double dt,
                    const double* ZC, const double* dZ, const double* HC, double tol, int maxItr, int smoother,
-                   int verbose, int is_steady, int precision, double* res_hist, h2g_result* out) {
+                   double omega, int verbose, int is_steady, int precision, double* res_hist, h2g_result* out) {
   if (precision < H2G_FP64 || precision > H2G_MIXED_IR) return fail(H2G_BAD_ARG, "unknown precision %d", precision);
   if (!theta || !b) return fail(H2G_BAD_ARG, "null theta/b");
   std::lock_guard<std::mutex> lk(g_cache_mu);
@@ -1219,7 +1394,8 @@ static int oneshot(bool cg, int MX, int MY, int MZ, double* theta, const double*
   if ((rc = h2g_set_fields(h, lambda, mask, is_steady ? nullptr : rho, is_steady ? nullptr : cp))) return rc;
   if ((rc = h2g_set_rhs(h, b))) return rc;
   if ((rc = h2g_set_theta(h, theta))) return rc;
-  int st = h2g::solve(S(h), cg, tol, maxItr, smoother, verbose, res_hist, out);
+  int st = method == 2 ? h2g::solve_sor(S(h), omega, tol, maxItr, verbose, res_hist, out)
+                       : h2g::solve(S(h), method == 1, tol, maxItr, smoother, verbose, res_hist, out);
   if (st == H2G_BAD_ARG || st == H2G_CUDA_ERROR) return st;
   if ((rc = h2g_get_theta(h, theta))) return rc;
   return st;
@@ -1229,7 +1405,7 @@ int h2g_PBiCGSTAB(int MX, int MY, int MZ, double* theta, const double* b, const 
                   const double* rho, const double* cp, double dx, double dy, double dt, const double* ZC,
                   const double* dZ, const double* HC, double tol, int maxItr, int smoother, int verbose,
                   int is_steady, int precision, double* res_hist, h2g_result* out) {
-  return oneshot(false, MX, MY, MZ, theta, b, lambda, mask, rho, cp, dx, dy, dt, ZC, dZ, HC, tol, maxItr, smoother,
+  return oneshot(0, MX, MY, MZ, theta, b, lambda, mask, rho, cp, dx, dy, dt, ZC, dZ, HC, tol, maxItr, smoother, 1.0,
                  verbose, is_steady, precision, res_hist, out);
 }
 
@@ -1237,8 +1413,109 @@ int h2g_CG(int MX, int MY, int MZ, double* theta, const double* b, const double*
            const double* rho, const double* cp, double dx, double dy, double dt, const double* ZC, const double* dZ,
            const double* HC, double tol, int maxItr, int smoother, int verbose, int is_steady, int precision,
            double* res_hist, h2g_result* out) {
-  return oneshot(true, MX, MY, MZ, theta, b, lambda, mask, rho, cp, dx, dy, dt, ZC, dZ, HC, tol, maxItr, smoother,
+  return oneshot(1, MX, MY, MZ, theta, b, lambda, mask, rho, cp, dx, dy, dt, ZC, dZ, HC, tol, maxItr, smoother, 1.0,
                  verbose, is_steady, precision, res_hist, out);
+}
+
+int h2g_sor(h2g_solver* h, double omega, double tol, int maxItr, int verbose, double* res_hist, h2g_result* out) {
+  if (int rc = h2g::check_handle(h)) return rc;
+  return h2g::solve_sor(S(h), omega, tol, maxItr, verbose, res_hist, out);
+}
+
+int h2g_SolveSOR(int MX, int MY, int MZ, double* theta, const double* b, const double* lambda, const double* mask,
+                 const double* rho, const double* cp, double dx, double dy, double dt, double omega,
+                 const double* ZC, const double* dZ, const double* HC, double tol, int maxItr, int verbose,
+                 int is_steady, double* res_hist, h2g_result* out) {
+  return oneshot(2, MX, MY, MZ, theta, b, lambda, mask, rho, cp, dx, dy, dt, ZC, dZ, HC, tol, maxItr, 0, omega,
+                 verbose, is_steady, H2G_FP64, res_hist, out);
+}
+
+int h2g_set_hsrc(h2g_solver* h, const double* hsrc) {
+  if (int rc = h2g::check_handle(h)) return rc;
+  Solver* s = S(h);
+  if (int rc = h2g::ensure_hsrc(s)) return rc;
+  return h2g::upload<double>(s, hsrc, s->hsrc);
+}
+
+int h2g_calrhs(h2g_solver* h, const h2g_bc* bc, int zero_b) {
+  if (int rc = h2g::check_handle(h)) return rc;
+  h2g::FaceBC f;
+  if (int rc = h2g::face_bc(bc, f)) return rc;
+  Solver* s = S(h);
+  if (int rc = h2g::calrhs(s, f, zero_b ? 1 : 0)) return rc;
+  CK(cudaStreamSynchronize(s->stream));
+  return H2G_OK;
+}
+
+int h2g_transient(h2g_solver* h, const h2g_bc* bc, int nt, int method, double tol, int maxItr, int smoother,
+                  int verbose, double* step_stats, h2g_result* out) {
+  if (int rc = h2g::check_handle(h)) return rc;
+  h2g::FaceBC f;
+  if (int rc = h2g::face_bc(bc, f)) return rc;
+  return h2g::transient(S(h), f, nt, method, tol, maxItr, smoother, verbose, step_stats, out);
+}
+
+int h2g_batch_solve(int n, h2g_solver* const* hs, int method, double tol, int maxItr, int smoother, int threads,
+                    h2g_result* outs) {
+  if (n < 1 || !hs || !outs) return fail(H2G_BAD_ARG, "need n >= 1 handles and n results");
+  if (method != 0 && method != 1 && method != 2) return fail(H2G_BAD_ARG, "method must be 0, 1 or 2");
+  for (int q = 0; q < n; ++q) {
+    if (!hs[q]) return fail(H2G_BAD_ARG, "handle %d is null", q);
+    for (int r = 0; r < q; ++r)
+      if (hs[r] == hs[q]) return fail(H2G_BAD_ARG, "handle %d appears twice", q);
+  }
+  // one non-blocking stream per handle for the duration of the batch
+  std::vector<cudaStream_t> own(n, nullptr), saved(n, nullptr);
+  for (int q = 0; q < n; ++q) {
+    Solver* s = S(hs[q]);
+    saved[q] = s->stream;
+    if (cudaSetDevice(s->device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&own[q], cudaStreamNonBlocking) != cudaSuccess) {
+      for (int r = 0; r < q; ++r) cudaStreamDestroy(own[r]);
+      return fail(H2G_CUDA_ERROR, "stream creation failed");
+    }
+    // the handle's pending work (uploads) comes first
+    if (saved[q]) cudaStreamSynchronize(saved[q]);
+    s->stream = own[q];
+  }
+  cudaDeviceSynchronize();
+  const int nt = std::max(1, std::min(threads > 0 ? threads : 16, n));
+  std::atomic<int> next(0);
+  std::vector<std::string> errs(n);
+  auto work = [&]() {
+    for (int q = next.fetch_add(1); q < n; q = next.fetch_add(1)) {
+      Solver* s = S(hs[q]);
+      cudaSetDevice(s->device);
+      h2g_result r{};
+      int st;
+      if (method == 2) st = h2g::solve_sor(s, 1.0, tol, maxItr, 0, nullptr, &r);
+      else st = h2g::solve(s, method == 1, tol, maxItr, smoother, 0, nullptr, &r);
+      r.status = st;
+      outs[q] = r;
+      if (st == H2G_BAD_ARG || st == H2G_CUDA_ERROR) errs[q] = h2g_last_error();
+    }
+  };
+  std::vector<std::thread> pool;
+  for (int t = 1; t < nt; ++t) pool.emplace_back(work);
+  work();
+  for (auto& t : pool) t.join();
+  for (int q = 0; q < n; ++q) {
+    Solver* s = S(hs[q]);
+    cudaSetDevice(s->device);
+    cudaStreamSynchronize(own[q]);
+    s->stream = saved[q];
+    cudaStreamDestroy(own[q]);
+  }
+  int worst = H2G_OK;
+  for (int q = 0; q < n; ++q) {
+    const int st = outs[q].status;
+    if (st == H2G_BAD_ARG || st == H2G_CUDA_ERROR) {
+      fail(st, "batch member %d: %s", q, errs[q].c_str());
+      return st;
+    }
+    if (st != H2G_OK && worst == H2G_OK) worst = st;
+  }
+  return worst;
 }
 
 int h2g_release_cached(void) {

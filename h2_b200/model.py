@@ -6,9 +6,10 @@ right-hand side.
   NZ = 30*m refines each of the 30 Zcase2! cells into m equal sub-cells.
 * Geometry: h2g_model_fill_id, the GPU version of fillID! (src/modelA.jl:545-556).
 * setProperties! (modelA.jl:499-542), apply_boundary_conditions! (boundary_conditions.jl:94-313),
-  set_BC_coef (360-394), HeatSrc! (heat3ds.jl:55-64) and calRHS! (NonUniform.jl:57-91 with
-  RHS.jl:23-192) are restated here with numpy in the reference's operation order (numpy does
-  not fuse multiply-adds), so b is bit-identical to the reference's.
+  set_BC_coef (360-394) and HeatSrc! (heat3ds.jl:55-64) are table look-ups and copies, done
+  here with numpy.
+* calRHS! (NonUniform.jl:57-91 with RHS.jl:23-192) runs on the GPU (h2g_calrhs), in the
+  reference's operation order, so b is bit-identical to the reference's.
 """
 from __future__ import annotations
 
@@ -133,43 +134,21 @@ def heat_src(wk: WorkBuffers, ID: np.ndarray):
     hs[ID[inner] == 7] = Q_SRC
 
 
-def calRHS(wk: WorkBuffers, dx: float, dy: float, dt: float, dZ: np.ndarray, bcs, is_steady: bool):
-    """calRHS! (NonUniform.jl:57-91): boundary terms (RHS.jl:83-192), then
-    b = -(a_p0*theta + hsrc*dx*dy*dz_k + b).  b accumulates (the caller zeroes it per step)."""
-    b, th = wk.b, wk.theta
-    MX, MY, MZ = b.shape
-    dz = dZ[1:MZ - 1]
-    for f, (typ, _T, q, h, ta) in enumerate(bcs):
-        if typ == ISOTHERMAL:
-            continue
-        ax, plus = f // 2, f % 2
-        idx = [slice(1, -1)] * 3
-        idx[ax] = (MX - 2, MY - 2, MZ - 2)[ax] if plus else 1
-        idx = tuple(idx)
-        if ax == 0:
-            area = dy * dz[None, :]
-        elif ax == 1:
-            area = dx * dz[None, :]
-        else:
-            area = np.full((MX - 2, MY - 2), dx * dy)
-        if typ == HEAT_FLUX:
-            if plus:
-                b[idx] -= q * area
-            else:
-                b[idx] += q * area
-        else:
-            term = h * area * (ta - th[idx])
-            if plus:
-                b[idx] += term
-            else:
-                b[idx] -= term
-    inner = (slice(1, -1),) * 3
-    dzk = dz[None, None, :]
-    if is_steady:
-        a_p_0 = 0.0
-    else:
-        a_p_0 = wk.rho[inner] * wk.cp[inner] * dx * dy * dzk * (1.0 / dt)
-    b[inner] = -(a_p_0 * th[inner] + wk.hsrc[inner] * dx * dy * dzk + b[inner])
+def calRHS(wk: WorkBuffers, dx: float, dy: float, dt: float, ZC: np.ndarray, dZ: np.ndarray, HC, bcs,
+           is_steady: bool):
+    """calRHS! (NonUniform.jl:57-91, with apply_bc2RHS! RHS.jl:23-192) on the GPU: wk.b is
+    overwritten with -(a_p0*theta + hsrc*dx*dy*dz + boundary terms), computed from b = 0."""
+    from .nonuniform import Solver
+    s = Solver(*wk.theta.shape)
+    try:
+        s.set_grid(ZC, dZ, dx, dy, dt, HC, is_steady)
+        s.set_fields(wk.lam, wk.mask, None if is_steady else wk.rho, None if is_steady else wk.cp)
+        s.set_theta(wk.theta)
+        s.set_hsrc(wk.hsrc)
+        s.calrhs(bcs, zero_b=True)
+        s.get_rhs(wk.b)
+    finally:
+        s.close()
 
 
 @dataclass
@@ -213,5 +192,5 @@ def build_mode3(NX: int, NY: int | None = None, NZ: int = 30, *, is_steady: bool
     else:
         wk.hsrc[...] = hsrc
     dx, dy = pitch(NX), pitch(NY)
-    calRHS(wk, dx, dy, dt, dZ, bcs, is_steady)
+    calRHS(wk, dx, dy, dt, ZC, dZ, HC, bcs, is_steady)
     return Model(NX, NY, NZ, dx, dy, dt, is_steady, Z, ZC, dZ, HC, bcs, ID, wk)

@@ -20,6 +20,17 @@ _SMOOTHERS = {"none": L.H2G_SMOOTHER_NONE, "gs": L.H2G_SMOOTHER_GS}
 _PRECISION = {"fp64": L.H2G_FP64, "mixed": L.H2G_MIXED, "mixed_ir": L.H2G_MIXED_IR}
 
 
+def bc_array(bcs):
+    """Six boundary conditions (type, temperature, heat_flux, htc, ambient), faces x-, x+, y-,
+    y+, z-, z+ (BoundaryConditionSet, boundary_conditions.jl:24-31), as an h2g_bc[6]."""
+    if len(bcs) != 6:
+        raise ValueError("need 6 boundary conditions (x-, x+, y-, y+, z-, z+)")
+    arr = (L.Bc * 6)()
+    for f, (typ, temp, q, h, amb) in enumerate(bcs):
+        arr[f] = L.Bc(int(typ), float(temp), float(q), float(h), float(amb))
+    return arr
+
+
 def _f64(a: np.ndarray, name: str) -> np.ndarray:
     if not isinstance(a, np.ndarray) or a.dtype != np.float64 or a.ndim != 3 or not a.flags.f_contiguous:
         raise TypeError(f"{name}: expected a Float64 3-D array in column-major (Fortran) order")
@@ -150,6 +161,37 @@ class Solver:
         L.check(st, allowed=(L.H2G_OK, L.H2G_NOT_CONVERGED, L.H2G_BREAKDOWN, L.H2G_NONFINITE))
         return st, res
 
+    def get_rhs(self, out=None):
+        out = np.zeros(self.shape, order="F") if out is None else self._arr(out, "b")
+        L.check(self.lib.h2g_get_rhs(self.h, _ptr(out)))
+        return out
+
+    def set_hsrc(self, hsrc):
+        L.check(self.lib.h2g_set_hsrc(self.h, _ptr(self._arr(hsrc, "hsrc"))))
+
+    def calrhs(self, bcs, zero_b: bool = True):
+        """calRHS! on the device (b of the handle; zero_b=False accumulates like the reference)."""
+        L.check(self.lib.h2g_calrhs(self.h, bc_array(bcs), int(bool(zero_b))))
+
+    def transient(self, bcs, nt: int, method="pbicgstab", tol=1e-6, maxItr=20_000, smoother="gs", verbose=False):
+        """nt steps of main()'s loop on the device.  Returns (status, Result, stats) with stats
+        an (nt, 5) array: theta min, max, L2 norm, iterations, final relative residual."""
+        sm = smoother_selector(smoother)
+        stats = np.zeros((int(nt), 5))
+        res = L.Result()
+        st = self.lib.h2g_transient(self.h, bc_array(bcs), int(nt), 0 if method == "pbicgstab" else 1, float(tol),
+                                    int(maxItr), sm, int(bool(verbose)), _ptr(stats), C.byref(res))
+        L.check(st, allowed=(L.H2G_OK, L.H2G_NOT_CONVERGED, L.H2G_BREAKDOWN, L.H2G_NONFINITE))
+        return st, res, stats[: res.outer]
+
+    def sor(self, omega=1.0, tol=1e-6, maxItr=20_000, verbose=False, hist=None):
+        """solveSOR! on the handle's theta and b (FP64).  Returns (status, Result)."""
+        res = L.Result()
+        st = self.lib.h2g_sor(self.h, float(omega), float(tol), int(maxItr), int(bool(verbose)), _ptr(hist),
+                              C.byref(res))
+        L.check(st, allowed=(L.H2G_OK, L.H2G_NOT_CONVERGED, L.H2G_NONFINITE))
+        return st, res
+
     # single kernels (host arrays in and out)
     def calc_ax(self, x):
         ax = np.zeros(self.shape, order="F")
@@ -224,6 +266,41 @@ def CG(wk: WorkBuffers, dh, dt, ZC, dZ, HC, *, tol=1e-6, maxItr=20_000, smoother
        is_steady=False, precision="fp64", hist=None):
     """CG! (NonUniform.jl:115-226).  Updates wk.theta in place and returns (isconverged, itr, res0)."""
     return _oneshot("cg", wk, dh, dt, ZC, dZ, HC, tol, maxItr, smoother, par, verbose, is_steady, precision, hist)
+
+
+def solveSOR(theta, lam, b, mask, rho, cp, dh, dt, omega, ZC, dZ, HC, F=None, tol=1e-6, par="gpu", *,
+             maxItr=20_000, is_steady=False, verbose=True, hist=None):
+    """solveSOR! (NonUniform.jl:1004-1051): RB-SOR with relaxation omega until
+    sqrt(sum r^2)/res0 < tol; theta is updated in place.  The reference prints
+    "Initial residual", one "%10d %24.14E" line per pass and "Converged at n" to F and stdout;
+    with verbose the library prints them to stdout and, when F is a writable text stream, the
+    per-pass lines are written to F as well.  Returns (isconverged, itr, res0)."""
+    _check_par(par)
+    lib = L.load()
+    MX, MY, MZ = theta.shape
+    for n, a in (("theta", theta), ("lambda", lam), ("b", b), ("mask", mask), ("rho", rho), ("cp", cp)):
+        a = _f64(a, n)
+        if a.shape != (MX, MY, MZ):
+            raise ValueError(f"{n}: shape {a.shape} != {(MX, MY, MZ)}")
+    dx, dy = _dh(dh)
+    ZC = np.ascontiguousarray(ZC, dtype=np.float64)
+    dZ = np.ascontiguousarray(dZ, dtype=np.float64)
+    if dZ.size == MZ - 1:
+        dZ = np.append(dZ, dZ[-1])
+    HC = np.ascontiguousarray(HC, dtype=np.float64)
+    if ZC.size != MZ or dZ.size != MZ or HC.size != 6:
+        raise ValueError("ZC needs MZ entries, dZ MZ (or MZ-1), HC 6")
+    if F is not None and hist is None:
+        hist = np.zeros(int(maxItr))
+    res = L.Result()
+    st = lib.h2g_SolveSOR(MX, MY, MZ, _ptr(theta), _ptr(b), _ptr(lam), _ptr(mask), _ptr(rho), _ptr(cp), dx, dy,
+                          float(dt), float(omega), _ptr(ZC), _ptr(dZ), _ptr(HC), float(tol), int(maxItr),
+                          int(bool(verbose)), int(bool(is_steady)), _ptr(hist), C.byref(res))
+    L.check(st, allowed=(L.H2G_OK, L.H2G_NOT_CONVERGED, L.H2G_NONFINITE))
+    if F is not None:
+        for n in range(int(res.itr)):
+            F.write("%10d %24.14E\n" % (n + 1, hist[n]))
+    return bool(res.isconverged), int(res.itr), float(res.res0)
 
 
 def _kernel_solver(shape, dh, dt, ZC, dZ, HC, lam, m, rho, cp, is_steady, par):

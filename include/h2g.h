@@ -136,8 +136,54 @@ int h2g_CG(int MX, int MY, int MZ, double *theta, const double *b, const double 
            const double *rho, const double *cp, double dx, double dy, double dt, const double *ZC,
            const double *dZ, const double *HC, double tol, int maxItr, int smoother, int verbose, int is_steady,
            int precision, double *res_hist, h2g_result *out);
-/* Release the handles kept by h2g_PBiCGSTAB / h2g_CG. */
+/* solveSOR!(θ, λ, b, mask, ρ, cp, Δh, Δt, ω, ZC, ΔZ, HC, F, tol, par; maxItr, is_steady)
+ *   (src/NonUniform.jl:1004-1051): res0 = resSOR (1 if it is 0), then rbsor! passes (colour 0,
+ *   colour 1) with relaxation omega in (0, 2) until sqrt(sum of r^2)/res0 < tol.  Runs in FP64
+ *   whatever the handle's precision.  res_hist and verbose as for h2g_pbicgstab (the reference
+ *   writes the same lines to F and stdout).  A non-finite residual stops the loop with
+ *   H2G_NONFINITE (the reference would run on to maxItr). */
+int h2g_sor(h2g_solver *h, double omega, double tol, int maxItr, int verbose, double *res_hist, h2g_result *out);
+/* One-call drop-in for solveSOR! with the reference's arrays (FP64; handle cached as above). */
+int h2g_SolveSOR(int MX, int MY, int MZ, double *theta, const double *b, const double *lambda, const double *mask,
+                 const double *rho, const double *cp, double dx, double dy, double dt, double omega,
+                 const double *ZC, const double *dZ, const double *HC, double tol, int maxItr, int verbose,
+                 int is_steady, double *res_hist, h2g_result *out);
+/* Release the handles kept by h2g_PBiCGSTAB / h2g_CG / h2g_SolveSOR. */
 int h2g_release_cached(void);
+
+/* ---- batches ----------------------------------------------------------------------------
+ * Solve n independent systems at once (many power maps and grids of uneven size): every handle
+ * keeps its own grid, fields, θ and b (set beforehand), gets its own non-blocking stream for the
+ * batch, and its whole solve (a CUDA graph looping on the device) is issued from one of
+ * `threads` host threads (<= 0: 16), so the solves run concurrently on the GPU.  method 0
+ * PBiCGSTAB, 1 CG, 2 RB-SOR with omega = 1.  outs[q] receives handle q's result (the same values
+ * as a lone h2g_pbicgstab/h2g_cg on that handle: kernels are deterministic).  Returns H2G_OK
+ * when every member converged, else the first non-OK member status (H2G_BAD_ARG /
+ * H2G_CUDA_ERROR if a member failed that way).  No reference counterpart: the reference solves
+ * one system per call (heat3ds.jl:128-141). */
+int h2g_batch_solve(int n, h2g_solver *const *hs, int method, double tol, int maxItr, int smoother, int threads,
+                    h2g_result *outs);
+
+/* ---- right-hand side and time stepping ---------------------------------------------------
+ * wk.hsrc (src/common.jl:64, filled by HeatSrc!): volumetric heat source in W/m^3, guard layers
+ * included.  A handle without one uses zero. */
+int h2g_set_hsrc(h2g_solver *h, const double *hsrc);
+/* calRHS!(wk, Δh, Δt, ΔZ, bc_set, qsrf, par; is_steady) (src/NonUniform.jl:57-91) with
+ * apply_bc2RHS! (src/RHS.jl:23-192) on the device, with the handle's θ, hsrc, ρ·cp and grid:
+ * the boundary terms of bc[6] (x-, x+, y-, y+, z-, z+; heat flux ±q·area, convection
+ * ∓h·area·(θ∞ − θ), isothermal nothing) are added to b in that order, then
+ * b = −(a_p0·θ + hsrc·dx·dy·dz + b) over the interior.  zero_b = 0 accumulates into the current
+ * b as the reference does; zero_b = 1 starts from b = 0 (a step of a multi-step run). */
+int h2g_calrhs(h2g_solver *h, const h2g_bc *bc, int zero_b);
+/* The time loop of main() (src/heat3ds.jl:123-151) with θ resident on the device: nt steps of
+ * [h2g_calrhs(zero_b = 1); PBiCGSTAB!/CG! (method 0/1) from the previous θ].  step_stats
+ * (nullable, 5*nt doubles) receives per step the interior θmin, θmax, ||θ||_2 (the log.txt line,
+ * heat3ds.jl:149-151), the iterations and the final relative residual.  out: itr = iterations of
+ * all steps, outer = steps run, isconverged = every step converged, res0/res of the last step.
+ * A step that does not converge is reported and the loop goes on (heat3ds.jl:144-146); a
+ * non-finite residual ends it. */
+int h2g_transient(h2g_solver *h, const h2g_bc *bc, int nt, int method, double tol, int maxItr, int smoother,
+                  int verbose, double *step_stats, h2g_result *out);
 
 /* ---- kernels of the path, callable one at a time (host arrays in and out) ---------------
  * CalcAX! (NonUniform.jl:454-511): ax = A x over the interior; guard cells of ax are 0. */
