@@ -55,6 +55,8 @@ def parse():
     ap.add_argument("--kernel-reps", type=int, default=30)
     ap.add_argument("--cpu-sample-iters", type=int, default=0, help="0 = choose ~10 s of CPU work")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batch", type=int, default=64, help="members of the batched workload (0 = skip)")
+    ap.add_argument("--batch-steps", type=int, default=2)
     return ap.parse_args()
 
 
@@ -367,6 +369,8 @@ def run_ours(a, dist: Dist):
     except Exception as e:  # pragma: no cover
         log("e2e failed:", e)
 
+    batch = run_batch(a, dist, torch, stream, flush) if a.batch > 0 else None
+
     cpu = None
     if dist.rank == 0 and dist.world == 1 and not a.no_cpu_baseline:
         try:
@@ -412,6 +416,7 @@ def run_ours(a, dist: Dist):
                      "kernel": "k_rb_pass<double>: one RB-GS sweep (colour 0 then colour 1) of the FP64 smoother",
                      "algorithmic_bytes": rm["bytes"], "seconds": rm["seconds"], "peak_kind": peak_kind},
         "kernels": {f"{k[0]}_{k[1]}": v for k, v in roof.items()},
+        "batch": batch,
         "cpu_baseline": cpu,
         "e2e": e2e,
         "gpu_launches": f64["launches"],
@@ -422,6 +427,58 @@ def run_ours(a, dist: Dist):
     for s in solvers.values():
         s.close()
     dist.close()
+
+
+def run_batch(a, dist, torch, stream, flush):
+    """The batched workload: a.batch steady solves (seeded hotspot heat maps, grids drawn from
+    120^2/180^2/240^2 x 30), sharded across ranks by cell count, each rank's members solved
+    concurrently by one h2g_batch_solve.  Time = max over ranks of the CUDA-event time of the
+    (synchronous) call."""
+    from h2_b200 import batch as B
+    members = B.draw_batch(a.batch, 1000)
+    mine = [members[i] for i in B.shard(members, dist.world)[dist.rank]]
+    t0 = time.perf_counter()
+    bs = B.BatchSolver(mine)
+    t_setup = time.perf_counter() - t0
+
+    def timed(fn):
+        bs.restore()
+        torch.cuda.synchronize()
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        out = fn()  # synchronous: returns when every member's stream is idle
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) * 1e-3, out
+
+    try:
+        timed(lambda: bs.solve(tol=a.tol))  # warm-up: graph instantiation per handle
+        dist.barrier()
+        ts, res = [], None
+        for _ in range(max(1, a.batch_steps)):
+            dt_, (st, res) = timed(lambda: bs.solve(tol=a.tol))
+            ts.append(dt_)
+        dist.barrier()
+        t_seq, _ = timed(lambda: bs.solve_sequential(tol=a.tol))
+        local = {m.index: {"itr": r.itr, "conv": r.isconverged} for m, r in zip(mine, res)}
+        merged = B.gather_results(local)
+        out = {"solves": a.batch, "cells": sum(m.cells for m in members),
+               "sizes": {str(n): sum(1 for m in members if m.nx == n) for n in B.SIZES},
+               "seconds": dist.max(float(np.mean(ts))), "steps": len(ts),
+               "sequential_seconds_rank0": t_seq,
+               "speedup_vs_sequential": t_seq / float(np.mean(ts)),
+               "setup_seconds_rank0": t_setup,
+               "timing": "CUDA events around the synchronous call (includes its host-side issue of the solves)",
+               "precision": "fp64", "method": "PBiCGSTAB + RB-GS(5)", "tol": a.tol,
+               "sharding": f"greedy by cell count over {dist.world} rank(s)"}
+        if merged is not None:
+            out["iterations_total"] = int(sum(v["itr"] for v in merged.values()))
+            out["all_converged"] = bool(all(v["conv"] for v in merged.values()))
+        return out
+    finally:
+        bs.close()
 
 
 def main():
