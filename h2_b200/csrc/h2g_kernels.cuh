@@ -1138,6 +1138,77 @@ __global__ void __launch_bounds__(32) k_theta_stats2(const double* __restrict__ 
 }
 
 // ------------------------------------------------------------------------------------------
+// Steady adjoint of J = (sum_c w_c theta_c^p)^(1/p) (no reference counterpart).
+// ------------------------------------------------------------------------------------------
+// sum w*theta^p over the vector (guards and padding carry w = 0) -> kStageDot (dot1)
+__global__ void __launch_bounds__(256) k_objective(long long n, const double* __restrict__ th,
+                                                    const double* __restrict__ w, double p, SolverState* st,
+                                                    double* __restrict__ partials) {
+  pdl_enter();
+  double v[1] = {0.0};
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const double wi = w[i];
+    if (wi != 0.0) v[0] += wi * pow(th[i], p);
+  }
+  reduce_finish<1>(v, partials, st, kStageDot, 0, 0);
+}
+
+// g = dJ/dtheta = w * theta^(p-1) * J^(1-p), J = dot1^(1/p)
+__global__ void __launch_bounds__(256) k_adj_rhs(long long n, const double* __restrict__ th,
+                                                  const double* __restrict__ w, double p,
+                                                  const SolverState* __restrict__ st, double* __restrict__ g) {
+  pdl_enter();
+  const double J = pow(st->dot1, 1.0 / p), sc = pow(J, 1.0 - p);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const double wi = w[i];
+    g[i] = wi != 0.0 ? wi * pow(th[i], p - 1.0) * sc : 0.0;
+  }
+}
+
+// Gradients from theta (physical guards) and the adjoint field la (zero guards), A la = g:
+//   dJ/dhsrc_c       = -V_c la_c                        (b = -(hsrc V + ...), calRHS!)
+//   dJ/dln(lambda_c) = -sum over the faces f of c of  c_f w_f (theta_q - theta_c)(la_c - la_q)
+// with c_f the face conductance (the operator's tables) and w_f = d ln c_f / d ln lambda_c =
+// lambda_q / (lambda_c + lambda_q) for a neighbour with its own lambda, 1 for a guard (a guard's
+// lambda is 0, or a copy of lambda_c on an isothermal face, boundary_conditions.jl:198-205).
+// One thread per interior cell.
+__global__ void __launch_bounds__(256) k_adj_grad(OpParams<double> op, const double* __restrict__ lamv,
+                                                   const double* __restrict__ th, const double* __restrict__ la,
+                                                   double* __restrict__ G, double* __restrict__ gh) {
+  const Geo& g = op.g;
+  const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = 1 + blockIdx.y, k = 1 + blockIdx.z;
+  if (i > g.NX) return;
+  const int o = g.off(i, j, k);
+  const int nb[6] = {g.off(i - 1, j, k), g.off(i + 1, j, k), g.off(i, j - 1, k),
+                     g.off(i, j + 1, k), g.off(i, j, k - 1), g.off(i, j, k + 1)};
+  const uint8_t k0 = op.key[o];
+  uint8_t kn[6];
+#pragma unroll
+  for (int f = 0; f < 6; ++f) kn[f] = op.key[nb[f]];
+  Coef<double> c;
+  if (!cell_coef(op, k, k0, kn[0], kn[1], kn[2], kn[3], kn[4], kn[5], o, c)) {
+    G[o] = 0.0;
+    gh[o] = 0.0;
+    return;
+  }
+  const double cf[6] = {c.cxm, c.cxp, c.cym, c.cyp, c.czm, c.czp};
+  const double lp = lamv[k0 & 0x7f], tp = th[o], ap = la[o];
+  double s = 0.0;
+#pragma unroll
+  for (int f = 0; f < 6; ++f) {
+    if (cf[f] == 0.0) continue;
+    const bool guard = !(kn[f] & 0x80);
+    const double lq = lamv[kn[f] & 0x7f];
+    const double wf = guard ? 1.0 : lq / (lp + lq);
+    const double aq = guard ? 0.0 : la[nb[f]];
+    s += cf[f] * wf * (th[nb[f]] - tp) * (ap - aq);
+  }
+  G[o] = -s;
+  gh[o] = -(op.dx0 * op.dy0 * __ldg(op.dzk + k)) * ap;
+}
+
+// ------------------------------------------------------------------------------------------
 // Material keys.  Pass 1 collects the distinct lambda bit patterns into a small open-addressing
 // table and validates the fields; pass 2 writes key = index | mask << 7 in the device layout
 // (and rho*cp for transient grids).

@@ -115,6 +115,8 @@ struct Solver {
   double* hsrc = nullptr;      // heat source per cell (device layout), set by h2g_set_hsrc
   double* stats = nullptr;     // per-step theta statistics of the transient driver
   int stats_cap = 0;
+  double* adj[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // adjoint: w, g, la, G, dJ/dhsrc
+  double* lamv = nullptr;      // lambda value of every material key (adjoint gradient)
   // Krylov vectors in working precision: r, r0, p, ph, q, s, sh, t (+ e for refinement)
   void* kv[10] = {nullptr};
   void* hook[2] = {nullptr, nullptr};  // scratch of the single-kernel entry points (never a Krylov vector)
@@ -249,6 +251,8 @@ static void destroy(Solver* s) {
   cudaFree(s->rc64); cudaFree(s->rc32);
   cudaFree(s->th); cudaFree(s->b); cudaFree(s->th_snap); cudaFree(s->r64);
   cudaFree(s->hsrc); cudaFree(s->stats);
+  for (auto& p : s->adj) cudaFree(p);
+  cudaFree(s->lamv);
   for (auto& p : s->kv) cudaFree(p);
   for (auto& p : s->hook) cudaFree(p);
   for (auto& p : s->stage) cudaFree(p);
@@ -1012,6 +1016,66 @@ static int transient(Solver* s, const FaceBC& f, int nt, int method, double tol,
   return last;
 }
 
+// ---- steady adjoint -------------------------------------------------------------------------
+// Forward solve, J = (sum w theta^p)^(1/p), adjoint solve A la = dJ/dtheta with the same solver
+// (the operator is symmetric: lambda_f is symmetric in its arguments and every face area and
+// distance is shared by the two cells of the face), then the gradients.
+static int adjoint(Solver* s, const double* w_host, double p, double tol, int maxItr, int smoother, double* J,
+                   double* dJ_dhsrc, double* dJ_dlnlam, h2g_result* out_fwd, h2g_result* out_adj) {
+  if (!s->grid_set || !s->fields_set) return fail(H2G_BAD_ARG, "h2g_set_grid and h2g_set_fields must come first");
+  if (!w_host || !J) return fail(H2G_BAD_ARG, "null weights or J");
+  if (!(p >= 1.0)) return fail(H2G_BAD_ARG, "p must be >= 1");
+  const Geo& g = s->g;
+  const size_t nb = sizeof(double) * (size_t)g.n;
+  for (auto& q : s->adj)
+    if (!q) {
+      CK(cudaMalloc(&q, nb));
+      CK(cudaMemsetAsync(q, 0, nb, s->stream));
+    }
+  double *W = s->adj[0], *gv = s->adj[1], *la = s->adj[2], *G = s->adj[3], *gh = s->adj[4];
+  int rc = upload<double>(s, w_host, W);
+  if (rc) return rc;
+  // forward
+  h2g_result rf{};
+  int st = solve(s, false, tol, maxItr, smoother, 0, nullptr, &rf);
+  if (out_fwd) *out_fwd = rf;
+  if (st != H2G_OK) return st;
+  // objective and adjoint right-hand side
+  if ((rc = prime_state(s, s->st, tol, maxItr, s->hist, maxItr))) return rc;
+  launch(s, k_objective, elementwise_blocks(s), 256, s->stream, g.n, (const double*)s->th, (const double*)W, p,
+         s->st, s->partials);
+  launch(s, k_adj_rhs, elementwise_blocks(s), 256, s->stream, g.n, (const double*)s->th, (const double*)W, p,
+         (const SolverState*)s->st, gv);
+  CKL();
+  CK(cudaMemcpyAsync(s->st_host, s->st, sizeof(SolverState), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaMemsetAsync(la, 0, nb, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  const double sum = s->st_host->dot1;
+  *J = pow(sum, 1.0 / p);
+  if (!(sum > 0.0) || !std::isfinite(sum)) return fail(H2G_NONFINITE, "objective sum %g", sum);
+  // adjoint solve on (la, g) in place of (theta, b)
+  std::swap(s->th, la);
+  std::swap(s->b, gv);
+  h2g_result ra{};
+  st = solve(s, false, tol, maxItr, smoother, 0, nullptr, &ra);
+  std::swap(s->th, la);
+  std::swap(s->b, gv);
+  if (out_adj) *out_adj = ra;
+  if (st != H2G_OK) return st;
+  // gradients
+  if (!s->lamv) CK(cudaMalloc(&s->lamv, sizeof(double) * kMaxKeys));
+  CK(cudaMemcpyAsync(s->lamv, s->lam_values.data(), sizeof(double) * s->lam_values.size(), cudaMemcpyHostToDevice,
+                     s->stream));
+  const OpParams<double> op = op_params<double>(s, s->t64);
+  dim3 grid((g.NX + 127) / 128, g.NY, g.NZ);
+  k_adj_grad<<<grid, 128, 0, s->stream>>>(op, s->lamv, s->th, la, G, gh);
+  CKL();
+  if (dJ_dlnlam && (rc = download<double>(s, G, dJ_dlnlam))) return rc;
+  if (dJ_dhsrc && (rc = download<double>(s, gh, dJ_dhsrc))) return rc;
+  CK(cudaStreamSynchronize(s->stream));
+  return H2G_OK;
+}
+
 static int create(int MX, int MY, int MZ, int precision, Solver** out) {
   if (!out) return fail(H2G_BAD_ARG, "null output pointer");
   *out = nullptr;
@@ -1516,6 +1580,12 @@ int h2g_batch_solve(int n, h2g_solver* const* hs, int method, double tol, int ma
     if (st != H2G_OK && worst == H2G_OK) worst = st;
   }
   return worst;
+}
+
+int h2g_adjoint(h2g_solver* h, const double* weights, double p, double tol, int maxItr, int smoother, double* J,
+                double* dJ_dhsrc, double* dJ_dlnlam, h2g_result* out_fwd, h2g_result* out_adj) {
+  if (int rc = h2g::check_handle(h)) return rc;
+  return h2g::adjoint(S(h), weights, p, tol, maxItr, smoother, J, dJ_dhsrc, dJ_dlnlam, out_fwd, out_adj);
 }
 
 int h2g_release_cached(void) {

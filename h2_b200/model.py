@@ -175,14 +175,18 @@ class Model:
 
 def build_mode3(NX: int, NY: int | None = None, NZ: int = 30, *, is_steady: bool = True, dt: float = 1.0e4,
                 theta_init: float = 300.0, symmetric: bool = False, ID: np.ndarray | None = None,
-                hsrc: np.ndarray | None = None) -> Model:
-    """q3d's set-up (heat3ds.jl:193-230 and main 113-128) for the Mode-3 IC stack."""
+                hsrc: np.ndarray | None = None, lam_scale: np.ndarray | None = None) -> Model:
+    """q3d's set-up (heat3ds.jl:193-230 and main 113-128) for the Mode-3 IC stack.
+    lam_scale (MZ factors, optional) multiplies the conductivity of every interior cell of plane
+    k before the boundary conditions copy it into isothermal guards."""
     NY = NX if NY is None else NY
     Z, ZC, dZ = zgrid(NZ)
     if ID is None:
         ID = fill_id(NX, NY, NZ)
     wk = WorkBuffers.allocate(NX + 2, NY + 2, NZ + 2)
     set_properties(wk, ID)
+    if lam_scale is not None:
+        wk.lam[1:-1, 1:-1, 1:-1] *= np.asarray(lam_scale, dtype=np.float64)[None, None, 1:-1]
     bcs = mode3_bc(symmetric)
     wk.theta[...] = theta_init
     apply_boundary_conditions(wk, bcs)

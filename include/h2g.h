@@ -164,6 +164,18 @@ int h2g_release_cached(void);
 int h2g_batch_solve(int n, h2g_solver *const *hs, int method, double tol, int maxItr, int smoother, int threads,
                     h2g_result *outs);
 
+/* ---- steady adjoint (no reference counterpart) -------------------------------------------
+ * Gradient of J = (sum_c w_c θ_c^p)^(1/p) (w_c >= 0 per cell, column-major with guards, e.g.
+ * the cell volume on the silicon cells and 0 elsewhere; p >= 1) where θ solves the handle's
+ * current system A θ = b: PBiCGSTAB! from the handle's θ to tol (θ is left at the solution),
+ * then one adjoint solve A λa = dJ/dθ with the same solver (A is symmetric), then
+ *   dJ_dhsrc[c]  = -V_c λa_c                  (b = -(hsrc·V + ...), calRHS!)
+ *   dJ_dlnlam[c] = dJ / d ln λ_c              (λ_c scaled with its isothermal guard copy)
+ * as column-major host arrays (nullable; guards 0).  out_fwd / out_adj (nullable) receive the
+ * two solves' results. */
+int h2g_adjoint(h2g_solver *h, const double *weights, double p, double tol, int maxItr, int smoother, double *J,
+                double *dJ_dhsrc, double *dJ_dlnlam, h2g_result *out_fwd, h2g_result *out_adj);
+
 /* ---- right-hand side and time stepping ---------------------------------------------------
  * wk.hsrc (src/common.jl:64, filled by HeatSrc!): volumetric heat source in W/m^3, guard layers
  * included.  A handle without one uses zero. */
