@@ -85,3 +85,22 @@ def steady_gradient(s: Solver, weights: np.ndarray, p: float = 8.0, tol: float =
                            smoother_selector(smoother), C.byref(J), _ptr(gh), _ptr(gl), C.byref(rf), C.byref(ra))
     L.check(st)
     return J.value, gh, gl, rf, ra
+
+
+def transient_gradient(s: Solver, bcs, nt: int, weights: np.ndarray, p: float = 8.0, tol: float = 1e-10,
+                       maxItr: int = 20_000, smoother: str = "gs", checkpoint_every: int = 0):
+    """h2g_adjoint_transient: J on theta after nt implicit steps of the transient model (grid set
+    with is_steady=False, rho and cp, hsrc set) and its gradients summed over the steps.
+    checkpoint_every = 0 picks ceil(sqrt(nt)).  Returns (J, dJ_dhsrc, dJ_dlnlam, Result)."""
+    from .nonuniform import bc_array
+    k = int(checkpoint_every) or max(1, int(np.ceil(np.sqrt(nt))))
+    w = np.asfortranarray(weights, dtype=np.float64)
+    J = C.c_double()
+    gh = np.zeros(s.shape, order="F")
+    gl = np.zeros(s.shape, order="F")
+    res = L.Result()
+    st = s.lib.h2g_adjoint_transient(s.h, bc_array(bcs), int(nt), _ptr(s._arr(w, "weights")), float(p), float(tol),
+                                     int(maxItr), smoother_selector(smoother), k, C.byref(J), _ptr(gh), _ptr(gl),
+                                     C.byref(res))
+    L.check(st)
+    return J.value, gh, gl, res

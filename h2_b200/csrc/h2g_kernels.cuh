@@ -1174,7 +1174,7 @@ __global__ void __launch_bounds__(256) k_adj_rhs(long long n, const double* __re
 // One thread per interior cell.
 __global__ void __launch_bounds__(256) k_adj_grad(OpParams<double> op, const double* __restrict__ lamv,
                                                    const double* __restrict__ th, const double* __restrict__ la,
-                                                   double* __restrict__ G, double* __restrict__ gh) {
+                                                   double* __restrict__ G, double* __restrict__ gh, int acc) {
   const Geo& g = op.g;
   const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = 1 + blockIdx.y, k = 1 + blockIdx.z;
@@ -1188,8 +1188,10 @@ __global__ void __launch_bounds__(256) k_adj_grad(OpParams<double> op, const dou
   for (int f = 0; f < 6; ++f) kn[f] = op.key[nb[f]];
   Coef<double> c;
   if (!cell_coef(op, k, k0, kn[0], kn[1], kn[2], kn[3], kn[4], kn[5], o, c)) {
-    G[o] = 0.0;
-    gh[o] = 0.0;
+    if (!acc) {
+      G[o] = 0.0;
+      gh[o] = 0.0;
+    }
     return;
   }
   const double cf[6] = {c.cxm, c.cxp, c.cym, c.cyp, c.czm, c.czp};
@@ -1204,8 +1206,30 @@ __global__ void __launch_bounds__(256) k_adj_grad(OpParams<double> op, const dou
     const double aq = guard ? 0.0 : la[nb[f]];
     s += cf[f] * wf * (th[nb[f]] - tp) * (ap - aq);
   }
-  G[o] = -s;
-  gh[o] = -(op.dx0 * op.dy0 * __ldg(op.dzk + k)) * ap;
+  const double gv = -(op.dx0 * op.dy0 * __ldg(op.dzk + k)) * ap;
+  G[o] = acc ? G[o] - s : -s;
+  gh[o] = acc ? gh[o] + gv : gv;
+}
+
+// Transient adjoint step: the right-hand side of step n+1 depends on theta^n through calRHS!
+// (NonUniform.jl:87-90, RHS.jl:140-186):  db_c/dtheta_c = -a_p0 - sum_{convective minus faces}
+// h*area + sum_{convective plus faces} h*area, so lam^n = (db/dtheta^n) * mu^{n+1} per cell.
+__global__ void __launch_bounds__(256) k_adj_step(Geo g, const double* __restrict__ mu, double* __restrict__ lam,
+                                                   const double* __restrict__ rc, const double* __restrict__ dzk,
+                                                   double dx, double dy, double ddt, FaceBC bc) {
+  const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = 1 + blockIdx.y, k = 1 + blockIdx.z;
+  if (i > g.NX) return;
+  const int o = g.off(i, j, k);
+  const double dz = __ldg(dzk + k);
+  const double ax = dy * dz, ay = dx * dz, az = dx * dy;
+  double d = -(rc[o] * dx * dy * dz * ddt);
+  const bool on[6] = {i == 1, i == g.NX, j == 1, j == g.NY, k == 1, k == g.NZ};
+  const double area[6] = {ax, ax, ay, ay, az, az};
+#pragma unroll
+  for (int f = 0; f < 6; ++f)
+    if (on[f] && bc.type[f] == 2) d += (f & 1) ? bc.h[f] * area[f] : -bc.h[f] * area[f];
+  lam[o] = d * mu[o];
 }
 
 // ------------------------------------------------------------------------------------------

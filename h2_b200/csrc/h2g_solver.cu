@@ -117,6 +117,8 @@ struct Solver {
   int stats_cap = 0;
   double* adj[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // adjoint: w, g, la, G, dJ/dhsrc
   double* lamv = nullptr;      // lambda value of every material key (adjoint gradient)
+  double* tstates = nullptr;   // transient adjoint: checkpoints, segment states, final state
+  size_t tstates_cap = 0;      // in vectors
   // Krylov vectors in working precision: r, r0, p, ph, q, s, sh, t (+ e for refinement)
   void* kv[10] = {nullptr};
   void* hook[2] = {nullptr, nullptr};  // scratch of the single-kernel entry points (never a Krylov vector)
@@ -253,6 +255,7 @@ static void destroy(Solver* s) {
   cudaFree(s->hsrc); cudaFree(s->stats);
   for (auto& p : s->adj) cudaFree(p);
   cudaFree(s->lamv);
+  cudaFree(s->tstates);
   for (auto& p : s->kv) cudaFree(p);
   for (auto& p : s->hook) cudaFree(p);
   for (auto& p : s->stage) cudaFree(p);
@@ -1068,11 +1071,124 @@ static int adjoint(Solver* s, const double* w_host, double p, double tol, int ma
                      s->stream));
   const OpParams<double> op = op_params<double>(s, s->t64);
   dim3 grid((g.NX + 127) / 128, g.NY, g.NZ);
-  k_adj_grad<<<grid, 128, 0, s->stream>>>(op, s->lamv, s->th, la, G, gh);
+  k_adj_grad<<<grid, 128, 0, s->stream>>>(op, s->lamv, s->th, la, G, gh, 0);
   CKL();
   if (dJ_dlnlam && (rc = download<double>(s, G, dJ_dlnlam))) return rc;
   if (dJ_dhsrc && (rc = download<double>(s, gh, dJ_dhsrc))) return rc;
   CK(cudaStreamSynchronize(s->stream));
+  return H2G_OK;
+}
+
+// Transient adjoint of J(theta^N), theta^{n+1} = A^-1 b(theta^n) for nt steps of main()'s loop
+// (b rebuilt from zero each step), with checkpointed recomputation: the forward pass keeps
+// theta at every K-th step; the backward pass recomputes one segment of K states at a time from
+// its checkpoint (the solves are deterministic, so the recomputed states are the same bits), then
+// for n = N-1 .. 0:  mu = A^-1 lam (adjoint solve),  accumulate the gradients of step n with
+// theta^{n+1} and mu,  lam = (db/dtheta^n) mu.  Device memory: ceil(nt/K) + K + 1 states.
+static int adjoint_transient(Solver* s, const FaceBC& f, int nt, const double* w_host, double p, double tol,
+                             int maxItr, int smoother, int K, double* J, double* dJ_dhsrc, double* dJ_dlnlam,
+                             h2g_result* out) {
+  if (!s->grid_set || !s->fields_set) return fail(H2G_BAD_ARG, "h2g_set_grid and h2g_set_fields must come first");
+  if (s->steady || !s->rc64) return fail(H2G_BAD_ARG, "the transient adjoint needs a transient grid with rho and cp");
+  if (nt < 1 || K < 1) return fail(H2G_BAD_ARG, "nt and checkpoint_every must be >= 1");
+  if (!w_host || !J) return fail(H2G_BAD_ARG, "null weights or J");
+  if (!(p >= 1.0)) return fail(H2G_BAD_ARG, "p must be >= 1");
+  K = std::min(K, nt);
+  const Geo& g = s->g;
+  const size_t n = (size_t)g.n, nb = sizeof(double) * n;
+  const int ncp = (nt + K - 1) / K;
+  const size_t need = (size_t)ncp + (size_t)K + 1;
+  int rc = ensure_hsrc(s);
+  if (rc) return rc;
+  for (auto& q : s->adj)
+    if (!q) {
+      CK(cudaMalloc(&q, nb));
+      CK(cudaMemsetAsync(q, 0, nb, s->stream));
+    }
+  if (s->tstates_cap < need) {
+    cudaFree(s->tstates);
+    s->tstates = nullptr;
+    s->tstates_cap = 0;
+    CK(cudaMalloc(&s->tstates, nb * need));
+    s->tstates_cap = need;
+  }
+  double* cp = s->tstates;              // checkpoints: theta^{cK}
+  double* seg = s->tstates + n * ncp;   // theta^{n0+1} .. theta^{n0+K}
+  double* fin = seg + n * (size_t)K;    // theta^N
+  double *W = s->adj[0], *lam = s->adj[1], *G = s->adj[3], *gh = s->adj[4];
+  if ((rc = upload<double>(s, w_host, W))) return rc;
+  if (!s->lamv) CK(cudaMalloc(&s->lamv, sizeof(double) * kMaxKeys));
+  CK(cudaMemcpyAsync(s->lamv, s->lam_values.data(), sizeof(double) * s->lam_values.size(), cudaMemcpyHostToDevice,
+                     s->stream));
+  long long itr_total = 0, launches = 0;
+  auto step = [&](int nstep) -> int {
+    int r2 = calrhs(s, f, 1);
+    if (r2) return r2;
+    h2g_result r{};
+    const int st = solve(s, false, tol, maxItr, smoother, 0, nullptr, &r);
+    itr_total += r.itr;
+    launches += r.launches + 1;
+    if (st != H2G_OK) return fail(st, "forward step %d: %s", nstep + 1, h2g_status_string(st));
+    return H2G_OK;
+  };
+  // forward pass
+  for (int q = 0; q < nt; ++q) {
+    if (q % K == 0) CK(cudaMemcpyAsync(cp + n * (size_t)(q / K), s->th, nb, cudaMemcpyDeviceToDevice, s->stream));
+    if ((rc = step(q))) return rc;
+  }
+  CK(cudaMemcpyAsync(fin, s->th, nb, cudaMemcpyDeviceToDevice, s->stream));
+  // objective and lam^N = dJ/dtheta^N
+  if ((rc = prime_state(s, s->st, tol, maxItr, s->hist, maxItr))) return rc;
+  launch(s, k_objective, elementwise_blocks(s), 256, s->stream, g.n, (const double*)s->th, (const double*)W, p,
+         s->st, s->partials);
+  launch(s, k_adj_rhs, elementwise_blocks(s), 256, s->stream, g.n, (const double*)s->th, (const double*)W, p,
+         (const SolverState*)s->st, lam);
+  CKL();
+  CK(cudaMemcpyAsync(s->st_host, s->st, sizeof(SolverState), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaMemsetAsync(G, 0, nb, s->stream));
+  CK(cudaMemsetAsync(gh, 0, nb, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  const double sum = s->st_host->dot1;
+  *J = pow(sum, 1.0 / p);
+  if (!(sum > 0.0) || !std::isfinite(sum)) return fail(H2G_NONFINITE, "objective sum %g", sum);
+  const OpParams<double> op = op_params<double>(s, s->t64);
+  const dim3 cgrid((g.NX + 127) / 128, g.NY, g.NZ);
+  const double ddt = 1.0 / s->dt;
+  // backward pass, one segment at a time
+  for (int c = ncp - 1; c >= 0; --c) {
+    const int n0 = c * K, n1 = std::min(n0 + K, nt);
+    CK(cudaMemcpyAsync(s->th, cp + n * (size_t)c, nb, cudaMemcpyDeviceToDevice, s->stream));
+    for (int q = n0; q < n1; ++q) {
+      if ((rc = step(q))) return rc;
+      CK(cudaMemcpyAsync(seg + n * (size_t)(q - n0), s->th, nb, cudaMemcpyDeviceToDevice, s->stream));
+    }
+    for (int q = n1 - 1; q >= n0; --q) {
+      // mu = A^-1 lam, solved in the handle's theta / b
+      CK(cudaMemsetAsync(s->th, 0, nb, s->stream));
+      CK(cudaMemcpyAsync(s->b, lam, nb, cudaMemcpyDeviceToDevice, s->stream));
+      h2g_result r{};
+      const int st = solve(s, false, tol, maxItr, smoother, 0, nullptr, &r);
+      itr_total += r.itr;
+      launches += r.launches + 2;
+      if (st != H2G_OK) return fail(st, "adjoint step %d: %s", q + 1, h2g_status_string(st));
+      k_adj_grad<<<cgrid, 128, 0, s->stream>>>(op, s->lamv, seg + n * (size_t)(q - n0), s->th, G, gh, 1);
+      k_adj_step<<<cgrid, 128, 0, s->stream>>>(g, s->th, lam, s->rc64, s->t64.dzk, s->dx, s->dy, ddt, f);
+      CKL();
+    }
+  }
+  CK(cudaMemcpyAsync(s->th, fin, nb, cudaMemcpyDeviceToDevice, s->stream));
+  if (dJ_dlnlam && (rc = download<double>(s, G, dJ_dlnlam))) return rc;
+  if (dJ_dhsrc && (rc = download<double>(s, gh, dJ_dhsrc))) return rc;
+  CK(cudaStreamSynchronize(s->stream));
+  if (out) {
+    out->isconverged = 1;
+    out->itr = (int)std::min<long long>(itr_total, 2147483647LL);
+    out->outer = nt;
+    out->status = H2G_OK;
+    out->res0 = 0.0;
+    out->res = 0.0;
+    out->launches = launches;
+  }
   return H2G_OK;
 }
 
@@ -1586,6 +1702,16 @@ int h2g_adjoint(h2g_solver* h, const double* weights, double p, double tol, int 
                 double* dJ_dhsrc, double* dJ_dlnlam, h2g_result* out_fwd, h2g_result* out_adj) {
   if (int rc = h2g::check_handle(h)) return rc;
   return h2g::adjoint(S(h), weights, p, tol, maxItr, smoother, J, dJ_dhsrc, dJ_dlnlam, out_fwd, out_adj);
+}
+
+int h2g_adjoint_transient(h2g_solver* h, const h2g_bc* bc, int nt, const double* weights, double p, double tol,
+                          int maxItr, int smoother, int checkpoint_every, double* J, double* dJ_dhsrc,
+                          double* dJ_dlnlam, h2g_result* out) {
+  if (int rc = h2g::check_handle(h)) return rc;
+  h2g::FaceBC f;
+  if (int rc = h2g::face_bc(bc, f)) return rc;
+  return h2g::adjoint_transient(S(h), f, nt, weights, p, tol, maxItr, smoother, checkpoint_every, J, dJ_dhsrc,
+                                dJ_dlnlam, out);
 }
 
 int h2g_release_cached(void) {

@@ -176,6 +176,17 @@ int h2g_batch_solve(int n, h2g_solver *const *hs, int method, double tol, int ma
 int h2g_adjoint(h2g_solver *h, const double *weights, double p, double tol, int maxItr, int smoother, double *J,
                 double *dJ_dhsrc, double *dJ_dlnlam, h2g_result *out_fwd, h2g_result *out_adj);
 
+/* Transient form (no reference counterpart): J = (sum_c w_c θ_c^p)^(1/p) on θ after nt steps of
+ * h2g_transient (b rebuilt per step, PBiCGSTAB! from the previous θ; transient grid with ρ, cp
+ * and the handle's hsrc, boundary set bc[6]), from the handle's θ as θ^0.  Gradients summed over
+ * the steps, through the adjoint recursion mu = A^-1 lam, lam <- (db/dθ) mu.  The forward states
+ * are kept every checkpoint_every steps and recomputed per segment (device memory:
+ * ceil(nt/checkpoint_every) + checkpoint_every + 1 state vectors).  θ is left at θ^nt.  out.itr
+ * counts the iterations of all forward, recomputed and adjoint solves. */
+int h2g_adjoint_transient(h2g_solver *h, const h2g_bc *bc, int nt, const double *weights, double p, double tol,
+                          int maxItr, int smoother, int checkpoint_every, double *J, double *dJ_dhsrc,
+                          double *dJ_dlnlam, h2g_result *out);
+
 /* ---- right-hand side and time stepping ---------------------------------------------------
  * wk.hsrc (src/common.jl:64, filled by HeatSrc!): volumetric heat source in W/m^3, guard layers
  * included.  A handle without one uses zero. */
