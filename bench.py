@@ -57,6 +57,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch", type=int, default=64, help="members of the batched workload (0 = skip)")
     ap.add_argument("--batch-steps", type=int, default=2)
+    ap.add_argument("--adjoint-steps", type=int, default=200,
+                    help="implicit steps of the timed transient adjoint (0 = skip the adjoint section)")
     return ap.parse_args()
 
 
@@ -370,6 +372,7 @@ def run_ours(a, dist: Dist):
         log("e2e failed:", e)
 
     batch = run_batch(a, dist, torch, stream, flush) if a.batch > 0 else None
+    adjoint = run_adjoint(a, dist, torch, stream) if a.adjoint_steps > 0 else None
 
     cpu = None
     if dist.rank == 0 and dist.world == 1 and not a.no_cpu_baseline:
@@ -417,6 +420,7 @@ def run_ours(a, dist: Dist):
                      "algorithmic_bytes": rm["bytes"], "seconds": rm["seconds"], "peak_kind": peak_kind},
         "kernels": {f"{k[0]}_{k[1]}": v for k, v in roof.items()},
         "batch": batch,
+        "adjoint": adjoint,
         "cpu_baseline": cpu,
         "e2e": e2e,
         "gpu_launches": f64["launches"],
@@ -479,6 +483,68 @@ def run_batch(a, dist, torch, stream, flush):
         return out
     finally:
         bs.close()
+
+
+def run_adjoint(a, dist, torch, stream):
+    """Gradients of J = (sum_silicon V theta^8)^(1/8) on the benchmark grid: the steady adjoint
+    (forward + adjoint solve, to 1e-10) and the transient adjoint (a.adjoint_steps implicit steps
+    of dt = 1e-4 s with checkpointed recomputation, to 1e-10).  CUDA events around each call."""
+    import h2_b200
+    from h2_b200 import adjoint as A
+    from h2_b200 import model as M
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        out = fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) * 1e-3, out
+
+    out = {}
+    m = M.build_mode3(a.nx, a.nx, a.nz)
+    w = m.wk
+    wts = A.silicon_weights(m.ID, m.dx, m.dy, m.dZ)
+    s = h2_b200.Solver(*m.shape, stream=stream.cuda_stream)
+    try:
+        s.set_grid(m.ZC, m.dZ, m.dx, m.dy, m.dt, m.HC, True)
+        s.set_fields(w.lam, w.mask)
+        s.set_rhs(w.b)
+        s.set_theta(w.theta)
+        s.snapshot()
+        ts = []
+        for r in range(3):
+            s.snapshot(restore=True)
+            dt_, (J, _, _, rf, ra) = timed(lambda: A.steady_gradient(s, wts, 8.0, tol=1e-10))
+            if r:
+                ts.append(dt_)
+        out["steady"] = {"seconds": dist.max(float(np.mean(ts))), "J": J, "forward_iterations": rf.itr,
+                         "adjoint_iterations": ra.itr, "tol": 1e-10}
+    finally:
+        s.close()
+    nt = a.adjoint_steps
+    mt = M.build_mode3(a.nx, a.nx, a.nz, is_steady=False, dt=1e-4)
+    w = mt.wk
+    s = h2_b200.Solver(*mt.shape, stream=stream.cuda_stream)
+    try:
+        s.set_grid(mt.ZC, mt.dZ, mt.dx, mt.dy, mt.dt, mt.HC, False)
+        s.set_fields(w.lam, w.mask, w.rho, w.cp)
+        s.set_rhs(w.b)
+        s.set_theta(w.theta)
+        s.set_hsrc(w.hsrc)
+        s.snapshot()
+        t_fwd, (st, res, stats) = timed(lambda: s.transient(mt.bcs, nt, tol=1e-10, smoother="gs"))
+        s.snapshot(restore=True)
+        k = max(1, int(np.ceil(np.sqrt(nt))))
+        t_adj, (J, _, _, r) = timed(lambda: A.transient_gradient(s, mt.bcs, nt, wts, 8.0, tol=1e-10,
+                                                                 checkpoint_every=k))
+        out["transient"] = {"steps": nt, "dt": 1e-4, "seconds": dist.max(t_adj), "forward_only_seconds": t_fwd,
+                            "J": J, "iterations_total": r.itr, "forward_iterations": int(stats[:, 3].sum()),
+                            "checkpoint_every": k, "tol": 1e-10}
+    finally:
+        s.close()
+    out["objective"] = "(sum over silicon cells of V theta^8)^(1/8); gradients w.r.t. hsrc per cell and ln lambda"
+    return out
 
 
 def main():
