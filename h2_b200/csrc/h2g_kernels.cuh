@@ -457,13 +457,19 @@ __device__ __forceinline__ double rb_pass_column(const OpParams<T>& op, T* x, co
   return acc;
 }
 
-template <typename T>
-__global__ void __launch_bounds__(kThreads, H2G_MINB) k_rb_pass(OpParams<T> op, T* x, const T* __restrict__ bb, int color,
-                                                       T omega, const SolverState* __restrict__ st) {
+// The colour pass has no reduction, so its block height BY (rows per block) does not change any
+// result; the autotuner picks it per grid among kRbRows.  Every shape keeps the register cap of
+// H2G_MINB blocks of 256 threads per SM.
+constexpr int kRbRows[4] = {2, 4, 8, 16};
+
+template <typename T, int BY = kBY>
+__global__ void __launch_bounds__(kBX * BY, (H2G_MINB * kBY) / BY)
+    k_rb_pass(OpParams<T> op, T* x, const T* __restrict__ bb, int color, T omega,
+              const SolverState* __restrict__ st) {
   pdl_enter();
   if (st && st->stop) return;
   const int lane = threadIdx.x, p = blockIdx.x * kBX + lane;
-  const int j = 1 + blockIdx.y * kBY + threadIdx.y;
+  const int j = 1 + blockIdx.y * BY + threadIdx.y;
   const int k0 = 1 + 2 * blockIdx.z;
   if (j > op.g.NY) return;  // uniform per warp
   rb_pass_column<T, false>(op, x, bb, color, omega, lane, p, j, k0);
@@ -1230,6 +1236,13 @@ __global__ void __launch_bounds__(256) k_adj_step(Geo g, const double* __restric
   for (int f = 0; f < 6; ++f)
     if (on[f] && bc.type[f] == 2) d += (f & 1) ? bc.h[f] * area[f] : -bc.h[f] * area[f];
   lam[o] = d * mu[o];
+}
+
+// a[i] = v over a whole vector (scratch contents for the launch-shape tuner)
+template <typename T>
+__global__ void __launch_bounds__(256) k_fill_const(long long n, T* __restrict__ a, T v) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    a[i] = v;
 }
 
 // ------------------------------------------------------------------------------------------

@@ -9,7 +9,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <atomic>
+#include <map>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -139,6 +141,8 @@ struct Solver {
   int max_outer = 40;
   bool no_cond = false;
   bool pdl = true;  // programmatic dependent launch of the solver kernels
+  int rb_rows = kBY;      // rows per block of the colour pass (autotuned)
+  bool rb_tuned = false;  // rb_rows chosen (by the tuner or h2g_set_tuning)
 
   long long nfort() const { return (long long)g.MX * g.MY * g.MZ; }
 };
@@ -173,11 +177,27 @@ static void launch(const Solver* s, void (*kern)(KArgs...), dim3 grid, dim3 bloc
 }
 static int elementwise_blocks(const Solver* s) { return s->num_sms * 4; }
 
+
 // Grids of the stencil kernels: columns (p, j) in 32 x kBY blocks; the RB passes take two planes
 // per thread, CalcAX / CalcRK / the first pass one plane (both colours).
-static dim3 rb_grid(const Geo& g) { return dim3((g.HN + kBX - 1) / kBX, (g.NY + kBY - 1) / kBY, (g.NZ + 1) / 2); }
+static dim3 rb_grid(const Geo& g, int by = kBY) {
+  return dim3((g.HN + kBX - 1) / kBX, (g.NY + by - 1) / by, (g.NZ + 1) / 2);
+}
 static dim3 ax_grid(const Geo& g) { return dim3((g.HN + kBX - 1) / kBX, (g.NY + kBY - 1) / kBY, g.NZ); }
 static dim3 first_grid(const Geo& g) { return ax_grid(g); }
+
+// One colour pass with the handle's block height.
+template <typename T>
+static void launch_rb(const Solver* s, cudaStream_t cs, const OpParams<T>& op, T* x, const T* bb, int color, T omega,
+                      const SolverState* st) {
+  const Geo& g = op.g;
+  switch (s->rb_rows) {
+    case 2: launch(s, k_rb_pass<T, 2>, rb_grid(g, 2), dim3(kBX, 2), cs, op, x, bb, color, omega, st); break;
+    case 4: launch(s, k_rb_pass<T, 4>, rb_grid(g, 4), dim3(kBX, 4), cs, op, x, bb, color, omega, st); break;
+    case 16: launch(s, k_rb_pass<T, 16>, rb_grid(g, 16), dim3(kBX, 16), cs, op, x, bb, color, omega, st); break;
+    default: launch(s, k_rb_pass<T, 8>, rb_grid(g, 8), dim3(kBX, 8), cs, op, x, bb, color, omega, st); break;
+  }
+}
 
 static size_t partials_needed(const Solver* s) {
   dim3 a = ax_grid(s->g);
@@ -407,14 +427,14 @@ static void launch_pbicg_body(Solver* s, cudaStream_t cs, const OpParams<T>& opA
   launch(s, k_rb_first<TP, T, 1>, first_grid(g), blk, cs, opM, ph, p, bbm, r, q, st, none);
   if (!none)
     for (int pass = 1; pass < 2 * kSweeps; ++pass)
-      launch(s, k_rb_pass<TP>, rg, blk, cs, opM, ph, bbm ? bbm : reinterpret_cast<TP*>(p), pass & 1, TP(1), st);
+      launch_rb<TP>(s, cs, opM, ph, bbm ? bbm : reinterpret_cast<TP*>(p), pass & 1, TP(1), st);
   // q = A p_;  alpha = rho / (q, r0)                            NonUniform.jl:307-309
   launch(s, k_ax<T, 1, TP>, ag, blk, cs, opA, q, ph, r0, nullptr, st, s->partials, kStageAlpha);
   // s = r - alpha q; s_ = M^-1 s                                NonUniform.jl:310-315
   launch(s, k_rb_first<TP, T, 2>, first_grid(g), blk, cs, opM, sh, sv, bbm, r, q, st, none);
   if (!none)
     for (int pass = 1; pass < 2 * kSweeps; ++pass)
-      launch(s, k_rb_pass<TP>, rg, blk, cs, opM, sh, bbm ? bbm : reinterpret_cast<TP*>(sv), pass & 1, TP(1), st);
+      launch_rb<TP>(s, cs, opM, sh, bbm ? bbm : reinterpret_cast<TP*>(sv), pass & 1, TP(1), st);
   // t = A s_; omega = (t,s)/(t,t)                               NonUniform.jl:317-326
   launch(s, k_ax<T, 2, TP>, ag, blk, cs, opA, t, sh, nullptr, sv, st, s->partials, kStageOmega);
   // x += alpha p_ + omega s_; r = s - omega t; res; next rho    NonUniform.jl:328-346
@@ -433,7 +453,7 @@ static void launch_precond_r(Solver* s, cudaStream_t cs, const OpParams<TP>& opM
   launch(s, k_rb_first<TP, T, 0>, first_grid(g), blk, cs, opM, z, r, bbm, nullptr, nullptr, st, none);
   if (!none)
     for (int pass = 1; pass < 2 * kSweeps; ++pass)
-      launch(s, k_rb_pass<TP>, rg, blk, cs, opM, z, bbm ? bbm : reinterpret_cast<TP*>(r), pass & 1, TP(1), st);
+      launch_rb<TP>(s, cs, opM, z, bbm ? bbm : reinterpret_cast<TP*>(r), pass & 1, TP(1), st);
 }
 
 template <typename T, typename TX, typename TP>
@@ -847,6 +867,8 @@ static int solve_mixed(Solver* s, bool cg, double tol, int maxItr, int smoother,
   return status;
 }
 
+static int autotune(Solver* s);
+
 static int solve(Solver* s, bool cg, double tol, int maxItr, int smoother, int verbose, double* res_hist,
                  h2g_result* out) {
   if (!s->grid_set || !s->fields_set) return fail(H2G_BAD_ARG, "h2g_set_grid and h2g_set_fields must come first");
@@ -855,6 +877,7 @@ static int solve(Solver* s, bool cg, double tol, int maxItr, int smoother, int v
     return fail(H2G_BAD_ARG, "Unsupported smoother: %d. Use none (0) or gs (1)", smoother);
   if (!(tol >= 0.0) || !std::isfinite(tol)) return fail(H2G_BAD_ARG, "bad tolerance");
   CK(cudaSetDevice(s->device));
+  if (int rc = autotune(s)) return rc;
   if (s->precision == H2G_MIXED_IR) return solve_ir(s, cg, tol, maxItr, smoother, verbose, res_hist, out);
   if (s->precision == H2G_MIXED) return solve_mixed(s, cg, tol, maxItr, smoother, verbose, res_hist, out);
   return solve_krylov<double>(s, cg, tol, maxItr, smoother, verbose, res_hist, out);
@@ -874,6 +897,7 @@ static int solve_sor(Solver* s, double omega, double tol, int maxItr, int verbos
   if (!(omega > 0.0 && omega < 2.0)) return fail(H2G_BAD_ARG, "omega must lie in (0, 2)");
   const Geo& g = s->g;
   int rc = ensure_hist(s, maxItr);
+  if (rc) return rc;
   if (rc) return rc;
   const OpParams<double> op = op_params<double>(s, s->t64);
   SolverState* st = s->st;
@@ -1192,6 +1216,94 @@ static int adjoint_transient(Solver* s, const FaceBC& f, int nt, const double* w
   return H2G_OK;
 }
 
+// ---- launch-shape tuner --------------------------------------------------------------------
+// The colour pass has no reduction, so its rows per block change no result: the first solve of a
+// handle times every height of kRbRows on the handle's grid (two warm-up and five timed sweeps
+// each, on scratch vectors) and keeps the fastest.  Choices are cached per (grid, smoother
+// precision) for the process; H2G_RB_ROWS in the environment forces one.
+static std::mutex g_tune_mu;
+static std::map<std::array<int, 4>, int> g_tune_cache;
+
+static bool valid_rows(int r) {
+  for (int q : kRbRows)
+    if (q == r) return true;
+  return false;
+}
+
+template <typename T>
+static int tune_rows_t(Solver* s, const OpParams<T>& op, int* best_rows) {
+  const size_t n = (size_t)s->g.n, bytes = sizeof(double) * n;
+  for (auto& p : s->hook)
+    if (!p) CK(cudaMalloc(&p, bytes));
+  T* xa = static_cast<T*>(s->hook[0]);
+  T* xb = static_cast<T*>(s->hook[1]);
+  k_fill_const<T><<<elementwise_blocks(s), 256, 0, s->stream>>>((long long)n, xa, T(300));
+  k_fill_const<T><<<elementwise_blocks(s), 256, 0, s->stream>>>((long long)n, xb, T(-1.0e-3));
+  CKL();
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return fail(H2G_CUDA_ERROR, "event creation failed");
+  }
+  const int saved = s->rb_rows;
+  float best = 1e30f;
+  int rc = H2G_OK;
+  for (int by : kRbRows) {
+    s->rb_rows = by;
+    for (int r = 0; r < 2; ++r) {
+      launch_rb<T>(s, s->stream, op, xa, (const T*)xb, 0, T(1), nullptr);
+      launch_rb<T>(s, s->stream, op, xa, (const T*)xb, 1, T(1), nullptr);
+    }
+    cudaEventRecord(e0, s->stream);
+    for (int r = 0; r < 5; ++r) {
+      launch_rb<T>(s, s->stream, op, xa, (const T*)xb, 0, T(1), nullptr);
+      launch_rb<T>(s, s->stream, op, xa, (const T*)xb, 1, T(1), nullptr);
+    }
+    cudaEventRecord(e1, s->stream);
+    float ms = 0.f;
+    if (cudaGetLastError() != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+        cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+      rc = fail(H2G_CUDA_ERROR, "launch-shape tuning failed");
+      break;
+    }
+    if (ms < best) {
+      best = ms;
+      *best_rows = by;
+    }
+  }
+  s->rb_rows = saved;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return rc;
+}
+
+static int autotune(Solver* s) {
+  if (s->rb_tuned) return H2G_OK;
+  int rows = 0;
+  if (const char* e = getenv("H2G_RB_ROWS")) rows = atoi(e);
+  if (!valid_rows(rows)) {
+    rows = 0;
+    const std::array<int, 4> key = {s->g.MX, s->g.MY, s->g.MZ, s->precision == H2G_FP64 ? 64 : 32};
+    {
+      std::lock_guard<std::mutex> lk(g_tune_mu);
+      auto it = g_tune_cache.find(key);
+      if (it != g_tune_cache.end()) rows = it->second;
+    }
+    if (!rows) {
+      int rc = s->precision == H2G_FP64 ? tune_rows_t<double>(s, op_params<double>(s, s->t64), &rows)
+                                        : tune_rows_t<float>(s, op_params<float>(s, s->t32), &rows);
+      if (rc) return rc;
+      std::lock_guard<std::mutex> lk(g_tune_mu);
+      g_tune_cache[key] = rows;
+    }
+  }
+  if (rows != s->rb_rows) invalidate_graphs(s);
+  s->rb_rows = rows;
+  s->rb_tuned = true;
+  return H2G_OK;
+}
+
 static int create(int MX, int MY, int MZ, int precision, Solver** out) {
   if (!out) return fail(H2G_BAD_ARG, "null output pointer");
   *out = nullptr;
@@ -1392,7 +1504,7 @@ static int rbsor_t(Solver* s, double* x, const double* b, int color, double omeg
   T* bd = static_cast<T*>(hb);
   if ((rc = upload<T>(s, x, xd, 0))) return rc;
   if ((rc = upload<T>(s, b, bd, 1))) return rc;
-  launch(s, k_rb_pass<T>, rb_grid(s->g), dim3(kBX, kBY), s->stream, op, xd, bd, color, (T)omega, nullptr);
+  launch_rb<T>(s, s->stream, op, xd, (const T*)bd, color, (T)omega, nullptr);
   CKL();
   return download<T>(s, xd, x);
 }
@@ -1410,7 +1522,7 @@ static int precond_t(Solver* s, const double* bb, double* xx, int smoother, cons
   const int none = smoother == H2G_SMOOTHER_NONE;
   launch(s, k_rb_first<T, T, 0>, first_grid(s->g), blk, s->stream, op, xd, bd, nullptr, nullptr, nullptr, nullptr, none);
   if (!none)
-    for (int pass = 1; pass < 2 * kSweeps; ++pass) launch(s, k_rb_pass<T>, rg, blk, s->stream, op, xd, bd, pass & 1, T(1), nullptr);
+    for (int pass = 1; pass < 2 * kSweeps; ++pass) launch_rb<T>(s, s->stream, op, xd, (const T*)bd, pass & 1, T(1), nullptr);
   CKL();
   return download<T>(s, xd, xx);
 }
@@ -1418,6 +1530,8 @@ static int precond_t(Solver* s, const double* bb, double* xx, int smoother, cons
 template <typename T>
 static int bench_t(Solver* s, int kind, int reps, int* launches, const h2g::OpParams<T>& op) {
   using namespace h2g;
+  if (kind == 0)
+    if (int rc = autotune(s)) return rc;
   // the hook buffers (zeroed when allocated; values are irrelevant for timing)
   const size_t bytes = sizeof(double) * (size_t)s->g.n;
   for (auto& p : s->hook)
@@ -1431,8 +1545,8 @@ static int bench_t(Solver* s, int kind, int reps, int* launches, const h2g::OpPa
   int n = 0;
   for (int r = 0; r < reps; ++r) {
     if (kind == 0) {
-      launch(s, k_rb_pass<T>, rg, blk, s->stream, op, xa, xb, 0, T(1), nullptr);
-      launch(s, k_rb_pass<T>, rg, blk, s->stream, op, xa, xb, 1, T(1), nullptr);
+      launch_rb<T>(s, s->stream, op, xa, (const T*)xb, 0, T(1), nullptr);
+      launch_rb<T>(s, s->stream, op, xa, (const T*)xb, 1, T(1), nullptr);
       n += 2;
     } else {
       launch(s, k_ax<T, 0>, ag, blk, s->stream, op, xb, xa, nullptr, nullptr, nullptr, nullptr, 0);
@@ -1712,6 +1826,30 @@ int h2g_adjoint_transient(h2g_solver* h, const h2g_bc* bc, int nt, const double*
   if (int rc = h2g::face_bc(bc, f)) return rc;
   return h2g::adjoint_transient(S(h), f, nt, weights, p, tol, maxItr, smoother, checkpoint_every, J, dJ_dhsrc,
                                 dJ_dlnlam, out);
+}
+
+int h2g_autotune(h2g_solver* h, int* rows) {
+  if (int rc = h2g::check_handle(h)) return rc;
+  Solver* s = S(h);
+  if (!s->grid_set || !s->fields_set) return fail(H2G_BAD_ARG, "h2g_set_grid and h2g_set_fields must come first");
+  CK(cudaSetDevice(s->device));
+  if (int rc = h2g::autotune(s)) return rc;
+  if (rows) *rows = s->rb_rows;
+  return H2G_OK;
+}
+
+int h2g_set_tuning(h2g_solver* h, int rows) {
+  if (int rc = h2g::check_handle(h)) return rc;
+  Solver* s = S(h);
+  if (rows == 0) {
+    s->rb_tuned = false;
+    return H2G_OK;
+  }
+  if (!h2g::valid_rows(rows)) return fail(H2G_BAD_ARG, "rows per block must be 2, 4, 8 or 16 (0: tune)");
+  if (rows != s->rb_rows) h2g::invalidate_graphs(s);
+  s->rb_rows = rows;
+  s->rb_tuned = true;
+  return H2G_OK;
 }
 
 int h2g_release_cached(void) {

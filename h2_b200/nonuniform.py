@@ -214,6 +214,16 @@ class Solver:
         L.check(self.lib.h2g_preconditioner(self.h, _ptr(self._arr(bb, "bb")), _ptr(xx), smoother_selector(smoother)))
         return xx
 
+    def autotune(self) -> int:
+        """Run the launch-shape tuner now; returns the colour pass's rows per block."""
+        r = C.c_int(0)
+        L.check(self.lib.h2g_autotune(self.h, C.byref(r)))
+        return r.value
+
+    def set_tuning(self, rows: int):
+        """Force the colour pass's rows per block (2, 4, 8, 16); 0 tunes again."""
+        L.check(self.lib.h2g_set_tuning(self.h, int(rows)))
+
     def bench_kernel(self, kind: int, reps: int) -> int:
         n = C.c_int()
         L.check(self.lib.h2g_bench_kernel(self.h, int(kind), int(reps), C.byref(n)))

@@ -208,6 +208,15 @@ int h2g_calrhs(h2g_solver *h, const h2g_bc *bc, int zero_b);
 int h2g_transient(h2g_solver *h, const h2g_bc *bc, int nt, int method, double tol, int maxItr, int smoother,
                   int verbose, double *step_stats, h2g_result *out);
 
+/* ---- launch-shape tuning (no reference counterpart) ---------------------------------------
+ * The smoother's colour pass has no reduction, so its block height changes no result.  The
+ * first solve of a handle times heights of 2, 4, 8 and 16 rows (a few sweeps each on scratch
+ * vectors) and keeps the fastest; the choice is cached per grid size and smoother precision for
+ * the process, and H2G_RB_ROWS in the environment forces one.  h2g_autotune runs the tuner now
+ * (*rows: the choice, nullable); h2g_set_tuning forces rows (2, 4, 8, 16; 0 = tune again). */
+int h2g_autotune(h2g_solver *h, int *rows);
+int h2g_set_tuning(h2g_solver *h, int rows);
+
 /* ---- kernels of the path, callable one at a time (host arrays in and out) ---------------
  * CalcAX! (NonUniform.jl:454-511): ax = A x over the interior; guard cells of ax are 0. */
 int h2g_calcax(h2g_solver *h, const double *x, double *ax);

@@ -1,0 +1,44 @@
+"""Launch-shape tuning of the colour pass: every block height gives bit-identical results (the
+pass has no reduction), the tuner picks one of the allowed heights and caches it per grid."""
+import numpy as np
+import pytest
+
+import h2_b200
+from conftest import mode3_model
+from test_gpu_kernels import make_solver
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_heights_give_identical_solves(oracle, precision):
+    prob = mode3_model(oracle, 40)
+    ref = None
+    for rows in (2, 4, 8, 16):
+        s = make_solver(prob, precision=precision)
+        s.set_tuning(rows)
+        st, res = s.solve("pbicgstab", tol=1e-8, maxItr=20000, smoother="gs")
+        assert st == 0
+        out = (res.itr, res.res0, res.res, s.get_theta())
+        pre = s.preconditioner(prob.wk["b"])
+        if ref is None:
+            ref = out + (pre,)
+        else:
+            assert out[:3] == ref[:3]
+            assert np.array_equal(out[3], ref[3]) and np.array_equal(pre, ref[4])
+        s.close()
+
+
+def test_tuner_choice_is_cached(oracle):
+    prob = mode3_model(oracle, 32)
+    s1 = make_solver(prob)
+    r1 = s1.autotune()
+    assert r1 in (2, 4, 8, 16)
+    s2 = make_solver(prob)
+    assert s2.autotune() == r1
+    with pytest.raises(h2_b200.H2GError):
+        s2.set_tuning(3)
+    s2.set_tuning(0)  # tune again: the cached choice comes back
+    assert s2.autotune() == r1
+    s1.close()
+    s2.close()
