@@ -112,6 +112,7 @@ struct OpParams {
   const T* conv;       // [MZ][4] convective terms of x-, x+, y-, y+ faces at plane k
   const T* rc;         // rho*cp per cell (device layout), transient only
   const T* dzk;        // [MZ] dZ
+  const T* ddv;        // dd per cell (device layout), precomputed with the tables; may be null
   T czm, czp;          // convective terms of the z-, z+ faces
   T dx0, dy0, ddt;
   int P;

@@ -29,6 +29,10 @@ namespace h2g {
 #ifndef H2G_XNB_LOAD
 #define H2G_XNB_LOAD 1
 #endif
+// the smoother reads dd from a per-cell array (1) or sums its 13 terms per cell (0)
+#ifndef H2G_DD_ARRAY
+#define H2G_DD_ARRAY 1
+#endif
 constexpr int kBX = 32;       // threads along the half-row
 constexpr int kBY = H2G_BY;   // rows per block
 constexpr int kThreads = kBX * kBY;
@@ -240,7 +244,9 @@ struct Coef {
 // are indexed by the neighbour's whole key byte: its mask bit selects lambda_f's factor
 // 2 - div(ma+mb, 2) (1 if the neighbour is unmasked, 2 if it is a masked guard).  The order of
 // the additions of dd follows NonUniform.jl:501-502 exactly.
-template <typename T>
+// PRE: take dd from the per-cell array op.ddv (computed once per grid by k_make_dd with this same
+// function, so the values are identical) instead of summing its 13 terms.
+template <typename T, bool PRE = false>
 __device__ __forceinline__ bool cell_coef(const OpParams<T>& op, int k, uint8_t k0, uint8_t kxm, uint8_t kxp,
                                           uint8_t kym, uint8_t kyp, uint8_t kzm, uint8_t kzp, int ci, Coef<T>& c) {
   if (!(k0 & 0x80)) return false;
@@ -251,6 +257,10 @@ __device__ __forceinline__ bool cell_coef(const OpParams<T>& op, int k, uint8_t 
   c.cyp = __ldg(op.ty + (bx | kyp));
   c.czm = __ldg(op.tz + (bx | kzm));
   c.czp = __ldg(op.tz + ((bx + (op.P << 8)) | kzp));
+  if constexpr (PRE && H2G_DD_ARRAY) {
+    c.dd = __ldg(op.ddv + ci);
+    return true;
+  }
   const T* cv = op.conv + 4 * k;
   const T vxm = (kxm & 0x80) ? T(0) : __ldg(cv + 0);
   const T vxp = (kxp & 0x80) ? T(0) : __ldg(cv + 1);
@@ -443,8 +453,8 @@ __device__ __forceinline__ double rb_pass_column(const OpParams<T>& op, T* x, co
     if (!ok[u]) continue;
     const int ac = rc0 + u * PL + p;
     Coef<T> c;
-    if (!cell_coef(op, k0 + u, (uint8_t)kc[u], (uint8_t)kxm[u], (uint8_t)kxp[u], (uint8_t)kym[u], (uint8_t)kyp[u],
-                   (uint8_t)kcol[u], (uint8_t)kcol[u + 2], ac, c))
+    if (!cell_coef<T, true>(op, k0 + u, (uint8_t)kc[u], (uint8_t)kxm[u], (uint8_t)kxp[u], (uint8_t)kym[u],
+                            (uint8_t)kyp[u], (uint8_t)kcol[u], (uint8_t)kcol[u + 2], ac, c))
       continue;
     const T ss = nb_sum(c, xp[u], xm[u], yp[u], ym[u], col[u + 2], col[u]);
     const T dp = sub(gs_div(sub(ss, bv[u]), c.dd), pp[u]);  // * m0 (= 1)
@@ -578,8 +588,8 @@ __global__ void __launch_bounds__(kThreads) k_rb_first(OpParams<T> op, T* __rest
       out = b;
     } else if (col == 0) {
       Coef<T> c;
-      if (cell_coef(op, k, (uint8_t)k0c, (uint8_t)kxm, (uint8_t)kxp, (uint8_t)kym, (uint8_t)kyp, (uint8_t)k1m,
-                    (uint8_t)k1p, ci, c)) {
+      if (cell_coef<T, true>(op, k, (uint8_t)k0c, (uint8_t)kxm, (uint8_t)kxp, (uint8_t)kym, (uint8_t)kyp,
+                             (uint8_t)k1m, (uint8_t)k1p, ci, c)) {
         const T ss = T(0);
         const T dp = sub(gs_div(sub(ss, b), c.dd), T(0));
         out = add(T(0), dp);  // pp + omega*dp with pp = 0, omega = 1
@@ -1243,6 +1253,23 @@ template <typename T>
 __global__ void __launch_bounds__(256) k_fill_const(long long n, T* __restrict__ a, T v) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     a[i] = v;
+}
+
+// dd of every interior cell (cell_coef's 13-term sum in the reference's order; 1 for masked
+// cells), for the smoother.  One thread per interior cell.
+template <typename T>
+__global__ void __launch_bounds__(256) k_make_dd(OpParams<T> op, T* __restrict__ ddv) {
+  const Geo& g = op.g;
+  const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = 1 + blockIdx.y, k = 1 + blockIdx.z;
+  if (i > g.NX) return;
+  const int o = g.off(i, j, k);
+  const uint8_t* key = op.key;
+  Coef<T> c;
+  const bool has = cell_coef<T, false>(op, k, key[o], key[g.off(i - 1, j, k)], key[g.off(i + 1, j, k)],
+                                       key[g.off(i, j - 1, k)], key[g.off(i, j + 1, k)], key[g.off(i, j, k - 1)],
+                                       key[g.off(i, j, k + 1)], o, c);
+  ddv[o] = has ? c.dd : T(1);
 }
 
 // ------------------------------------------------------------------------------------------

@@ -81,6 +81,7 @@ struct OpTables {
   T* tz = nullptr;
   T* conv = nullptr;
   T* dzk = nullptr;
+  T* ddv = nullptr;  // dd per cell (device layout)
   int pcap = 0;
 };
 
@@ -230,6 +231,7 @@ static OpParams<T> op_params_rc(const Solver* s, const OpTables<T>& t, const T* 
   op.conv = t.conv;
   op.rc = rc;
   op.dzk = t.dzk;
+  op.ddv = t.ddv;
   const double dx0 = s->dx, dy0 = s->dy;
   op.czm = (T)((s->HC[4] * dx0) * dy0);
   op.czp = (T)((s->HC[5] * dx0) * dy0);
@@ -254,11 +256,11 @@ static OpParams<T> op_params(const Solver* s, const void* tables) {
 }
 
 static void free_tables64(OpTables<double>& t) {
-  cudaFree(t.tx); cudaFree(t.ty); cudaFree(t.tz); cudaFree(t.conv); cudaFree(t.dzk);
+  cudaFree(t.tx); cudaFree(t.ty); cudaFree(t.tz); cudaFree(t.conv); cudaFree(t.dzk); cudaFree(t.ddv);
   t = OpTables<double>();
 }
 static void free_tables32(OpTables<float>& t) {
-  cudaFree(t.tx); cudaFree(t.ty); cudaFree(t.tz); cudaFree(t.conv); cudaFree(t.dzk);
+  cudaFree(t.tx); cudaFree(t.ty); cudaFree(t.tz); cudaFree(t.conv); cudaFree(t.dzk); cudaFree(t.ddv);
   t = OpTables<float>();
 }
 
@@ -369,6 +371,8 @@ static int build_tables(Solver* s) {
     CK(cudaMalloc(&s->t64.tz, sizeof(double) * bytes_t));
     CK(cudaMalloc(&s->t64.conv, sizeof(double) * 4 * g.MZ));
     CK(cudaMalloc(&s->t64.dzk, sizeof(double) * g.MZ));
+    CK(cudaMalloc(&s->t64.ddv, sizeof(double) * (size_t)g.n));
+    CK(cudaMemsetAsync(s->t64.ddv, 0, sizeof(double) * (size_t)g.n, s->stream));
     s->t64.pcap = pc;
     if (s->precision != H2G_FP64) {
       CK(cudaMalloc(&s->t32.tx, sizeof(float) * bytes_t));
@@ -376,6 +380,8 @@ static int build_tables(Solver* s) {
       CK(cudaMalloc(&s->t32.tz, sizeof(float) * bytes_t));
       CK(cudaMalloc(&s->t32.conv, sizeof(float) * 4 * g.MZ));
       CK(cudaMalloc(&s->t32.dzk, sizeof(float) * g.MZ));
+      CK(cudaMalloc(&s->t32.ddv, sizeof(float) * (size_t)g.n));
+      CK(cudaMemsetAsync(s->t32.ddv, 0, sizeof(float) * (size_t)g.n, s->stream));
       s->t32.pcap = pc;
     }
   }
@@ -396,6 +402,19 @@ static int build_tables(Solver* s) {
     CK(cudaMemcpyAsync(s->t32.tz, fz.data(), sizeof(float) * bytes_t, cudaMemcpyHostToDevice, s->stream));
     CK(cudaMemcpyAsync(s->t32.conv, fc.data(), sizeof(float) * 4 * g.MZ, cudaMemcpyHostToDevice, s->stream));
     CK(cudaMemcpyAsync(s->t32.dzk, fd.data(), sizeof(float) * g.MZ, cudaMemcpyHostToDevice, s->stream));
+  }
+  // dd per cell for the smoother, from the tables just written (op.ddv null: summed in full)
+  {
+    const dim3 grid((g.NX + 127) / 128, g.NY, g.NZ);
+    OpParams<double> o64 = op_params<double>(s, s->t64);
+    o64.ddv = nullptr;
+    k_make_dd<double><<<grid, 128, 0, s->stream>>>(o64, s->t64.ddv);
+    if (s->precision != H2G_FP64) {
+      OpParams<float> o32 = op_params<float>(s, s->t32);
+      o32.ddv = nullptr;
+      k_make_dd<float><<<grid, 128, 0, s->stream>>>(o32, s->t32.ddv);
+    }
+    CKL();
   }
   // host vectors must stay alive until the copies ran
   CK(cudaStreamSynchronize(s->stream));
