@@ -35,8 +35,9 @@ METRIC = "PBiCGSTAB time-to-eps (s) + stencil HBM GB/s, mixed vs FP64 GPU at 240
 L2_FLUSH_BYTES = 256 << 20
 # DRAM bytes (read + write) of one FP64 RB-GS sweep (two k_rb_pass<double> launches) on the
 # 240x240x30 grid, from one ncu capture of `python -m h2_b200.kernel_bench --kind sweep
-# --precision fp64` (dram__bytes_read.sum 24.64 MB and dram__bytes_write.sum 0.5 KB per launch).
-SWEEP_TRAFFIC_F64 = {(240, 30): 2 * (24.637e6 + 512.0)}
+# --precision fp64` (dram__bytes_read.sum 32.0 MB and dram__bytes_write.sum 0 per launch; the
+# pass also reads the precomputed dd of the cells it updates, 6.9 MB, beyond the algorithmic bytes).
+SWEEP_TRAFFIC_F64 = {(240, 30): 2 * 32.006e6}
 
 
 def log(*a):

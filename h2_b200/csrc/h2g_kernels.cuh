@@ -33,6 +33,7 @@ namespace h2g {
 #ifndef H2G_DD_ARRAY
 #define H2G_DD_ARRAY 1
 #endif
+
 constexpr int kBX = 32;       // threads along the half-row
 constexpr int kBY = H2G_BY;   // rows per block
 constexpr int kThreads = kBX * kBY;
@@ -645,7 +646,9 @@ __device__ __forceinline__ void load_pair(const Geo& g, const TI* x, const uint8
 // and the stage finisher.  TI: type of x (the preconditioner output may be FP32 while A is
 // applied in FP64).  Grid (ceil(HN/32), ceil(NY/kBY), NZ).
 // ------------------------------------------------------------------------------------------
-template <typename T, int NDOT, typename TI = T>
+// DD: read dd from the per-cell array (FP64 only; the FP32 operator uses the difference form).
+// Which is faster depends on whether the vectors stay in L2; the launch-shape tuner decides.
+template <typename T, int NDOT, typename TI = T, bool DD = false>
 __global__ void __launch_bounds__(kThreads) k_ax(OpParams<T> op, T* __restrict__ y, const TI* __restrict__ x,
                                                   const T* __restrict__ u, const T* __restrict__ w,
                                                   SolverState* st, double* __restrict__ partials, int stage) {
@@ -690,10 +693,10 @@ __global__ void __launch_bounds__(kThreads) k_ax(OpParams<T> op, T* __restrict__
       T out = T(0);
       bool has;
       if (col == 0)
-        has = cell_coef(op, k, (uint8_t)P.kc0[1], (uint8_t)kxm0, (uint8_t)kxp0, (uint8_t)P.ky1m, (uint8_t)P.ky1p,
+        has = cell_coef<T, DD && sizeof(T) == 8>(op, k, (uint8_t)P.kc0[1], (uint8_t)kxm0, (uint8_t)kxp0, (uint8_t)P.ky1m, (uint8_t)P.ky1p,
                         (uint8_t)P.kc1[0], (uint8_t)P.kc1[2], ci, c);
       else
-        has = cell_coef(op, k, (uint8_t)P.kc1[1], (uint8_t)kxm1, (uint8_t)kxp1, (uint8_t)P.ky0m, (uint8_t)P.ky0p,
+        has = cell_coef<T, DD && sizeof(T) == 8>(op, k, (uint8_t)P.kc1[1], (uint8_t)kxm1, (uint8_t)kxp1, (uint8_t)P.ky0m, (uint8_t)P.ky0p,
                         (uint8_t)P.kc0[0], (uint8_t)P.kc0[2], ci, c);
       if (has) {
         if (col == 0) out = apply_a(c, P.c0[1], xp0, xm0, P.y1p, P.y1m, P.c1[2], P.c1[0]);
@@ -748,10 +751,10 @@ __global__ void __launch_bounds__(kThreads) k_rk(OpParams<double> op, T* __restr
       double rs = 0.0;
       bool has;
       if (col == 0)
-        has = cell_coef(op, k, (uint8_t)P.kc0[1], (uint8_t)kxm0, (uint8_t)kxp0, (uint8_t)P.ky1m, (uint8_t)P.ky1p,
+        has = cell_coef<double, true>(op, k, (uint8_t)P.kc0[1], (uint8_t)kxm0, (uint8_t)kxp0, (uint8_t)P.ky1m, (uint8_t)P.ky1p,
                         (uint8_t)P.kc1[0], (uint8_t)P.kc1[2], ci, c);
       else
-        has = cell_coef(op, k, (uint8_t)P.kc1[1], (uint8_t)kxm1, (uint8_t)kxp1, (uint8_t)P.ky0m, (uint8_t)P.ky0p,
+        has = cell_coef<double, true>(op, k, (uint8_t)P.kc1[1], (uint8_t)kxm1, (uint8_t)kxp1, (uint8_t)P.ky0m, (uint8_t)P.ky0p,
                         (uint8_t)P.kc0[0], (uint8_t)P.kc0[2], ci, c);
       if (has) {
         const double ss = col == 0 ? nb_sum(c, xp0, xm0, P.y1p, P.y1m, P.c1[2], P.c1[0])
@@ -806,10 +809,10 @@ __global__ void __launch_bounds__(kThreads) k_res_sor(OpParams<double> op, const
       Coef<double> c;
       bool has;
       if (col == 0)
-        has = cell_coef(op, k, (uint8_t)P.kc0[1], (uint8_t)kxm0, (uint8_t)kxp0, (uint8_t)P.ky1m, (uint8_t)P.ky1p,
+        has = cell_coef<double, true>(op, k, (uint8_t)P.kc0[1], (uint8_t)kxm0, (uint8_t)kxp0, (uint8_t)P.ky1m, (uint8_t)P.ky1p,
                         (uint8_t)P.kc1[0], (uint8_t)P.kc1[2], ci, c);
       else
-        has = cell_coef(op, k, (uint8_t)P.kc1[1], (uint8_t)kxm1, (uint8_t)kxp1, (uint8_t)P.ky0m, (uint8_t)P.ky0p,
+        has = cell_coef<double, true>(op, k, (uint8_t)P.kc1[1], (uint8_t)kxm1, (uint8_t)kxp1, (uint8_t)P.ky0m, (uint8_t)P.ky0p,
                         (uint8_t)P.kc0[0], (uint8_t)P.kc0[2], ci, c);
       if (!has) continue;
       const double ss = col == 0 ? nb_sum(c, xp0, xm0, P.y1p, P.y1m, P.c1[2], P.c1[0])

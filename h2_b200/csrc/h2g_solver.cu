@@ -143,6 +143,7 @@ struct Solver {
   bool no_cond = false;
   bool pdl = true;  // programmatic dependent launch of the solver kernels
   int rb_rows = kBY;      // rows per block of the colour pass (autotuned)
+  bool ax_dd = false;     // CalcAX reads dd from the per-cell array (autotuned)
   bool rb_tuned = false;  // rb_rows chosen (by the tuner or h2g_set_tuning)
 
   long long nfort() const { return (long long)g.MX * g.MY * g.MZ; }
@@ -186,6 +187,15 @@ static dim3 rb_grid(const Geo& g, int by = kBY) {
 }
 static dim3 ax_grid(const Geo& g) { return dim3((g.HN + kBX - 1) / kBX, (g.NY + kBY - 1) / kBY, g.NZ); }
 static dim3 first_grid(const Geo& g) { return ax_grid(g); }
+
+// CalcAX with the handle's choice of dd source.
+template <typename T, int NDOT, typename TI>
+static void launch_ax(const Solver* s, cudaStream_t cs, const OpParams<T>& op, T* y, const TI* x, const T* u,
+                      const T* w, SolverState* st, int stage) {
+  const dim3 ag((op.g.HN + kBX - 1) / kBX, (op.g.NY + kBY - 1) / kBY, op.g.NZ), blk(kBX, kBY);
+  if (s->ax_dd) launch(s, k_ax<T, NDOT, TI, true>, ag, blk, cs, op, y, x, u, w, st, s->partials, stage);
+  else launch(s, k_ax<T, NDOT, TI, false>, ag, blk, cs, op, y, x, u, w, st, s->partials, stage);
+}
 
 // One colour pass with the handle's block height.
 template <typename T>
@@ -448,14 +458,14 @@ static void launch_pbicg_body(Solver* s, cudaStream_t cs, const OpParams<T>& opA
     for (int pass = 1; pass < 2 * kSweeps; ++pass)
       launch_rb<TP>(s, cs, opM, ph, bbm ? bbm : reinterpret_cast<TP*>(p), pass & 1, TP(1), st);
   // q = A p_;  alpha = rho / (q, r0)                            NonUniform.jl:307-309
-  launch(s, k_ax<T, 1, TP>, ag, blk, cs, opA, q, ph, r0, nullptr, st, s->partials, kStageAlpha);
+  launch_ax<T, 1, TP>(s, cs, opA, q, ph, r0, nullptr, st, kStageAlpha);
   // s = r - alpha q; s_ = M^-1 s                                NonUniform.jl:310-315
   launch(s, k_rb_first<TP, T, 2>, first_grid(g), blk, cs, opM, sh, sv, bbm, r, q, st, none);
   if (!none)
     for (int pass = 1; pass < 2 * kSweeps; ++pass)
       launch_rb<TP>(s, cs, opM, sh, bbm ? bbm : reinterpret_cast<TP*>(sv), pass & 1, TP(1), st);
   // t = A s_; omega = (t,s)/(t,t)                               NonUniform.jl:317-326
-  launch(s, k_ax<T, 2, TP>, ag, blk, cs, opA, t, sh, nullptr, sv, st, s->partials, kStageOmega);
+  launch_ax<T, 2, TP>(s, cs, opA, t, sh, nullptr, sv, st, kStageOmega);
   // x += alpha p_ + omega s_; r = s - omega t; res; next rho    NonUniform.jl:328-346
   launch(s, k_bicg_update<T, TX, TP>, elementwise_blocks(s), 256, cs, g.n, x, ph, sh, r, sv, t, r0, st, s->partials, hc,
                                                                   use_cond);
@@ -486,7 +496,7 @@ static void launch_cg_body(Solver* s, cudaStream_t cs, const OpParams<T>& opA, c
   const dim3 ag = ax_grid(g), blk(kBX, kBY);
   const int nb = elementwise_blocks(s);
   // q = A p; alpha = rho_old / (p,q)                             NonUniform.jl:164-176
-  launch(s, k_ax<T, 1, T>, ag, blk, cs, opA, q, p, p, nullptr, st, s->partials, kStageCgAlpha);
+  launch_ax<T, 1, T>(s, cs, opA, q, p, p, nullptr, st, kStageCgAlpha);
   // x += alpha p; r -= alpha q; res                              NonUniform.jl:179-198
   launch(s, k_cg_update<T, TX>, nb, 256, cs, g.n, x, p, r, q, st, s->partials);
   // z = M^-1 r                                                  NonUniform.jl:201-203
@@ -1297,28 +1307,69 @@ static int tune_rows_t(Solver* s, const OpParams<T>& op, int* best_rows) {
   return rc;
 }
 
+// CalcAX (FP64 operator) with dd summed per cell or read from the array: 1 if reading is faster.
+static int tune_ax(Solver* s, int* use_dd) {
+  const size_t n = (size_t)s->g.n, bytes = sizeof(double) * n;
+  for (auto& p : s->hook)
+    if (!p) CK(cudaMalloc(&p, bytes));
+  double* xa = static_cast<double*>(s->hook[0]);
+  double* xb = static_cast<double*>(s->hook[1]);
+  k_fill_const<double><<<elementwise_blocks(s), 256, 0, s->stream>>>((long long)n, xa, 300.0);
+  CKL();
+  const OpParams<double> op = op_params<double>(s, s->t64);
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return fail(H2G_CUDA_ERROR, "event creation failed");
+  }
+  const bool saved = s->ax_dd;
+  float t[2] = {0.f, 0.f};
+  int rc = H2G_OK;
+  for (int v = 0; v < 2 && rc == H2G_OK; ++v) {
+    s->ax_dd = v == 1;
+    for (int r = 0; r < 2; ++r) launch_ax<double, 0, double>(s, s->stream, op, xb, xa, nullptr, nullptr, nullptr, 0);
+    cudaEventRecord(e0, s->stream);
+    for (int r = 0; r < 10; ++r) launch_ax<double, 0, double>(s, s->stream, op, xb, xa, nullptr, nullptr, nullptr, 0);
+    cudaEventRecord(e1, s->stream);
+    if (cudaGetLastError() != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+        cudaEventElapsedTime(&t[v], e0, e1) != cudaSuccess)
+      rc = fail(H2G_CUDA_ERROR, "CalcAX tuning failed");
+  }
+  s->ax_dd = saved;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *use_dd = t[1] < t[0] ? 1 : 0;
+  return rc;
+}
+
 static int autotune(Solver* s) {
   if (s->rb_tuned) return H2G_OK;
-  int rows = 0;
+  int rows = 0, dd = -1;
   if (const char* e = getenv("H2G_RB_ROWS")) rows = atoi(e);
-  if (!valid_rows(rows)) {
-    rows = 0;
-    const std::array<int, 4> key = {s->g.MX, s->g.MY, s->g.MZ, s->precision == H2G_FP64 ? 64 : 32};
-    {
-      std::lock_guard<std::mutex> lk(g_tune_mu);
-      auto it = g_tune_cache.find(key);
-      if (it != g_tune_cache.end()) rows = it->second;
-    }
-    if (!rows) {
-      int rc = s->precision == H2G_FP64 ? tune_rows_t<double>(s, op_params<double>(s, s->t64), &rows)
-                                        : tune_rows_t<float>(s, op_params<float>(s, s->t32), &rows);
-      if (rc) return rc;
-      std::lock_guard<std::mutex> lk(g_tune_mu);
-      g_tune_cache[key] = rows;
-    }
+  if (const char* e = getenv("H2G_AX_DD")) dd = atoi(e) ? 1 : 0;
+  const std::array<int, 4> key = {s->g.MX, s->g.MY, s->g.MZ, s->precision == H2G_FP64 ? 64 : 32};
+  int cached = 0;
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) cached = it->second;
   }
-  if (rows != s->rb_rows) invalidate_graphs(s);
+  if (!cached) {
+    int r2 = 0, d2 = 0;
+    int rc = s->precision == H2G_FP64 ? tune_rows_t<double>(s, op_params<double>(s, s->t64), &r2)
+                                      : tune_rows_t<float>(s, op_params<float>(s, s->t32), &r2);
+    if (!rc) rc = tune_ax(s, &d2);
+    if (rc) return rc;
+    cached = r2 | (d2 << 8);
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune_cache[key] = cached;
+  }
+  if (!valid_rows(rows)) rows = cached & 0xff;
+  if (dd < 0) dd = cached >> 8;
+  if (rows != s->rb_rows || (dd != 0) != s->ax_dd) invalidate_graphs(s);
   s->rb_rows = rows;
+  s->ax_dd = dd != 0;
   s->rb_tuned = true;
   return H2G_OK;
 }
@@ -1508,7 +1559,7 @@ static int calcax_t(Solver* s, const double* x, double* ax, const h2g::OpParams<
   T* xd = static_cast<T*>(ha);
   T* yd = static_cast<T*>(hb);
   if ((rc = upload<T>(s, x, xd))) return rc;
-  launch(s, k_ax<T, 0>, ax_grid(s->g), dim3(kBX, kBY), s->stream, op, yd, xd, nullptr, nullptr, nullptr, nullptr, 0);
+  launch_ax<T, 0, T>(s, s->stream, op, yd, (const T*)xd, nullptr, nullptr, nullptr, 0);
   CKL();
   return download<T>(s, yd, ax);
 }
@@ -1549,8 +1600,7 @@ static int precond_t(Solver* s, const double* bb, double* xx, int smoother, cons
 template <typename T>
 static int bench_t(Solver* s, int kind, int reps, int* launches, const h2g::OpParams<T>& op) {
   using namespace h2g;
-  if (kind == 0)
-    if (int rc = autotune(s)) return rc;
+  if (int rc = autotune(s)) return rc;
   // the hook buffers (zeroed when allocated; values are irrelevant for timing)
   const size_t bytes = sizeof(double) * (size_t)s->g.n;
   for (auto& p : s->hook)
@@ -1568,7 +1618,7 @@ static int bench_t(Solver* s, int kind, int reps, int* launches, const h2g::OpPa
       launch_rb<T>(s, s->stream, op, xa, (const T*)xb, 1, T(1), nullptr);
       n += 2;
     } else {
-      launch(s, k_ax<T, 0>, ag, blk, s->stream, op, xb, xa, nullptr, nullptr, nullptr, nullptr, 0);
+      launch_ax<T, 0, T>(s, s->stream, op, xb, (const T*)xa, nullptr, nullptr, nullptr, 0);
       n += 1;
     }
   }

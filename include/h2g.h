@@ -211,9 +211,11 @@ int h2g_transient(h2g_solver *h, const h2g_bc *bc, int nt, int method, double to
 /* ---- launch-shape tuning (no reference counterpart) ---------------------------------------
  * The smoother's colour pass has no reduction, so its block height changes no result.  The
  * first solve of a handle times heights of 2, 4, 8 and 16 rows (a few sweeps each on scratch
- * vectors) and keeps the fastest; the choice is cached per grid size and smoother precision for
- * the process, and H2G_RB_ROWS in the environment forces one.  h2g_autotune runs the tuner now
- * (*rows: the choice, nullable); h2g_set_tuning forces rows (2, 4, 8, 16; 0 = tune again). */
+ * vectors) and keeps the fastest; it also times the FP64 CalcAX with dd read from the per-cell
+ * array against dd summed per cell (the same bits either way).  The choices are cached per grid
+ * size and smoother precision for the process; H2G_RB_ROWS and H2G_AX_DD (0/1) in the
+ * environment force them.  h2g_autotune runs the tuner now (*rows: the colour pass's rows,
+ * nullable); h2g_set_tuning forces rows (2, 4, 8, 16; 0 = tune again on the next solve). */
 int h2g_autotune(h2g_solver *h, int *rows);
 int h2g_set_tuning(h2g_solver *h, int rows);
 

@@ -1,5 +1,7 @@
 """Launch-shape tuning of the colour pass: every block height gives bit-identical results (the
 pass has no reduction), the tuner picks one of the allowed heights and caches it per grid."""
+import os
+
 import numpy as np
 import pytest
 
@@ -42,3 +44,20 @@ def test_tuner_choice_is_cached(oracle):
     assert s2.autotune() == r1
     s1.close()
     s2.close()
+
+
+def test_calcax_dd_source_gives_identical_results(oracle, monkeypatch):
+    prob = mode3_model(oracle, 40)
+    x = np.zeros(prob.shape, order="F")
+    x[1:-1, 1:-1, 1:-1] = np.random.default_rng(1).standard_normal((prob.NX, prob.NY, prob.NZ))
+    outs = []
+    for dd in ("0", "1"):
+        monkeypatch.setenv("H2G_AX_DD", dd)
+        s = make_solver(prob)
+        st, res = s.solve("pbicgstab", tol=1e-8, maxItr=20000, smoother="gs")
+        assert st == 0
+        outs.append((res.itr, res.res, s.get_theta(), s.calc_ax(x)))
+        s.close()
+    assert outs[0][:2] == outs[1][:2]
+    assert np.array_equal(outs[0][2], outs[1][2]) and np.array_equal(outs[0][3], outs[1][3])
+    assert os.environ.get("H2G_AX_DD") == "1"
