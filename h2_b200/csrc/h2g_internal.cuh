@@ -90,16 +90,17 @@ struct SolverState {
   int passes;        // WHILE-body passes of this solve (bounds the graph loop independently)
 };
 
-// ---- arithmetic that must not be contracted into FMA (FP64 follows the reference's
-// ---- two-rounding a*b + c); FP32 is free to contract.
+// ---- arithmetic that must not be contracted into FMA: FP64 follows the reference's two-rounding
+// ---- a*b + c; FP32 is kept uncontracted too, so that every launch shape of a kernel (the
+// ---- compiler may contract differently per instantiation) gives the same bits.
 __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
 __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
 __device__ __forceinline__ double dvd(double a, double b) { return __ddiv_rn(a, b); }
-__device__ __forceinline__ float mul(float a, float b) { return a * b; }
-__device__ __forceinline__ float add(float a, float b) { return a + b; }
-__device__ __forceinline__ float sub(float a, float b) { return a - b; }
-__device__ __forceinline__ float dvd(float a, float b) { return a / b; }
+__device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float dvd(float a, float b) { return __fdiv_rn(a, b); }
 
 // Parameters of the operator for one precision T.
 template <typename T>

@@ -288,17 +288,32 @@ __device__ __forceinline__ bool cell_coef(const OpParams<T>& op, int k, uint8_t 
   return true;
 }
 
-// ss of NonUniform.jl:505-507 (products summed left to right)
+// ss of NonUniform.jl:505-507 (products summed left to right).  FP64: separately rounded, as the
+// reference.  FP32 (the mixed smoother): fused multiply-adds, written out so that every launch
+// shape computes the same bits.
 template <typename T>
 __device__ __forceinline__ T nb_sum(const Coef<T>& c, T xp, T xm, T yp, T ym, T zp, T zm) {
-  T s = mul(c.cxp, xp);
-  s = add(s, mul(c.cxm, xm));
-  s = add(s, mul(c.cyp, yp));
-  s = add(s, mul(c.cym, ym));
-  s = add(s, mul(c.czp, zp));
-  s = add(s, mul(c.czm, zm));
-  return s;
+  if constexpr (sizeof(T) == 4) {
+    float s = __fmul_rn(c.cxp, xp);
+    s = __fmaf_rn(c.cxm, xm, s);
+    s = __fmaf_rn(c.cyp, yp, s);
+    s = __fmaf_rn(c.cym, ym, s);
+    s = __fmaf_rn(c.czp, zp, s);
+    return __fmaf_rn(c.czm, zm, s);
+  } else {
+    T s = mul(c.cxp, xp);
+    s = add(s, mul(c.cxm, xm));
+    s = add(s, mul(c.cyp, yp));
+    s = add(s, mul(c.cym, ym));
+    s = add(s, mul(c.czp, zp));
+    s = add(s, mul(c.czm, zm));
+    return s;
+  }
 }
+
+// pp + omega*dp: FP64 two roundings (the reference), FP32 one fused multiply-add
+__device__ __forceinline__ double relax(double pp, double omega, double dp) { return add(pp, mul(omega, dp)); }
+__device__ __forceinline__ float relax(float pp, float omega, float dp) { return __fmaf_rn(omega, dp, pp); }
 
 // Gauss-Seidel update of one cell: (ss - b)/dd, correctly rounded in both precisions (an
 // approximate FP32 division weakens the FP32 preconditioner enough to multiply the iterations).
@@ -396,10 +411,11 @@ __device__ __forceinline__ void x_nbrs(T oc, int okc, int e, int lane, int p, in
 // Grid (ceil(HN/32), ceil(NY/kBY), ceil(NZ/2)); thread = colour-c cells of column (p,j) at
 // planes k0, k0+1.
 // ------------------------------------------------------------------------------------------
-// One colour pass over the two planes k0, k0+1 of column (p, j).  RES: also returns the sum of
-// the squared SOR residuals r = (dd + omega*(c_xm + c_ym + c_zm))*dp/omega of the updated cells
-// (rbsor_core!, NonUniform.jl:907-908); the preconditioner discards them and skips the work.
-template <typename T, bool RES>
+// One colour pass over the NP planes k0 .. k0+NP-1 (NP = 1 or 2) of column (p, j).  RES: also
+// returns the sum of the squared SOR residuals r = (dd + omega*(c_xm + c_ym + c_zm))*dp/omega of
+// the updated cells (rbsor_core!, NonUniform.jl:907-908); the preconditioner discards them and
+// skips the work.  With NP = 2 the two cells share the o-colour column loads.
+template <typename T, bool RES, int NP = 2>
 __device__ __forceinline__ double rb_pass_column(const OpParams<T>& op, T* x, const T* __restrict__ bb, int color,
                                                  T omega, int lane, int p, int j, int k0) {
   const Geo& g = op.g;
@@ -408,11 +424,11 @@ __device__ __forceinline__ double rb_pass_column(const OpParams<T>& op, T* x, co
   const uint8_t* key = op.key;
   const int HP2 = 2 * g.HP, PL = (int)g.plane;
   const int ro0 = g.row(o, j, k0), rc0 = g.row(color, j, k0);
-  // o-colour column at (p, j), planes k0-1 .. k0+2
-  T col[4];
-  int kcol[4];
+  // o-colour column at (p, j), planes k0-1 .. k0+NP
+  T col[NP + 2];
+  int kcol[NP + 2];
 #pragma unroll
-  for (int t = 0; t < 4; ++t) {
+  for (int t = 0; t < NP + 2; ++t) {
     col[t] = T(0);
     kcol[t] = 0;
     if (pok && k0 - 1 + t <= g.MZ - 1) {
@@ -421,11 +437,11 @@ __device__ __forceinline__ double rb_pass_column(const OpParams<T>& op, T* x, co
       kcol[t] = key[a];
     }
   }
-  T ym[2], yp[2], pp[2], bv[2];
-  int kym[2], kyp[2], kc[2];
-  bool ok[2];
+  T ym[NP], yp[NP], pp[NP], bv[NP];
+  int kym[NP], kyp[NP], kc[NP];
+  bool ok[NP];
 #pragma unroll
-  for (int u = 0; u < 2; ++u) {
+  for (int u = 0; u < NP; ++u) {
     const int k = k0 + u, e = (1 + color + j + k) & 1, i = 2 * p + e;
     ok[u] = pok && k <= g.NZ && i >= 1 && i <= g.NX;
     ym[u] = yp[u] = pp[u] = bv[u] = T(0);
@@ -441,16 +457,16 @@ __device__ __forceinline__ double rb_pass_column(const OpParams<T>& op, T* x, co
       bv[u] = bb[ac];
     }
   }
-  T xm[2], xp[2];
-  int kxm[2], kxp[2];
+  T xm[NP], xp[NP];
+  int kxm[NP], kxp[NP];
 #pragma unroll
-  for (int u = 0; u < 2; ++u) {
+  for (int u = 0; u < NP; ++u) {
     const int e = (1 + color + j + k0 + u) & 1;
     x_nbrs<T, true>(col[u + 1], kcol[u + 1], e, lane, p, g.HN, x, key, ro0 + u * PL, xm[u], xp[u], kxm[u], kxp[u]);
   }
   double acc = 0.0;
 #pragma unroll
-  for (int u = 0; u < 2; ++u) {
+  for (int u = 0; u < NP; ++u) {
     if (!ok[u]) continue;
     const int ac = rc0 + u * PL + p;
     Coef<T> c;
@@ -459,7 +475,7 @@ __device__ __forceinline__ double rb_pass_column(const OpParams<T>& op, T* x, co
       continue;
     const T ss = nb_sum(c, xp[u], xm[u], yp[u], ym[u], col[u + 2], col[u]);
     const T dp = sub(gs_div(sub(ss, bv[u]), c.dd), pp[u]);  // * m0 (= 1)
-    x[ac] = add(pp[u], mul(omega, dp));
+    x[ac] = relax(pp[u], omega, dp);
     if constexpr (RES) {
       const T r = dvd(mul(add(c.dd, mul(omega, add(add(c.cxm, c.cym), c.czm))), dp), omega);
       acc = add(acc, mul((double)r, (double)r));
@@ -468,12 +484,12 @@ __device__ __forceinline__ double rb_pass_column(const OpParams<T>& op, T* x, co
   return acc;
 }
 
-// The colour pass has no reduction, so its block height BY (rows per block) does not change any
-// result; the autotuner picks it per grid among kRbRows.  Every shape keeps the register cap of
-// H2G_MINB blocks of 256 threads per SM.
+// The colour pass has no reduction, so its block height BY (rows per block) and its planes per
+// thread NP change no result; the autotuner picks them per grid among kRbRows x {1, 2}.  Every
+// shape keeps the register cap of H2G_MINB blocks of 256 threads per SM.
 constexpr int kRbRows[4] = {2, 4, 8, 16};
 
-template <typename T, int BY = kBY>
+template <typename T, int BY = kBY, int NP = 2>
 __global__ void __launch_bounds__(kBX * BY, (H2G_MINB * kBY) / BY)
     k_rb_pass(OpParams<T> op, T* x, const T* __restrict__ bb, int color, T omega,
               const SolverState* __restrict__ st) {
@@ -481,9 +497,9 @@ __global__ void __launch_bounds__(kBX * BY, (H2G_MINB * kBY) / BY)
   if (st && st->stop) return;
   const int lane = threadIdx.x, p = blockIdx.x * kBX + lane;
   const int j = 1 + blockIdx.y * BY + threadIdx.y;
-  const int k0 = 1 + 2 * blockIdx.z;
+  const int k0 = 1 + NP * blockIdx.z;
   if (j > op.g.NY) return;  // uniform per warp
-  rb_pass_column<T, false>(op, x, bb, color, omega, lane, p, j, k0);
+  rb_pass_column<T, false, NP>(op, x, bb, color, omega, lane, p, j, k0);
 }
 
 // rbsor_core! with its residual (NonUniform.jl:848-915) for solveSOR! (NonUniform.jl:1004-1051):

@@ -143,6 +143,7 @@ struct Solver {
   bool no_cond = false;
   bool pdl = true;  // programmatic dependent launch of the solver kernels
   int rb_rows = kBY;      // rows per block of the colour pass (autotuned)
+  int rb_planes = 2;      // planes per thread of the colour pass (autotuned)
   bool ax_dd = false;     // CalcAX reads dd from the per-cell array (autotuned)
   bool rb_tuned = false;  // rb_rows chosen (by the tuner or h2g_set_tuning)
 
@@ -197,17 +198,30 @@ static void launch_ax(const Solver* s, cudaStream_t cs, const OpParams<T>& op, T
   else launch(s, k_ax<T, NDOT, TI, false>, ag, blk, cs, op, y, x, u, w, st, s->partials, stage);
 }
 
-// One colour pass with the handle's block height.
+// One colour pass with the handle's launch shape (rows per block, planes per thread).
+template <typename T, int NP>
+static void launch_rb_np(const Solver* s, cudaStream_t cs, const OpParams<T>& op, T* x, const T* bb, int color,
+                         T omega, const SolverState* st) {
+  const Geo& g = op.g;
+  const int gz = (g.NZ + NP - 1) / NP;
+  const int gx = (g.HN + kBX - 1) / kBX;
+  switch (s->rb_rows) {
+    case 2: launch(s, k_rb_pass<T, 2, NP>, dim3(gx, (g.NY + 1) / 2, gz), dim3(kBX, 2), cs, op, x, bb, color, omega, st);
+      break;
+    case 4: launch(s, k_rb_pass<T, 4, NP>, dim3(gx, (g.NY + 3) / 4, gz), dim3(kBX, 4), cs, op, x, bb, color, omega, st);
+      break;
+    case 16:
+      launch(s, k_rb_pass<T, 16, NP>, dim3(gx, (g.NY + 15) / 16, gz), dim3(kBX, 16), cs, op, x, bb, color, omega, st);
+      break;
+    default: launch(s, k_rb_pass<T, 8, NP>, dim3(gx, (g.NY + 7) / 8, gz), dim3(kBX, 8), cs, op, x, bb, color, omega, st);
+      break;
+  }
+}
 template <typename T>
 static void launch_rb(const Solver* s, cudaStream_t cs, const OpParams<T>& op, T* x, const T* bb, int color, T omega,
                       const SolverState* st) {
-  const Geo& g = op.g;
-  switch (s->rb_rows) {
-    case 2: launch(s, k_rb_pass<T, 2>, rb_grid(g, 2), dim3(kBX, 2), cs, op, x, bb, color, omega, st); break;
-    case 4: launch(s, k_rb_pass<T, 4>, rb_grid(g, 4), dim3(kBX, 4), cs, op, x, bb, color, omega, st); break;
-    case 16: launch(s, k_rb_pass<T, 16>, rb_grid(g, 16), dim3(kBX, 16), cs, op, x, bb, color, omega, st); break;
-    default: launch(s, k_rb_pass<T, 8>, rb_grid(g, 8), dim3(kBX, 8), cs, op, x, bb, color, omega, st); break;
-  }
+  if (s->rb_planes == 1) launch_rb_np<T, 1>(s, cs, op, x, bb, color, omega, st);
+  else launch_rb_np<T, 2>(s, cs, op, x, bb, color, omega, st);
 }
 
 static size_t partials_needed(const Solver* s) {
@@ -1275,11 +1289,13 @@ static int tune_rows_t(Solver* s, const OpParams<T>& op, int* best_rows) {
     cudaEventDestroy(e0);
     return fail(H2G_CUDA_ERROR, "event creation failed");
   }
-  const int saved = s->rb_rows;
+  const int saved = s->rb_rows, saved_np = s->rb_planes;
   float best = 1e30f;
   int rc = H2G_OK;
-  for (int by : kRbRows) {
+  for (int shape = 0; shape < 8; ++shape) {
+    const int by = kRbRows[shape & 3], np = 1 + (shape >> 2);
     s->rb_rows = by;
+    s->rb_planes = np;
     for (int r = 0; r < 2; ++r) {
       launch_rb<T>(s, s->stream, op, xa, (const T*)xb, 0, T(1), nullptr);
       launch_rb<T>(s, s->stream, op, xa, (const T*)xb, 1, T(1), nullptr);
@@ -1298,10 +1314,11 @@ static int tune_rows_t(Solver* s, const OpParams<T>& op, int* best_rows) {
     }
     if (ms < best) {
       best = ms;
-      *best_rows = by;
+      *best_rows = by | (np << 5);
     }
   }
   s->rb_rows = saved;
+  s->rb_planes = saved_np;
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   return rc;
@@ -1365,10 +1382,16 @@ static int autotune(Solver* s) {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     g_tune_cache[key] = cached;
   }
-  if (!valid_rows(rows)) rows = cached & 0xff;
+  int planes = (cached >> 5) & 3;
+  if (const char* e = getenv("H2G_RB_PLANES")) {
+    const int np = atoi(e);
+    if (np == 1 || np == 2) planes = np;
+  }
+  if (!valid_rows(rows)) rows = cached & 0x1f;
   if (dd < 0) dd = cached >> 8;
-  if (rows != s->rb_rows || (dd != 0) != s->ax_dd) invalidate_graphs(s);
+  if (rows != s->rb_rows || planes != s->rb_planes || (dd != 0) != s->ax_dd) invalidate_graphs(s);
   s->rb_rows = rows;
+  s->rb_planes = planes;
   s->ax_dd = dd != 0;
   s->rb_tuned = true;
   return H2G_OK;
@@ -1897,17 +1920,18 @@ int h2g_adjoint_transient(h2g_solver* h, const h2g_bc* bc, int nt, const double*
                                 dJ_dlnlam, out);
 }
 
-int h2g_autotune(h2g_solver* h, int* rows) {
+int h2g_autotune(h2g_solver* h, int* rows, int* planes) {
   if (int rc = h2g::check_handle(h)) return rc;
   Solver* s = S(h);
   if (!s->grid_set || !s->fields_set) return fail(H2G_BAD_ARG, "h2g_set_grid and h2g_set_fields must come first");
   CK(cudaSetDevice(s->device));
   if (int rc = h2g::autotune(s)) return rc;
   if (rows) *rows = s->rb_rows;
+  if (planes) *planes = s->rb_planes;
   return H2G_OK;
 }
 
-int h2g_set_tuning(h2g_solver* h, int rows) {
+int h2g_set_tuning(h2g_solver* h, int rows, int planes) {
   if (int rc = h2g::check_handle(h)) return rc;
   Solver* s = S(h);
   if (rows == 0) {
@@ -1915,8 +1939,10 @@ int h2g_set_tuning(h2g_solver* h, int rows) {
     return H2G_OK;
   }
   if (!h2g::valid_rows(rows)) return fail(H2G_BAD_ARG, "rows per block must be 2, 4, 8 or 16 (0: tune)");
-  if (rows != s->rb_rows) h2g::invalidate_graphs(s);
+  if (planes != 1 && planes != 2) return fail(H2G_BAD_ARG, "planes per thread must be 1 or 2");
+  if (rows != s->rb_rows || planes != s->rb_planes) h2g::invalidate_graphs(s);
   s->rb_rows = rows;
+  s->rb_planes = planes;
   s->rb_tuned = true;
   return H2G_OK;
 }

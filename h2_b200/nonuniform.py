@@ -214,15 +214,16 @@ class Solver:
         L.check(self.lib.h2g_preconditioner(self.h, _ptr(self._arr(bb, "bb")), _ptr(xx), smoother_selector(smoother)))
         return xx
 
-    def autotune(self) -> int:
-        """Run the launch-shape tuner now; returns the colour pass's rows per block."""
-        r = C.c_int(0)
-        L.check(self.lib.h2g_autotune(self.h, C.byref(r)))
-        return r.value
+    def autotune(self) -> tuple:
+        """Run the launch-shape tuner now; returns the colour pass's (rows per block, planes per
+        thread)."""
+        r, p = C.c_int(0), C.c_int(0)
+        L.check(self.lib.h2g_autotune(self.h, C.byref(r), C.byref(p)))
+        return r.value, p.value
 
-    def set_tuning(self, rows: int):
-        """Force the colour pass's rows per block (2, 4, 8, 16); 0 tunes again."""
-        L.check(self.lib.h2g_set_tuning(self.h, int(rows)))
+    def set_tuning(self, rows: int, planes: int = 2):
+        """Force the colour pass's shape (rows 2, 4, 8, 16; planes 1, 2); rows = 0 tunes again."""
+        L.check(self.lib.h2g_set_tuning(self.h, int(rows), int(planes)))
 
     def bench_kernel(self, kind: int, reps: int) -> int:
         n = C.c_int()

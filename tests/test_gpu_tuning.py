@@ -1,5 +1,6 @@
-"""Launch-shape tuning of the colour pass: every block height gives bit-identical results (the
-pass has no reduction), the tuner picks one of the allowed heights and caches it per grid."""
+"""Launch-shape tuning of the colour pass: every block height and planes-per-thread choice gives
+bit-identical results (the pass has no reduction); the tuner picks an allowed shape and caches
+it per grid."""
 import os
 
 import numpy as np
@@ -16,9 +17,9 @@ pytestmark = pytest.mark.gpu
 def test_heights_give_identical_solves(oracle, precision):
     prob = mode3_model(oracle, 40)
     ref = None
-    for rows in (2, 4, 8, 16):
+    for rows, planes in ((2, 2), (4, 2), (8, 2), (16, 2), (4, 1), (8, 1)):
         s = make_solver(prob, precision=precision)
-        s.set_tuning(rows)
+        s.set_tuning(rows, planes)
         st, res = s.solve("pbicgstab", tol=1e-8, maxItr=20000, smoother="gs")
         assert st == 0
         out = (res.itr, res.res0, res.res, s.get_theta())
@@ -35,11 +36,13 @@ def test_tuner_choice_is_cached(oracle):
     prob = mode3_model(oracle, 32)
     s1 = make_solver(prob)
     r1 = s1.autotune()
-    assert r1 in (2, 4, 8, 16)
+    assert r1[0] in (2, 4, 8, 16) and r1[1] in (1, 2)
     s2 = make_solver(prob)
     assert s2.autotune() == r1
     with pytest.raises(h2_b200.H2GError):
         s2.set_tuning(3)
+    with pytest.raises(h2_b200.H2GError):
+        s2.set_tuning(4, 3)
     s2.set_tuning(0)  # tune again: the cached choice comes back
     assert s2.autotune() == r1
     s1.close()
