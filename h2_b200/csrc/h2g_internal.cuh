@@ -114,6 +114,7 @@ struct OpParams {
   const T* rc;         // rho*cp per cell (device layout), transient only
   const T* dzk;        // [MZ] dZ
   const T* ddv;        // dd per cell (device layout), precomputed with the tables; may be null
+  const unsigned long long* nkey;  // per cell: own key and the 6 neighbours' keys, one byte each
   T czm, czp;          // convective terms of the z-, z+ faces
   T dx0, dy0, ddt;
   int P;

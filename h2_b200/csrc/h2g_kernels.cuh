@@ -33,6 +33,10 @@ namespace h2g {
 #ifndef H2G_DD_ARRAY
 #define H2G_DD_ARRAY 1
 #endif
+// the smoother reads the 7 keys a cell needs as one 8-byte word per cell (1) or byte by byte (0)
+#ifndef H2G_NKEY
+#define H2G_NKEY 1
+#endif
 
 constexpr int kBX = 32;       // threads along the half-row
 constexpr int kBY = H2G_BY;   // rows per block
@@ -365,7 +369,7 @@ __device__ __forceinline__ T ldro(const T* p) { return __ldg(p); }
 
 // x-neighbours of a colour-c cell at position p with parity e (x-1 = o[p-1+e], x+1 = o[p+e]),
 // given the o-colour value and key of this lane's column at that plane.  All lanes must call it.
-template <typename T, bool VAL, typename TI = T>
+template <typename T, bool VAL, typename TI = T, bool KEYS = true>
 __device__ __forceinline__ void x_nbrs(T oc, int okc, int e, int lane, int p, int HN, const TI* x,
                                        const uint8_t* key, int rowo, T& xm, T& xp, int& kxm, int& kxp) {
 #if H2G_XNB_LOAD
@@ -376,7 +380,7 @@ __device__ __forceinline__ void x_nbrs(T oc, int okc, int e, int lane, int p, in
   int ko = 0;
   if (q >= 0 && q < HN) {
     if (VAL) other = (T)ldro(x + rowo + q);
-    ko = key[rowo + q];
+    if (KEYS) ko = key[rowo + q];
   }
   if (e) {
     xm = oc; kxm = okc; xp = other; kxp = ko;
@@ -427,6 +431,7 @@ __device__ __forceinline__ double rb_pass_column(const OpParams<T>& op, T* x, co
   // o-colour column at (p, j), planes k0-1 .. k0+NP
   T col[NP + 2];
   int kcol[NP + 2];
+  constexpr bool NK = H2G_NKEY != 0;
 #pragma unroll
   for (int t = 0; t < NP + 2; ++t) {
     col[t] = T(0);
@@ -434,11 +439,12 @@ __device__ __forceinline__ double rb_pass_column(const OpParams<T>& op, T* x, co
     if (pok && k0 - 1 + t <= g.MZ - 1) {
       const int a = ro0 + (t - 1) * PL + p;
       col[t] = ldro(x + a);
-      kcol[t] = key[a];
+      if (!NK) kcol[t] = key[a];
     }
   }
   T ym[NP], yp[NP], pp[NP], bv[NP];
   int kym[NP], kyp[NP], kc[NP];
+  unsigned long long nk[NP];
   bool ok[NP];
 #pragma unroll
   for (int u = 0; u < NP; ++u) {
@@ -446,13 +452,18 @@ __device__ __forceinline__ double rb_pass_column(const OpParams<T>& op, T* x, co
     ok[u] = pok && k <= g.NZ && i >= 1 && i <= g.NX;
     ym[u] = yp[u] = pp[u] = bv[u] = T(0);
     kym[u] = kyp[u] = kc[u] = 0;
+    nk[u] = 0ull;
     if (ok[u]) {
       const int ao = ro0 + u * PL + p, ac = rc0 + u * PL + p;
       ym[u] = ldro(x + ao - HP2);
       yp[u] = ldro(x + ao + HP2);
-      kym[u] = key[ao - HP2];
-      kyp[u] = key[ao + HP2];
-      kc[u] = key[ac];
+      if (NK) {
+        nk[u] = __ldg(op.nkey + ac);
+      } else {
+        kym[u] = key[ao - HP2];
+        kyp[u] = key[ao + HP2];
+        kc[u] = key[ac];
+      }
       pp[u] = x[ac];
       bv[u] = bb[ac];
     }
@@ -462,7 +473,8 @@ __device__ __forceinline__ double rb_pass_column(const OpParams<T>& op, T* x, co
 #pragma unroll
   for (int u = 0; u < NP; ++u) {
     const int e = (1 + color + j + k0 + u) & 1;
-    x_nbrs<T, true>(col[u + 1], kcol[u + 1], e, lane, p, g.HN, x, key, ro0 + u * PL, xm[u], xp[u], kxm[u], kxp[u]);
+    x_nbrs<T, true, T, !NK>(col[u + 1], kcol[u + 1], e, lane, p, g.HN, x, key, ro0 + u * PL, xm[u], xp[u], kxm[u],
+                            kxp[u]);
   }
   double acc = 0.0;
 #pragma unroll
@@ -470,9 +482,16 @@ __device__ __forceinline__ double rb_pass_column(const OpParams<T>& op, T* x, co
     if (!ok[u]) continue;
     const int ac = rc0 + u * PL + p;
     Coef<T> c;
-    if (!cell_coef<T, true>(op, k0 + u, (uint8_t)kc[u], (uint8_t)kxm[u], (uint8_t)kxp[u], (uint8_t)kym[u],
-                            (uint8_t)kyp[u], (uint8_t)kcol[u], (uint8_t)kcol[u + 2], ac, c))
-      continue;
+    bool has;
+    if (NK) {
+      const unsigned long long w = nk[u];  // own, x-, x+, y-, y+, z-, z+ keys in bytes 0..6
+      has = cell_coef<T, true>(op, k0 + u, (uint8_t)w, (uint8_t)(w >> 8), (uint8_t)(w >> 16), (uint8_t)(w >> 24),
+                               (uint8_t)(w >> 32), (uint8_t)(w >> 40), (uint8_t)(w >> 48), ac, c);
+    } else {
+      has = cell_coef<T, true>(op, k0 + u, (uint8_t)kc[u], (uint8_t)kxm[u], (uint8_t)kxp[u], (uint8_t)kym[u],
+                               (uint8_t)kyp[u], (uint8_t)kcol[u], (uint8_t)kcol[u + 2], ac, c);
+    }
+    if (!has) continue;
     const T ss = nb_sum(c, xp[u], xm[u], yp[u], ym[u], col[u + 2], col[u]);
     const T dp = sub(gs_div(sub(ss, bv[u]), c.dd), pp[u]);  // * m0 (= 1)
     x[ac] = relax(pp[u], omega, dp);
@@ -1289,6 +1308,22 @@ __global__ void __launch_bounds__(256) k_make_dd(OpParams<T> op, T* __restrict__
                                        key[g.off(i, j - 1, k)], key[g.off(i, j + 1, k)], key[g.off(i, j, k - 1)],
                                        key[g.off(i, j, k + 1)], o, c);
   ddv[o] = has ? c.dd : T(1);
+}
+
+// Per interior cell, the 7 keys its stencil reads packed in one word: own key (byte 0) and the
+// keys of its x-, x+, y-, y+, z-, z+ neighbours (bytes 1..6).  Guards and padding: 0.
+__global__ void __launch_bounds__(256) k_make_nkeys(Geo g, const uint8_t* __restrict__ key,
+                                                     unsigned long long* __restrict__ nk) {
+  const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = 1 + blockIdx.y, k = 1 + blockIdx.z;
+  if (i > g.NX) return;
+  const int o = g.off(i, j, k);
+  const int nb[6] = {g.off(i - 1, j, k), g.off(i + 1, j, k), g.off(i, j - 1, k),
+                     g.off(i, j + 1, k), g.off(i, j, k - 1), g.off(i, j, k + 1)};
+  unsigned long long w = key[o];
+#pragma unroll
+  for (int f = 0; f < 6; ++f) w |= (unsigned long long)key[nb[f]] << (8 * (f + 1));
+  nk[o] = w;
 }
 
 // ------------------------------------------------------------------------------------------

@@ -99,6 +99,7 @@ struct Solver {
   int steady = 1;
   // keys
   uint8_t* key = nullptr;
+  unsigned long long* nkey = nullptr;  // the 7 stencil keys of every cell (smoother)
   int P = 0;
   std::vector<double> lam_values;
   unsigned long long* slots = nullptr;
@@ -256,6 +257,7 @@ static OpParams<T> op_params_rc(const Solver* s, const OpTables<T>& t, const T* 
   op.rc = rc;
   op.dzk = t.dzk;
   op.ddv = t.ddv;
+  op.nkey = s->nkey;
   const double dx0 = s->dx, dy0 = s->dy;
   op.czm = (T)((s->HC[4] * dx0) * dy0);
   op.czp = (T)((s->HC[5] * dx0) * dy0);
@@ -293,7 +295,7 @@ static void destroy(Solver* s) {
   cudaSetDevice(s->device);
   for (auto& gk : s->graphs)
     for (auto& gg : gk) gg.reset();
-  cudaFree(s->key); cudaFree(s->slots); cudaFree(s->slot_index); cudaFree(s->flags);
+  cudaFree(s->key); cudaFree(s->nkey); cudaFree(s->slots); cudaFree(s->slot_index); cudaFree(s->flags);
   free_tables64(s->t64);
   free_tables32(s->t32);
   cudaFree(s->rc64); cudaFree(s->rc32);
@@ -1550,6 +1552,16 @@ static int set_fields(Solver* s, const double* lam, const double* mask, const do
   if (rho && s->precision != H2G_FP64) {
     k_make_keys<float><<<grid, 128, 0, s->stream>>>(g, s->stage[0], s->stage[1], s->stage[2], s->stage[3], s->slots,
                                                     s->slot_index, s->key, s->rc32);
+    CKL();
+  }
+  if (!s->nkey) {
+    CK(cudaMalloc(&s->nkey, sizeof(unsigned long long) * (size_t)g.n));
+    CK(cudaMemsetAsync(s->nkey, 0, sizeof(unsigned long long) * (size_t)g.n, s->stream));
+    invalidate_graphs(s);
+  }
+  {
+    const dim3 gi((g.NX + 127) / 128, g.NY, g.NZ);
+    k_make_nkeys<<<gi, 128, 0, s->stream>>>(g, s->key, s->nkey);
     CKL();
   }
   s->rc_valid = rho != nullptr;
