@@ -595,21 +595,34 @@ __global__ void __launch_bounds__(kThreads) k_rb_first(OpParams<T> op, T* __rest
   }
   // keys for the colour-0 cell: its own and its colour-1 neighbours
   int k1c = 0, k1m = 0, k1p = 0, kym = 0, kyp = 0, k0c = 0;
-  if (!copy_only && pok) {
-    const int a1 = r1 + p;
-    k1c = key[a1];
-    if (ok[0]) {
-      k1m = key[a1 - PL];
-      k1p = key[a1 + PL];
-      kym = key[a1 - HP2];
-      kyp = key[a1 + HP2];
-      k0c = key[r0 + p];
-    }
-  }
   int kxm = 0, kxp = 0;
-  if (!copy_only) {
-    T dm, dp_;
-    x_nbrs<T, false>(T(0), k1c, e0, lane, p, g.HN, (const T*)nullptr, key, r1, dm, dp_, kxm, kxp);
+  if (H2G_NKEY) {
+    if (!copy_only && ok[0]) {
+      const unsigned long long w = __ldg(op.nkey + r0 + p);  // own, x-, x+, y-, y+, z-, z+
+      k0c = (int)(w & 0xff);
+      kxm = (int)((w >> 8) & 0xff);
+      kxp = (int)((w >> 16) & 0xff);
+      kym = (int)((w >> 24) & 0xff);
+      kyp = (int)((w >> 32) & 0xff);
+      k1m = (int)((w >> 40) & 0xff);
+      k1p = (int)((w >> 48) & 0xff);
+    }
+  } else {
+    if (!copy_only && pok) {
+      const int a1 = r1 + p;
+      k1c = key[a1];
+      if (ok[0]) {
+        k1m = key[a1 - PL];
+        k1p = key[a1 + PL];
+        kym = key[a1 - HP2];
+        kyp = key[a1 + HP2];
+        k0c = key[r0 + p];
+      }
+    }
+    if (!copy_only) {
+      T dm, dp_;
+      x_nbrs<T, false>(T(0), k1c, e0, lane, p, g.HN, (const T*)nullptr, key, r1, dm, dp_, kxm, kxp);
+    }
   }
 #pragma unroll
   for (int col = 0; col < 2; ++col) {
@@ -645,7 +658,7 @@ struct Pair {
   int ky0m, ky0p, ky1m, ky1p;
 };
 
-template <typename T, typename TI>
+template <typename T, typename TI, bool KEYS = true>
 __device__ __forceinline__ void load_pair(const Geo& g, const TI* x, const uint8_t* key, int r0, int p, bool pok,
                                           Pair<T, TI>& P) {
   const int r1 = r0 + g.HP, PL = (int)g.plane, HP2 = 2 * g.HP;
@@ -662,17 +675,21 @@ __device__ __forceinline__ void load_pair(const Geo& g, const TI* x, const uint8
     const int a0 = r0 + (t - 1) * PL + p, a1 = r1 + (t - 1) * PL + p;
     P.c0[t] = (T)ldro(x + a0);
     P.c1[t] = (T)ldro(x + a1);
-    P.kc0[t] = key[a0];
-    P.kc1[t] = key[a1];
+    if (KEYS) {
+      P.kc0[t] = key[a0];
+      P.kc1[t] = key[a1];
+    }
   }
   P.y0m = (T)ldro(x + r0 + p - HP2);
   P.y0p = (T)ldro(x + r0 + p + HP2);
   P.y1m = (T)ldro(x + r1 + p - HP2);
   P.y1p = (T)ldro(x + r1 + p + HP2);
-  P.ky0m = key[r0 + p - HP2];
-  P.ky0p = key[r0 + p + HP2];
-  P.ky1m = key[r1 + p - HP2];
-  P.ky1p = key[r1 + p + HP2];
+  if (KEYS) {
+    P.ky0m = key[r0 + p - HP2];
+    P.ky0p = key[r0 + p + HP2];
+    P.ky1m = key[r1 + p - HP2];
+    P.ky1p = key[r1 + p + HP2];
+  }
 }
 
 // ------------------------------------------------------------------------------------------
@@ -713,13 +730,20 @@ __global__ void __launch_bounds__(kThreads) k_ax(OpParams<T> op, T* __restrict__
         if (NDOT >= 2) ww[col] = w[ci];
       }
     }
+    constexpr bool NK = H2G_NKEY != 0;
+    unsigned long long nk[2] = {0ull, 0ull};
+    if (NK) {
+#pragma unroll
+      for (int col = 0; col < 2; ++col)
+        if (ok[col]) nk[col] = __ldg(op.nkey + (col ? r1 : r0) + p);
+    }
     Pair<T, TI> P;
-    load_pair<T, TI>(g, x, key, r0, p, pok, P);
+    load_pair<T, TI, !NK>(g, x, key, r0, p, pok, P);
     T xm0, xp0, xm1, xp1;
     int kxm0, kxp0, kxm1, kxp1;
     // colour-0 cell: neighbours of colour 1; colour-1 cell: neighbours of colour 0
-    x_nbrs<T, true, TI>(P.c1[1], P.kc1[1], e0, lane, p, g.HN, x, key, r1, xm0, xp0, kxm0, kxp0);
-    x_nbrs<T, true, TI>(P.c0[1], P.kc0[1], e0 ^ 1, lane, p, g.HN, x, key, r0, xm1, xp1, kxm1, kxp1);
+    x_nbrs<T, true, TI, !NK>(P.c1[1], P.kc1[1], e0, lane, p, g.HN, x, key, r1, xm0, xp0, kxm0, kxp0);
+    x_nbrs<T, true, TI, !NK>(P.c0[1], P.kc0[1], e0 ^ 1, lane, p, g.HN, x, key, r0, xm1, xp1, kxm1, kxp1);
 #pragma unroll
     for (int col = 0; col < 2; ++col) {
       if (!ok[col]) continue;
@@ -727,12 +751,20 @@ __global__ void __launch_bounds__(kThreads) k_ax(OpParams<T> op, T* __restrict__
       Coef<T> c;
       T out = T(0);
       bool has;
-      if (col == 0)
-        has = cell_coef<T, DD && sizeof(T) == 8>(op, k, (uint8_t)P.kc0[1], (uint8_t)kxm0, (uint8_t)kxp0, (uint8_t)P.ky1m, (uint8_t)P.ky1p,
-                        (uint8_t)P.kc1[0], (uint8_t)P.kc1[2], ci, c);
-      else
-        has = cell_coef<T, DD && sizeof(T) == 8>(op, k, (uint8_t)P.kc1[1], (uint8_t)kxm1, (uint8_t)kxp1, (uint8_t)P.ky0m, (uint8_t)P.ky0p,
-                        (uint8_t)P.kc0[0], (uint8_t)P.kc0[2], ci, c);
+      if (NK) {
+        const unsigned long long wk = nk[col];  // own, x-, x+, y-, y+, z-, z+ keys in bytes 0..6
+        has = cell_coef<T, DD && sizeof(T) == 8>(op, k, (uint8_t)wk, (uint8_t)(wk >> 8), (uint8_t)(wk >> 16),
+                                                 (uint8_t)(wk >> 24), (uint8_t)(wk >> 32), (uint8_t)(wk >> 40),
+                                                 (uint8_t)(wk >> 48), ci, c);
+      } else if (col == 0) {
+        has = cell_coef<T, DD && sizeof(T) == 8>(op, k, (uint8_t)P.kc0[1], (uint8_t)kxm0, (uint8_t)kxp0,
+                                                 (uint8_t)P.ky1m, (uint8_t)P.ky1p, (uint8_t)P.kc1[0],
+                                                 (uint8_t)P.kc1[2], ci, c);
+      } else {
+        has = cell_coef<T, DD && sizeof(T) == 8>(op, k, (uint8_t)P.kc1[1], (uint8_t)kxm1, (uint8_t)kxp1,
+                                                 (uint8_t)P.ky0m, (uint8_t)P.ky0p, (uint8_t)P.kc0[0],
+                                                 (uint8_t)P.kc0[2], ci, c);
+      }
       if (has) {
         if (col == 0) out = apply_a(c, P.c0[1], xp0, xm0, P.y1p, P.y1m, P.c1[2], P.c1[0]);
         else out = apply_a(c, P.c1[1], xp1, xm1, P.y0p, P.y0m, P.c0[2], P.c0[0]);
