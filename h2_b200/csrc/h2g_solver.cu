@@ -1425,7 +1425,6 @@ static int create(int MX, int MY, int MZ, int precision, Solver** out) {
   s->no_cond = nc && nc[0] == '1';
   const char* np = getenv("H2G_NO_PDL");
   s->pdl = !(np && np[0] == '1');
-  int rc = H2G_OK;
   auto bail = [&](int code) {
     destroy(s);
     return code;
@@ -1463,7 +1462,6 @@ static int create(int MX, int MY, int MZ, int precision, Solver** out) {
     return bail(fail(H2G_CUDA_ERROR, "cudaMallocHost failed"));
   if (cudaStreamCreateWithFlags(&s->cap, cudaStreamNonBlocking) != cudaSuccess)
     return bail(fail(H2G_CUDA_ERROR, "cudaStreamCreate failed"));
-  (void)rc;
   *out = s;
   return H2G_OK;
 }

@@ -1,4 +1,4 @@
-"""GPU PBiCGSTAB!/CG! against the oracle (theta within 1e-3 K,
+"""GPU PBiCGSTAB!/CG! against the oracle (parity tolerances: theta within 1e-3 K,
 FP64 iteration counts within 10 %), through the C ABI, plus the status/edge cases of the
 reference's control flow (res0 == 0, maxItr, breakdown, non-finite input)."""
 import numpy as np
