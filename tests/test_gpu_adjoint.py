@@ -107,3 +107,23 @@ def test_hsrc_gradient_finite_differences(case):
     fd = (_J_of(case["beta"], hsrc=base + eps * v) - _J_of(case["beta"], hsrc=base - eps * v)) / (2 * eps)
     ad = float(np.sum(case["gh"] * v))
     assert abs(fd - ad) <= 1e-5 * abs(ad), (fd, ad)
+
+
+def test_mixed_precision_gradient(case):
+    """The same gradients from a handle whose solves use the FP32 preconditioner (H2G_MIXED):
+    both solves still converge on the FP64 true residual (to 1e-9: the FP32 smoother's noise
+    keeps the mixed solver from much tighter tolerances), so the gradients agree with the FP64
+    ones to about that tolerance."""
+    m = case["m"]
+    w = m.wk
+    s = h2_b200.Solver(*m.shape, precision="mixed")
+    s.set_grid(m.ZC, m.dZ, m.dx, m.dy, m.dt, m.HC, True)
+    s.set_fields(w.lam, w.mask)
+    s.set_rhs(w.b)
+    s.set_theta(w.theta)
+    J, gh, gl, rf, ra = A.steady_gradient(s, case["w"], P, tol=1e-9)
+    s.close()
+    assert rf.isconverged and ra.isconverged
+    assert abs(J - case["J"]) <= 1e-9 * case["J"]
+    assert np.abs(gh - case["gh"]).max() <= 1e-4 * np.abs(case["gh"]).max()
+    assert np.abs(gl - case["gl"]).max() <= 1e-4 * np.abs(case["gl"]).max()
