@@ -117,6 +117,7 @@ struct Solver {
   double* th_snap = nullptr;
   double* r64 = nullptr;
   double* hsrc = nullptr;      // heat source per cell (device layout), set by h2g_set_hsrc
+  double* th_prev = nullptr;   // theta before a mixed-precision pass (restored on breakdown)
   double* stats = nullptr;     // per-step theta statistics of the transient driver
   int stats_cap = 0;
   double* adj[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // adjoint: w, g, la, G, dJ/dhsrc
@@ -300,7 +301,7 @@ static void destroy(Solver* s) {
   free_tables32(s->t32);
   cudaFree(s->rc64); cudaFree(s->rc32);
   cudaFree(s->th); cudaFree(s->b); cudaFree(s->th_snap); cudaFree(s->r64);
-  cudaFree(s->hsrc); cudaFree(s->stats);
+  cudaFree(s->hsrc); cudaFree(s->stats); cudaFree(s->th_prev);
   for (auto& p : s->adj) cudaFree(p);
   cudaFree(s->lamv);
   cudaFree(s->tstates);
@@ -879,26 +880,65 @@ static int solve_mixed(Solver* s, bool cg, double tol, int maxItr, int smoother,
   int total = 0, status = H2G_NOT_CONVERGED, converged = 0, passes = 0;
   long long launches = 0;
   double res0 = 0.0, res = 1.0, tol_cur = tol;
+  bool escalate = false;
+  const size_t nb = sizeof(double) * (size_t)s->g.n;
+  if (!s->th_prev) CK(cudaMalloc(&s->th_prev, nb));
   for (int restart = 0; restart < 16 && total < maxItr; ++restart) {
+    // theta before this pass: restored if the FP32-preconditioned pass breaks down
+    CK(cudaMemcpyAsync(s->th_prev, s->th, nb, cudaMemcpyDeviceToDevice, s->stream));
     h2g_result r;
     memset(&r, 0, sizeof r);
     const int st = solve_krylov<float>(s, cg, tol_cur, maxItr - total, smoother, verbose && restart == 0,
                                        res_hist ? res_hist + total : nullptr, &r);
     if (st == H2G_BAD_ARG || st == H2G_CUDA_ERROR) return st;
     ++passes;
-    launches += r.launches + 2;
+    launches += r.launches + 3;
     total += r.itr;
     if (restart == 0) res0 = r.res0;
     if (res0 == 0.0) { status = H2G_OK; converged = 1; res = 0.0; break; }
     double tr;
     int rc;
     if ((rc = true_residual(s, &tr))) return rc;
+    if (!std::isfinite(tr) || st == H2G_NONFINITE || st == H2G_BREAKDOWN) {
+      if (!std::isfinite(res0)) { status = H2G_NONFINITE; break; }
+      CK(cudaMemcpyAsync(s->th, s->th_prev, nb, cudaMemcpyDeviceToDevice, s->stream));
+      escalate = true;
+      break;
+    }
     res = tr / res0;
-    if (!std::isfinite(res)) { status = H2G_NONFINITE; break; }
     if (res < tol) { status = H2G_OK; converged = 1; break; }
     if (st != H2G_OK && st != H2G_NOT_CONVERGED) { status = st; break; }
     if (r.itr == 0) break;
     tol_cur = tol / res;  // relative to the restart's initial residual
+  }
+  if (escalate) {
+    // the FP32 smoother's rounding broke the iteration: finish with the FP64 preconditioner
+    // from the last good theta (res is its relative true residual), restarting on the true
+    // residual like the FP32 passes.  The Krylov buffers held FP32 data and possibly non-finite
+    // values (a NaN step length reaches the guard entries of the linear updates); the FP64
+    // kernels need their guards zero, so clear them all first, and again at the end for the FP32
+    // layout of the next mixed solve on this handle.
+    for (int i = 0; i < 8; ++i) CK(cudaMemsetAsync(s->kv[i], 0, s->elem * (size_t)s->g.n, s->stream));
+    status = H2G_NOT_CONVERGED;
+    for (int pass = 0; pass < 4 && total < maxItr; ++pass) {
+      h2g_result r;
+      memset(&r, 0, sizeof r);
+      const int st = solve_krylov<double>(s, cg, tol / res, maxItr - total, smoother, 0,
+                                          res_hist ? res_hist + total : nullptr, &r);
+      if (st == H2G_BAD_ARG || st == H2G_CUDA_ERROR) return st;
+      ++passes;
+      launches += r.launches + 1;
+      total += r.itr;
+      double tr;
+      int rc;
+      if ((rc = true_residual(s, &tr))) return rc;
+      res = tr / res0;
+      if (!std::isfinite(res)) { status = H2G_NONFINITE; break; }
+      if (res < tol) { status = H2G_OK; converged = 1; break; }
+      if (st != H2G_OK && st != H2G_NOT_CONVERGED) { status = st; break; }
+      if (r.itr == 0) break;
+    }
+    for (int i = 0; i < 8; ++i) CK(cudaMemsetAsync(s->kv[i], 0, s->elem * (size_t)s->g.n, s->stream));
   }
   if (out) {
     out->isconverged = converged;
@@ -1380,19 +1420,20 @@ static int autotune(Solver* s) {
   const std::array<int, 4> key = {s->g.MX, s->g.MY, s->g.MZ, s->precision == H2G_FP64 ? 64 : 32};
   int cached = 0;
   {
+    // held while tuning, so that handles of one grid solved concurrently (h2g_batch_solve) tune
+    // once and no two tunings disturb each other's timings
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_tune_cache.find(key);
     if (it != g_tune_cache.end()) cached = it->second;
-  }
-  if (!cached) {
-    int r2 = 0, d2 = 0;
-    int rc = s->precision == H2G_FP64 ? tune_rows_t<double>(s, op_params<double>(s, s->t64), &r2)
-                                      : tune_rows_t<float>(s, op_params<float>(s, s->t32), &r2);
-    if (!rc) rc = tune_ax(s, &d2);
-    if (rc) return rc;
-    cached = r2 | (d2 << 8);
-    std::lock_guard<std::mutex> lk(g_tune_mu);
-    g_tune_cache[key] = cached;
+    if (!cached) {
+      int r2 = 0, d2 = 0;
+      int rc = s->precision == H2G_FP64 ? tune_rows_t<double>(s, op_params<double>(s, s->t64), &r2)
+                                        : tune_rows_t<float>(s, op_params<float>(s, s->t32), &r2);
+      if (!rc) rc = tune_ax(s, &d2);
+      if (rc) return rc;
+      cached = r2 | (d2 << 8);
+      g_tune_cache[key] = cached;
+    }
   }
   int planes = (cached >> 5) & 3;
   if (const char* e = getenv("H2G_RB_PLANES")) {

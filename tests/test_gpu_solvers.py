@@ -232,3 +232,24 @@ def test_verbose_log_format(oracle, capfd):
     assert out[1] == "%10d %24.14E" % (1, float(out[1].split()[1]))
     assert out[-1] == f"Converged at {res.itr}"
     s.close()
+
+
+def test_mixed_converges_on_fine_grid():
+    """480x480x60: the FP32-preconditioned iteration breaks down on this grid (its rounding noise
+    grows with the condition number); the mixed solver restores the last good theta and finishes
+    with the FP64 preconditioner, so it still converges to the FP64 answer."""
+    from h2_b200 import model as M
+    m = M.build_mode3(480, 480, 60)
+    w = m.wk
+    sols = {}
+    for prec in ("fp64", "mixed"):
+        s = h2_b200.Solver(*m.shape, precision=prec)
+        s.set_grid(m.ZC, m.dZ, m.dx, m.dy, m.dt, m.HC, True)
+        s.set_fields(w.lam, w.mask)
+        s.set_rhs(w.b)
+        s.set_theta(w.theta)
+        st, res = s.solve("pbicgstab", tol=1e-8, maxItr=20000, smoother="gs")
+        assert st == 0 and res.isconverged and res.res < 1e-8, (prec, st, res.res)
+        sols[prec] = s.get_theta()
+        s.close()
+    assert np.abs(sols["mixed"] - sols["fp64"]).max() <= THETA_TOL_K
