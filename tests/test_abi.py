@@ -44,6 +44,23 @@ def test_bad_arguments_rejected_on_host(lib):
     assert lib.h2g_cg(None, 1e-6, 10, 1, 0, None, C.byref(res)) == L.H2G_BAD_ARG
     assert b"null" in lib.h2g_last_error()
     assert lib.h2g_destroy(None) == L.H2G_OK
+    # the entry points added beside the reference's path check their handle and sizes first
+    J = C.c_double()
+    bcs = (L.Bc * 6)()
+    assert lib.h2g_sor(None, 1.5, 1e-6, 10, 0, None, C.byref(res)) == L.H2G_BAD_ARG
+    assert lib.h2g_calrhs(None, bcs, 1) == L.H2G_BAD_ARG
+    assert lib.h2g_transient(None, bcs, 3, 0, 1e-6, 10, 1, 0, None, C.byref(res)) == L.H2G_BAD_ARG
+    assert lib.h2g_adjoint(None, None, 8.0, 1e-6, 10, 1, C.byref(J), None, None, None, None) == L.H2G_BAD_ARG
+    assert lib.h2g_adjoint_transient(None, bcs, 3, None, 8.0, 1e-6, 10, 1, 2, C.byref(J), None, None,
+                                     None) == L.H2G_BAD_ARG
+    assert lib.h2g_autotune(None, None, None) == L.H2G_BAD_ARG
+    assert lib.h2g_set_tuning(None, 4, 2) == L.H2G_BAD_ARG
+    hs = (C.c_void_p * 1)()
+    assert lib.h2g_batch_solve(0, hs, 0, 1e-6, 10, 1, 1, (L.Result * 1)()) == L.H2G_BAD_ARG
+    assert lib.h2g_batch_solve(1, hs, 0, 1e-6, 10, 1, 1, (L.Result * 1)()) == L.H2G_BAD_ARG  # null handle
+    assert lib.h2g_batch_solve(1, hs, 7, 1e-6, 10, 1, 1, (L.Result * 1)()) == L.H2G_BAD_ARG
+    assert lib.h2g_calcrk_noalloc(2, 5, 5, None, None, None, None, None, None, None, None, 1.0, 1.0, 1.0, None, 1,
+                                  None, None, None) == L.H2G_BAD_ARG
 
 
 def test_smoother_selector_errors():
