@@ -35,9 +35,10 @@ METRIC = "PBiCGSTAB time-to-eps (s) + stencil HBM GB/s, mixed vs FP64 GPU at 240
 L2_FLUSH_BYTES = 256 << 20
 # DRAM bytes (read + write) of one FP64 RB-GS sweep (two k_rb_pass<double> launches) on the
 # 240x240x30 grid, from one ncu capture of `python -m h2_b200.kernel_bench --kind sweep
-# --precision fp64` (dram__bytes_read.sum 32.0 MB and dram__bytes_write.sum 0 per launch; the
-# pass also reads the precomputed dd of the cells it updates, 6.9 MB, beyond the algorithmic bytes).
-SWEEP_TRAFFIC_F64 = {(240, 30): 2 * 32.006e6}
+# --precision fp64` (dram__bytes_read.sum 37.46 MB and dram__bytes_write.sum < 1 KB per launch;
+# the pass also reads the precomputed dd and the packed stencil keys of the cells it updates,
+# 13.8 MB, beyond the algorithmic bytes).
+SWEEP_TRAFFIC_F64 = {(240, 30): 2 * 37.463e6}
 
 
 def log(*a):
