@@ -1302,10 +1302,12 @@ static int adjoint_transient(Solver* s, const FaceBC& f, int nt, const double* w
 }
 
 // ---- launch-shape tuner --------------------------------------------------------------------
-// The colour pass has no reduction, so its rows per block change no result: the first solve of a
-// handle times every height of kRbRows on the handle's grid (two warm-up and five timed sweeps
-// each, on scratch vectors) and keeps the fastest.  Choices are cached per (grid, smoother
-// precision) for the process; H2G_RB_ROWS in the environment forces one.
+// The colour pass has no reduction, so its launch shape changes no result: the first solve of a
+// handle times every shape (kRbRows x 1 or 2 planes per thread) on the handle's grid (three
+// interleaved rounds of two warm-up and ten timed sweeps each, on scratch vectors) and keeps the
+// fastest.  CalcAX is timed with dd summed and read from the array.  Choices are cached per
+// (grid, smoother precision) for the process; H2G_RB_ROWS, H2G_RB_PLANES and H2G_AX_DD in the
+// environment force them.
 static std::mutex g_tune_mu;
 static std::map<std::array<int, 4>, int> g_tune_cache;
 
@@ -1342,7 +1344,8 @@ static int tune_rows_t(Solver* s, const OpParams<T>& op, int* best_rows) {
   }
   float tbest[8];
   for (int q = 0; q < 8; ++q) tbest[q] = 1e30f;
-  for (int round = 0; round < 2 && rc == H2G_OK; ++round)
+  constexpr int kRounds = 3;
+  for (int round = 0; round < kRounds && rc == H2G_OK; ++round)
   for (int shape = 0; shape < 8; ++shape) {
     const int by = kRbRows[shape & 3], np = 1 + (shape >> 2);
     s->rb_rows = by;
@@ -1352,7 +1355,7 @@ static int tune_rows_t(Solver* s, const OpParams<T>& op, int* best_rows) {
       launch_rb<T>(s, s->stream, op, xa, (const T*)xb, 1, T(1), nullptr);
     }
     cudaEventRecord(e0, s->stream);
-    for (int r = 0; r < 5; ++r) {
+    for (int r = 0; r < 10; ++r) {
       launch_rb<T>(s, s->stream, op, xa, (const T*)xb, 0, T(1), nullptr);
       launch_rb<T>(s, s->stream, op, xa, (const T*)xb, 1, T(1), nullptr);
     }
@@ -1364,7 +1367,7 @@ static int tune_rows_t(Solver* s, const OpParams<T>& op, int* best_rows) {
       break;
     }
     tbest[shape] = std::min(tbest[shape], ms);
-    if (round == 1 && tbest[shape] < best) {
+    if (round == kRounds - 1 && tbest[shape] < best) {
       best = tbest[shape];
       *best_rows = by | (np << 5);
     }
