@@ -132,3 +132,17 @@ def test_nonfinite_and_unsupported_fields(oracle):
         s.set_fields(prob.wk["lam"], mask)
     assert e.value.status == 7  # H2G_UNSUPPORTED
     s.close()
+
+
+@pytest.mark.parametrize("case", CASES, ids=["mode3", "adiabatic", "odd", "transient"])
+def test_calcax_symmetric(oracle, case):
+    """(A x, y) = (x, A y) to rounding on the GPU operator (test_symmetry.jl:11-81 restated): the
+    adjoint solves rely on it.  Vectors with zero guards, as every Krylov vector."""
+    prob = mode3_model(oracle, **case)
+    s = make_solver(prob)
+    x = random_interior(prob.shape, 21)
+    y = random_interior(prob.shape, 22)
+    ax, ay = s.calc_ax(x), s.calc_ax(y)
+    l, r = float(np.sum(ax * y)), float(np.sum(x * ay))
+    assert abs(l - r) <= 1e-12 * max(abs(l), abs(r))
+    s.close()
