@@ -233,7 +233,7 @@ def run_reference(a, dist: Dist):
         "impl": "reference", "metric": METRIC, "value": value, "unit": "s", "n_gpus": a.gpus, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": 1e3 * float(np.mean(times)), "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (reference Mode-3 model)",
-        "config": {"workload": workload_name(a).replace("FP32 RB-GS preconditioner inside FP64 PBiCGSTAB", "FP64"),
+        "config": {"workload": workload_name(a),
                    "grid": [a.nx, a.nx, a.nz], "tol": a.tol, "parallelism": "host threads"},
         "cpu_baseline": {"value": value, "unit": "s", "cores": cb.cores, "kind": "port",
                          "sample": f"{per_step} PBiCGSTAB iterations per step (OpenMP reductions, "
