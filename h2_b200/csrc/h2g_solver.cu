@@ -70,6 +70,11 @@ struct SolveGraph {
   }
 };
 
+#ifndef H2G_UNROLL
+#define H2G_UNROLL 4
+#endif
+constexpr int kUnroll = H2G_UNROLL;  // Krylov iterations per captured loop-body pass
+
 enum GraphKind {
   kGPbicg64 = 0, kGCg64 = 1, kGPbicg32 = 2, kGCg32 = 3, kGPbicgMx = 4, kGCgMx = 5, kGSor = 6, kGNum = 7
 };
@@ -601,8 +606,14 @@ static int get_graph(Solver* s, int kind, int smoother, const OpParams<T>& op, c
   }
   const bool cg = (kind == kGCg64 || kind == kGCg32 || kind == kGCgMx);
   int rc = make_loop_graph(s, G, [&](cudaStream_t cs, cudaGraphConditionalHandle hc, int use_cond) {
-    if (cg) launch_cg_body<T, TX, TP>(s, cs, op, opM, x, st, smoother, hc, use_cond);
-    else launch_pbicg_body<T, TX, TP>(s, cs, op, opM, x, st, smoother, hc, use_cond);
+    // kUnroll iterations per WHILE-body pass: the device re-evaluates the loop condition
+    // kUnroll times less often.  Every kernel returns at once when the state says stop, and the
+    // last update kernel of the body sets the condition, so an iteration that converges in the
+    // middle of a pass only leaves the rest of the pass as empty launches.
+    for (int u = 0; u < kUnroll; ++u) {
+      if (cg) launch_cg_body<T, TX, TP>(s, cs, op, opM, x, st, smoother, hc, use_cond);
+      else launch_pbicg_body<T, TX, TP>(s, cs, op, opM, x, st, smoother, hc, use_cond);
+    }
   });
   if (rc) return rc;
   G.sig = sig;
@@ -620,7 +631,7 @@ static int run_graph(Solver* s, SolveGraph* G, SolverState* st, int maxItr) {
   const int batch = 8;
   while (done < maxItr + 1) {
     for (int i = 0; i < batch; ++i) CK(cudaGraphLaunch(G->exec, s->stream));
-    done += batch;
+    done += batch * kUnroll;
     CK(cudaMemcpyAsync(s->st_host, st, sizeof(SolverState), cudaMemcpyDeviceToHost, s->stream));
     CK(cudaStreamSynchronize(s->stream));
     if (s->st_host->stop) break;
