@@ -55,7 +55,7 @@ static int fail(int code, const char* fmt, ...) {
                                        __LINE__);                                                         \
   } while (0)
 
-// Graph of one solve: parent graph {WHILE node}, body = one iteration.
+// Graph of one solve: parent graph {WHILE node}, body = kUnroll iterations (SOR: one pass).
 struct SolveGraph {
   cudaGraphExec_t exec = nullptr;
   cudaGraph_t graph = nullptr;
@@ -541,9 +541,9 @@ static std::vector<unsigned char> signature(const OpParams<T>& opA, const OpPara
   return v;
 }
 
-// Instantiate the loop of a solve: a conditional WHILE node whose body is one iteration
-// (body(stream, handle, 1) captured into it), or, where conditional nodes are unavailable, a graph
-// of one iteration (body(stream, 0, 0)) that run_graph relaunches from the host.
+// Instantiate the loop of a solve: a conditional WHILE node whose body is what body(stream,
+// handle, 1) captures, or, where conditional nodes are unavailable, a graph of the same body
+// (body(stream, 0, 0)) that run_graph relaunches from the host.
 template <typename Body>
 static int make_loop_graph(Solver* s, SolveGraph& G, Body body) {
   G.reset();
@@ -621,7 +621,8 @@ static int get_graph(Solver* s, int kind, int smoother, const OpParams<T>& op, c
   return H2G_OK;
 }
 
-static int run_graph(Solver* s, SolveGraph* G, SolverState* st, int maxItr) {
+// per: iterations (SOR passes) in one launch of the body graph
+static int run_graph(Solver* s, SolveGraph* G, SolverState* st, int maxItr, int per) {
   if (G->cond) {
     CK(cudaGraphLaunch(G->exec, s->stream));
     return H2G_OK;
@@ -631,7 +632,7 @@ static int run_graph(Solver* s, SolveGraph* G, SolverState* st, int maxItr) {
   const int batch = 8;
   while (done < maxItr + 1) {
     for (int i = 0; i < batch; ++i) CK(cudaGraphLaunch(G->exec, s->stream));
-    done += batch * kUnroll;
+    done += batch * per;
     CK(cudaMemcpyAsync(s->st_host, st, sizeof(SolverState), cudaMemcpyDeviceToHost, s->stream));
     CK(cudaStreamSynchronize(s->stream));
     if (s->st_host->stop) break;
@@ -736,7 +737,7 @@ static int solve_krylov(Solver* s, bool cg, double tol, int maxItr, int smoother
   if ((rc = get_graph<double, double, TP>(s, kind, smoother, op, opM, s->th, st, &G))) return rc;
   // a state that stopped at the start turns every kernel of the body into a no-op and the
   // last one ends the WHILE loop after one pass
-  if ((rc = run_graph(s, G, st, maxItr))) return rc;
+  if ((rc = run_graph(s, G, st, maxItr, kUnroll))) return rc;
   CK(cudaMemcpyAsync(s->st_host, st, sizeof(SolverState), cudaMemcpyDeviceToHost, s->stream));
   CK(cudaStreamSynchronize(s->stream));
   SolverState fin = *s->st_host;
@@ -816,7 +817,7 @@ static int solve_ir(Solver* s, bool cg, double tol, int maxItr, int smoother, in
       }
       if ((rc = get_graph<float, float, float>(s, cg ? kGCg32 : kGPbicg32, smoother, op32, op32, e, si, &G)))
         return rc;
-      if ((rc = run_graph(s, G, si, cap))) return rc;
+      if ((rc = run_graph(s, G, si, cap, kUnroll))) return rc;
       // theta += ||r64|| e ; r64 = b - A theta
       launch(s, k_ir_apply, nb, 256, s->stream, g.n, s->th, e, st);
       launch(s, k_rk<double>, ag, blk, s->stream, op64, s->r64, nullptr, s->th, s->b, st, s->partials, kStageResid);
@@ -1016,7 +1017,7 @@ static int solve_sor(Solver* s, double omega, double tol, int maxItr, int verbos
     if (rc) return rc;
     G.sig = sig;
   }
-  if ((rc = run_graph(s, &G, st, maxItr))) return rc;
+  if ((rc = run_graph(s, &G, st, maxItr, 1))) return rc;
   CK(cudaMemcpyAsync(s->st_host, st, sizeof(SolverState), cudaMemcpyDeviceToHost, s->stream));
   CK(cudaStreamSynchronize(s->stream));
   SolverState fin = *s->st_host;
