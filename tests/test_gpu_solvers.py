@@ -253,3 +253,22 @@ def test_mixed_converges_on_fine_grid():
         sols[prec] = s.get_theta()
         s.close()
     assert np.abs(sols["mixed"] - sols["fp64"]).max() <= THETA_TOL_K
+
+
+@pytest.mark.parametrize("method", ["pbicgstab", "cg", "sor"])
+def test_host_loop_fallback_matches_graph_loop(oracle, method, monkeypatch):
+    """H2G_NO_COND=1 relaunches the captured loop body from the host instead of a device-side
+    WHILE node: the same kernels in the same order, so the same bits and iteration count."""
+    prob = mode3_model(oracle, 40, symmetric=(method == "cg"))
+    out = []
+    for nc in ("0", "1"):
+        monkeypatch.setenv("H2G_NO_COND", nc)
+        s = make_solver(prob)
+        if method == "sor":
+            st, res = s.sor(omega=1.8, tol=1e-4, maxItr=3000)
+        else:
+            st, res = s.solve(method, tol=1e-8, maxItr=20000, smoother="gs")
+        out.append((st, res.itr, res.res, s.get_theta()))
+        s.close()
+    assert out[0][:3] == out[1][:3]
+    assert np.array_equal(out[0][3], out[1][3])
