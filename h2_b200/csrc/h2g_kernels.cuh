@@ -419,7 +419,7 @@ __device__ __forceinline__ void x_nbrs(T oc, int okc, int e, int lane, int p, in
 // returns the sum of the squared SOR residuals r = (dd + omega*(c_xm + c_ym + c_zm))*dp/omega of
 // the updated cells (rbsor_core!, NonUniform.jl:907-908); the preconditioner discards them and
 // skips the work.  With NP = 2 the two cells share the o-colour column loads.
-template <typename T, bool RES, int NP = 2>
+template <typename T, bool RES, int NP = 2, bool DD = true>
 __device__ __forceinline__ double rb_pass_column(const OpParams<T>& op, T* x, const T* __restrict__ bb, int color,
                                                  T omega, int lane, int p, int j, int k0) {
   const Geo& g = op.g;
@@ -485,10 +485,10 @@ __device__ __forceinline__ double rb_pass_column(const OpParams<T>& op, T* x, co
     bool has;
     if (NK) {
       const unsigned long long w = nk[u];  // own, x-, x+, y-, y+, z-, z+ keys in bytes 0..6
-      has = cell_coef<T, true>(op, k0 + u, (uint8_t)w, (uint8_t)(w >> 8), (uint8_t)(w >> 16), (uint8_t)(w >> 24),
+      has = cell_coef<T, DD>(op, k0 + u, (uint8_t)w, (uint8_t)(w >> 8), (uint8_t)(w >> 16), (uint8_t)(w >> 24),
                                (uint8_t)(w >> 32), (uint8_t)(w >> 40), (uint8_t)(w >> 48), ac, c);
     } else {
-      has = cell_coef<T, true>(op, k0 + u, (uint8_t)kc[u], (uint8_t)kxm[u], (uint8_t)kxp[u], (uint8_t)kym[u],
+      has = cell_coef<T, DD>(op, k0 + u, (uint8_t)kc[u], (uint8_t)kxm[u], (uint8_t)kxp[u], (uint8_t)kym[u],
                                (uint8_t)kyp[u], (uint8_t)kcol[u], (uint8_t)kcol[u + 2], ac, c);
     }
     if (!has) continue;
@@ -508,7 +508,10 @@ __device__ __forceinline__ double rb_pass_column(const OpParams<T>& op, T* x, co
 // shape keeps the register cap of H2G_MINB blocks of 256 threads per SM.
 constexpr int kRbRows[4] = {2, 4, 8, 16};
 
-template <typename T, int BY = kBY, int NP = 2>
+// DD: dd read from the per-cell array (fewer instructions; faster while the vectors stay in L2)
+// or summed per cell (8 bytes fewer per cell; faster on grids that stream from HBM).  The tuner
+// picks it with the shape.
+template <typename T, int BY = kBY, int NP = 2, bool DD = true>
 __global__ void __launch_bounds__(kBX * BY, (H2G_MINB * kBY) / BY)
     k_rb_pass(OpParams<T> op, T* x, const T* __restrict__ bb, int color, T omega,
               const SolverState* __restrict__ st) {
@@ -518,7 +521,7 @@ __global__ void __launch_bounds__(kBX * BY, (H2G_MINB * kBY) / BY)
   const int j = 1 + blockIdx.y * BY + threadIdx.y;
   const int k0 = 1 + NP * blockIdx.z;
   if (j > op.g.NY) return;  // uniform per warp
-  rb_pass_column<T, false, NP>(op, x, bb, color, omega, lane, p, j, k0);
+  rb_pass_column<T, false, NP, DD>(op, x, bb, color, omega, lane, p, j, k0);
 }
 
 // rbsor_core! with its residual (NonUniform.jl:848-915) for solveSOR! (NonUniform.jl:1004-1051):

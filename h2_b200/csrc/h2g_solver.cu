@@ -151,6 +151,7 @@ struct Solver {
   bool pdl = true;  // programmatic dependent launch of the solver kernels
   int rb_rows = kBY;      // rows per block of the colour pass (autotuned)
   int rb_planes = 2;      // planes per thread of the colour pass (autotuned)
+  bool rb_dd = true;      // colour pass reads dd from the per-cell array (autotuned)
   bool ax_dd = false;     // CalcAX reads dd from the per-cell array (autotuned)
   bool rb_tuned = false;  // rb_rows chosen (by the tuner or h2g_set_tuning)
 
@@ -206,29 +207,38 @@ static void launch_ax(const Solver* s, cudaStream_t cs, const OpParams<T>& op, T
 }
 
 // One colour pass with the handle's launch shape (rows per block, planes per thread).
-template <typename T, int NP>
+template <typename T, int NP, bool DD>
 static void launch_rb_np(const Solver* s, cudaStream_t cs, const OpParams<T>& op, T* x, const T* bb, int color,
                          T omega, const SolverState* st) {
   const Geo& g = op.g;
   const int gz = (g.NZ + NP - 1) / NP;
   const int gx = (g.HN + kBX - 1) / kBX;
   switch (s->rb_rows) {
-    case 2: launch(s, k_rb_pass<T, 2, NP>, dim3(gx, (g.NY + 1) / 2, gz), dim3(kBX, 2), cs, op, x, bb, color, omega, st);
+    case 2:
+      launch(s, k_rb_pass<T, 2, NP, DD>, dim3(gx, (g.NY + 1) / 2, gz), dim3(kBX, 2), cs, op, x, bb, color, omega, st);
       break;
-    case 4: launch(s, k_rb_pass<T, 4, NP>, dim3(gx, (g.NY + 3) / 4, gz), dim3(kBX, 4), cs, op, x, bb, color, omega, st);
+    case 4:
+      launch(s, k_rb_pass<T, 4, NP, DD>, dim3(gx, (g.NY + 3) / 4, gz), dim3(kBX, 4), cs, op, x, bb, color, omega, st);
       break;
     case 16:
-      launch(s, k_rb_pass<T, 16, NP>, dim3(gx, (g.NY + 15) / 16, gz), dim3(kBX, 16), cs, op, x, bb, color, omega, st);
+      launch(s, k_rb_pass<T, 16, NP, DD>, dim3(gx, (g.NY + 15) / 16, gz), dim3(kBX, 16), cs, op, x, bb, color, omega,
+             st);
       break;
-    default: launch(s, k_rb_pass<T, 8, NP>, dim3(gx, (g.NY + 7) / 8, gz), dim3(kBX, 8), cs, op, x, bb, color, omega, st);
+    default:
+      launch(s, k_rb_pass<T, 8, NP, DD>, dim3(gx, (g.NY + 7) / 8, gz), dim3(kBX, 8), cs, op, x, bb, color, omega, st);
       break;
   }
 }
 template <typename T>
 static void launch_rb(const Solver* s, cudaStream_t cs, const OpParams<T>& op, T* x, const T* bb, int color, T omega,
                       const SolverState* st) {
-  if (s->rb_planes == 1) launch_rb_np<T, 1>(s, cs, op, x, bb, color, omega, st);
-  else launch_rb_np<T, 2>(s, cs, op, x, bb, color, omega, st);
+  if (s->rb_dd) {
+    if (s->rb_planes == 1) launch_rb_np<T, 1, true>(s, cs, op, x, bb, color, omega, st);
+    else launch_rb_np<T, 2, true>(s, cs, op, x, bb, color, omega, st);
+  } else {
+    if (s->rb_planes == 1) launch_rb_np<T, 1, false>(s, cs, op, x, bb, color, omega, st);
+    else launch_rb_np<T, 2, false>(s, cs, op, x, bb, color, omega, st);
+  }
 }
 
 static size_t partials_needed(const Solver* s) {
@@ -1315,11 +1325,11 @@ static int adjoint_transient(Solver* s, const FaceBC& f, int nt, const double* w
 
 // ---- launch-shape tuner --------------------------------------------------------------------
 // The colour pass has no reduction, so its launch shape changes no result: the first solve of a
-// handle times every shape (kRbRows x 1 or 2 planes per thread) on the handle's grid (three
-// interleaved rounds of two warm-up and ten timed sweeps each, on scratch vectors) and keeps the
-// fastest.  CalcAX is timed with dd summed and read from the array.  Choices are cached per
-// (grid, smoother precision) for the process; H2G_RB_ROWS, H2G_RB_PLANES and H2G_AX_DD in the
-// environment force them.
+// handle times every variant (kRbRows x 1 or 2 planes per thread x dd read or summed) on the
+// handle's grid (three interleaved rounds of two warm-up and ten timed sweeps each, on scratch
+// vectors) and keeps the fastest.  CalcAX is timed with dd summed and read from the array.
+// Choices are cached per (grid, smoother precision) for the process; H2G_RB_ROWS,
+// H2G_RB_PLANES, H2G_RB_DD and H2G_AX_DD in the environment force them.
 static std::mutex g_tune_mu;
 static std::map<std::array<int, 4>, int> g_tune_cache;
 
@@ -1346,6 +1356,7 @@ static int tune_rows_t(Solver* s, const OpParams<T>& op, int* best_rows) {
     return fail(H2G_CUDA_ERROR, "event creation failed");
   }
   const int saved = s->rb_rows, saved_np = s->rb_planes;
+  const bool saved_dd = s->rb_dd;
   float best = 1e30f;
   int rc = H2G_OK;
   // warm the GPU up first (clocks ramp), then time every shape twice, interleaved, keeping the
@@ -1354,14 +1365,15 @@ static int tune_rows_t(Solver* s, const OpParams<T>& op, int* best_rows) {
     launch_rb<T>(s, s->stream, op, xa, (const T*)xb, 0, T(1), nullptr);
     launch_rb<T>(s, s->stream, op, xa, (const T*)xb, 1, T(1), nullptr);
   }
-  float tbest[8];
-  for (int q = 0; q < 8; ++q) tbest[q] = 1e30f;
+  float tbest[16];
+  for (int q = 0; q < 16; ++q) tbest[q] = 1e30f;
   constexpr int kRounds = 3;
   for (int round = 0; round < kRounds && rc == H2G_OK; ++round)
-  for (int shape = 0; shape < 8; ++shape) {
-    const int by = kRbRows[shape & 3], np = 1 + (shape >> 2);
+  for (int shape = 0; shape < 16; ++shape) {
+    const int by = kRbRows[shape & 3], np = 1 + ((shape >> 2) & 1), dd = shape >> 3;
     s->rb_rows = by;
     s->rb_planes = np;
+    s->rb_dd = dd != 0;
     for (int r = 0; r < 2; ++r) {
       launch_rb<T>(s, s->stream, op, xa, (const T*)xb, 0, T(1), nullptr);
       launch_rb<T>(s, s->stream, op, xa, (const T*)xb, 1, T(1), nullptr);
@@ -1381,11 +1393,12 @@ static int tune_rows_t(Solver* s, const OpParams<T>& op, int* best_rows) {
     tbest[shape] = std::min(tbest[shape], ms);
     if (round == kRounds - 1 && tbest[shape] < best) {
       best = tbest[shape];
-      *best_rows = by | (np << 5);
+      *best_rows = by | (np << 5) | (dd << 7);
     }
   }
   s->rb_rows = saved;
   s->rb_planes = saved_np;
+  s->rb_dd = saved_dd;
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   return rc;
@@ -1451,15 +1464,19 @@ static int autotune(Solver* s) {
     }
   }
   int planes = (cached >> 5) & 3;
+  int rbdd = (cached >> 7) & 1;
+  if (const char* e = getenv("H2G_RB_DD")) rbdd = atoi(e) ? 1 : 0;
   if (const char* e = getenv("H2G_RB_PLANES")) {
     const int np = atoi(e);
     if (np == 1 || np == 2) planes = np;
   }
   if (!valid_rows(rows)) rows = cached & 0x1f;
   if (dd < 0) dd = cached >> 8;
-  if (rows != s->rb_rows || planes != s->rb_planes || (dd != 0) != s->ax_dd) invalidate_graphs(s);
+  if (rows != s->rb_rows || planes != s->rb_planes || (rbdd != 0) != s->rb_dd || (dd != 0) != s->ax_dd)
+    invalidate_graphs(s);
   s->rb_rows = rows;
   s->rb_planes = planes;
+  s->rb_dd = rbdd != 0;
   s->ax_dd = dd != 0;
   s->rb_tuned = true;
   return H2G_OK;

@@ -49,13 +49,15 @@ def test_tuner_choice_is_cached(oracle):
     s2.close()
 
 
-def test_calcax_dd_source_gives_identical_results(oracle, monkeypatch):
+def test_dd_source_gives_identical_results(oracle, monkeypatch):
+    """dd summed per cell or read from the per-cell array, in CalcAX and in the colour pass."""
     prob = mode3_model(oracle, 40)
     x = np.zeros(prob.shape, order="F")
     x[1:-1, 1:-1, 1:-1] = np.random.default_rng(1).standard_normal((prob.NX, prob.NY, prob.NZ))
     outs = []
     for dd in ("0", "1"):
         monkeypatch.setenv("H2G_AX_DD", dd)
+        monkeypatch.setenv("H2G_RB_DD", dd)
         s = make_solver(prob)
         st, res = s.solve("pbicgstab", tol=1e-8, maxItr=20000, smoother="gs")
         assert st == 0
@@ -63,4 +65,4 @@ def test_calcax_dd_source_gives_identical_results(oracle, monkeypatch):
         s.close()
     assert outs[0][:2] == outs[1][:2]
     assert np.array_equal(outs[0][2], outs[1][2]) and np.array_equal(outs[0][3], outs[1][3])
-    assert os.environ.get("H2G_AX_DD") == "1"
+    assert os.environ.get("H2G_AX_DD") == "1" and os.environ.get("H2G_RB_DD") == "1"
