@@ -1329,7 +1329,7 @@ static int adjoint_transient(Solver* s, const FaceBC& f, int nt, const double* w
 // handle's grid (three interleaved rounds of two warm-up and ten timed sweeps each, on scratch
 // vectors) and keeps the fastest.  CalcAX is timed with dd summed and read from the array.
 // Choices are cached per (grid, smoother precision) for the process; H2G_RB_ROWS,
-// H2G_RB_PLANES, H2G_RB_DD and H2G_AX_DD in the environment force them.
+// H2G_RB_PLANES, H2G_RB_DD and H2G_AX_DD in the environment force them (all four: no timing).
 static std::mutex g_tune_mu;
 static std::map<std::array<int, 4>, int> g_tune_cache;
 
@@ -1442,36 +1442,36 @@ static int tune_ax(Solver* s, int* use_dd) {
 
 static int autotune(Solver* s) {
   if (s->rb_tuned) return H2G_OK;
-  int rows = 0, dd = -1;
-  if (const char* e = getenv("H2G_RB_ROWS")) rows = atoi(e);
-  if (const char* e = getenv("H2G_AX_DD")) dd = atoi(e) ? 1 : 0;
-  const std::array<int, 4> key = {s->g.MX, s->g.MY, s->g.MZ, s->precision == H2G_FP64 ? 64 : 32};
-  int cached = 0;
-  {
-    // held while tuning, so that handles of one grid solved concurrently (h2g_batch_solve) tune
-    // once and no two tunings disturb each other's timings
-    std::lock_guard<std::mutex> lk(g_tune_mu);
-    auto it = g_tune_cache.find(key);
-    if (it != g_tune_cache.end()) cached = it->second;
-    if (!cached) {
-      int r2 = 0, d2 = 0;
-      int rc = s->precision == H2G_FP64 ? tune_rows_t<double>(s, op_params<double>(s, s->t64), &r2)
-                                        : tune_rows_t<float>(s, op_params<float>(s, s->t32), &r2);
-      if (!rc) rc = tune_ax(s, &d2);
-      if (rc) return rc;
-      cached = r2 | (d2 << 8);
-      g_tune_cache[key] = cached;
-    }
-  }
-  int planes = (cached >> 5) & 3;
-  int rbdd = (cached >> 7) & 1;
+  // choices forced by the environment (-1: not forced)
+  int rows = -1, planes = -1, rbdd = -1, dd = -1;
+  if (const char* e = getenv("H2G_RB_ROWS")) rows = valid_rows(atoi(e)) ? atoi(e) : -1;
+  if (const char* e = getenv("H2G_RB_PLANES")) planes = (atoi(e) == 1 || atoi(e) == 2) ? atoi(e) : -1;
   if (const char* e = getenv("H2G_RB_DD")) rbdd = atoi(e) ? 1 : 0;
-  if (const char* e = getenv("H2G_RB_PLANES")) {
-    const int np = atoi(e);
-    if (np == 1 || np == 2) planes = np;
+  if (const char* e = getenv("H2G_AX_DD")) dd = atoi(e) ? 1 : 0;
+  if (rows < 0 || planes < 0 || rbdd < 0 || dd < 0) {
+    const std::array<int, 4> key = {s->g.MX, s->g.MY, s->g.MZ, s->precision == H2G_FP64 ? 64 : 32};
+    int cached = 0;
+    {
+      // held while tuning, so that handles of one grid solved concurrently (h2g_batch_solve) tune
+      // once and no two tunings disturb each other's timings
+      std::lock_guard<std::mutex> lk(g_tune_mu);
+      auto it = g_tune_cache.find(key);
+      if (it != g_tune_cache.end()) cached = it->second;
+      if (!cached) {
+        int r2 = 0, d2 = 0;
+        int rc = s->precision == H2G_FP64 ? tune_rows_t<double>(s, op_params<double>(s, s->t64), &r2)
+                                          : tune_rows_t<float>(s, op_params<float>(s, s->t32), &r2);
+        if (!rc) rc = tune_ax(s, &d2);
+        if (rc) return rc;
+        cached = r2 | (d2 << 8);
+        g_tune_cache[key] = cached;
+      }
+    }
+    if (rows < 0) rows = cached & 0x1f;
+    if (planes < 0) planes = (cached >> 5) & 3;
+    if (rbdd < 0) rbdd = (cached >> 7) & 1;
+    if (dd < 0) dd = (cached >> 8) & 1;
   }
-  if (!valid_rows(rows)) rows = cached & 0x1f;
-  if (dd < 0) dd = cached >> 8;
   if (rows != s->rb_rows || planes != s->rb_planes || (rbdd != 0) != s->rb_dd || (dd != 0) != s->ax_dd)
     invalidate_graphs(s);
   s->rb_rows = rows;
