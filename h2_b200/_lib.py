@@ -82,7 +82,7 @@ _SIGS = {
                               C.POINTER(Result), C.POINTER(Result)]),
     "h2g_adjoint_transient": (C.c_int, [_vp, C.POINTER(Bc), C.c_int, _dp, C.c_double, C.c_double, C.c_int, C.c_int,
                                         C.c_int, _dp, _dp, _dp, C.POINTER(Result)]),
-    "h2g_autotune": (C.c_int, [_vp, _ip, _ip]),
+    "h2g_autotune": (C.c_int, [_vp, _ip, _ip, _ip, _ip]),
     "h2g_set_tuning": (C.c_int, [_vp, C.c_int, C.c_int]),
     "h2g_release_cached": (C.c_int, []),
     "h2g_calcax": (C.c_int, [_vp, _dp, _dp]),

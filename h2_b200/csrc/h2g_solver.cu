@@ -1717,15 +1717,16 @@ template <typename T>
 static int bench_t(Solver* s, int kind, int reps, int* launches, const h2g::OpParams<T>& op) {
   using namespace h2g;
   if (int rc = autotune(s)) return rc;
-  // the hook buffers (zeroed when allocated; values are irrelevant for timing)
+  // the hook buffers, filled with non-zero values: a zero numerator sends the correctly rounded
+  // division of the smoother down a slower special-case path, which solves do not see
   const size_t bytes = sizeof(double) * (size_t)s->g.n;
   for (auto& p : s->hook)
-    if (!p) {
-      CK(cudaMalloc(&p, bytes));
-      CK(cudaMemset(p, 0, bytes));
-    }
+    if (!p) CK(cudaMalloc(&p, bytes));
   T* xa = static_cast<T*>(s->hook[0]);
   T* xb = static_cast<T*>(s->hook[1]);
+  k_fill_const<T><<<elementwise_blocks(s), 256, 0, s->stream>>>((long long)s->g.n, xa, T(300));
+  k_fill_const<T><<<elementwise_blocks(s), 256, 0, s->stream>>>((long long)s->g.n, xb, T(-1.0e-3));
+  CKL();
   const dim3 rg = rb_grid(s->g), ag = ax_grid(s->g), blk(kBX, kBY);
   int n = 0;
   for (int r = 0; r < reps; ++r) {
@@ -2013,7 +2014,7 @@ int h2g_adjoint_transient(h2g_solver* h, const h2g_bc* bc, int nt, const double*
                                 dJ_dlnlam, out);
 }
 
-int h2g_autotune(h2g_solver* h, int* rows, int* planes) {
+int h2g_autotune(h2g_solver* h, int* rows, int* planes, int* rb_dd, int* ax_dd) {
   if (int rc = h2g::check_handle(h)) return rc;
   Solver* s = S(h);
   if (!s->grid_set || !s->fields_set) return fail(H2G_BAD_ARG, "h2g_set_grid and h2g_set_fields must come first");
@@ -2021,6 +2022,8 @@ int h2g_autotune(h2g_solver* h, int* rows, int* planes) {
   if (int rc = h2g::autotune(s)) return rc;
   if (rows) *rows = s->rb_rows;
   if (planes) *planes = s->rb_planes;
+  if (rb_dd) *rb_dd = s->rb_dd ? 1 : 0;
+  if (ax_dd) *ax_dd = s->ax_dd ? 1 : 0;
   return H2G_OK;
 }
 

@@ -75,7 +75,9 @@ def main(argv=None):
             launches += n
     N = a.nx * a.nx * a.nz
     w_elem = 8 if (a.precision == "fp64" or (a.kind == "calcax" and a.precision == "mixed")) else 4
+    rows, planes, rb_dd, ax_dd = s.tuning()
     out = {"kind": a.kind, "precision": a.precision, "grid": [a.nx, a.nx, a.nz], "reps": a.reps,
+           "tuning": {"rows": rows, "planes": planes, "rb_dd": rb_dd, "ax_dd": ax_dd},
            "us_per_rep": float(np.mean(times)), "us_min": float(np.min(times)),
            "launches_per_rep": launches / a.reps, "model_build_s": t_model}
     if a.kind != "solve":

@@ -217,9 +217,14 @@ class Solver:
     def autotune(self) -> tuple:
         """Run the launch-shape tuner now; returns the colour pass's (rows per block, planes per
         thread)."""
-        r, p = C.c_int(0), C.c_int(0)
-        L.check(self.lib.h2g_autotune(self.h, C.byref(r), C.byref(p)))
-        return r.value, p.value
+        return self.tuning()[:2]
+
+    def tuning(self) -> tuple:
+        """The tuner's choices (running it if needed): (rows, planes, colour pass reads dd,
+        CalcAX reads dd)."""
+        r, p, a, b = C.c_int(0), C.c_int(0), C.c_int(0), C.c_int(0)
+        L.check(self.lib.h2g_autotune(self.h, C.byref(r), C.byref(p), C.byref(a), C.byref(b)))
+        return r.value, p.value, bool(a.value), bool(b.value)
 
     def set_tuning(self, rows: int, planes: int = 2):
         """Force the colour pass's shape (rows 2, 4, 8, 16; planes 1, 2); rows = 0 tunes again."""

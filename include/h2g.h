@@ -209,15 +209,17 @@ int h2g_transient(h2g_solver *h, const h2g_bc *bc, int nt, int method, double to
                   int verbose, double *step_stats, h2g_result *out);
 
 /* ---- launch-shape tuning (no reference counterpart) ---------------------------------------
- * The smoother's colour pass has no reduction, so its launch shape changes no result.  The first
- * solve of a handle times blocks of 2, 4, 8 and 16 rows with 1 or 2 planes per thread and dd
- * read from the per-cell array or summed per cell (a few sweeps each on scratch vectors) and
- * keeps the fastest; it also times the FP64 CalcAX with either dd source (the same bits either
- * way).  The choices are cached per grid size and smoother precision for the process;
- * H2G_RB_ROWS, H2G_RB_PLANES, H2G_RB_DD and H2G_AX_DD (0/1) in the environment force them.  h2g_autotune runs the tuner
- * now (*rows, *planes: the colour pass's shape, nullable); h2g_set_tuning forces a shape (rows 2,
- * 4, 8 or 16 and planes 1 or 2; rows = 0: tune again on the next solve). */
-int h2g_autotune(h2g_solver *h, int *rows, int *planes);
+ * The smoother's colour pass has no reduction, so its launch variant changes no result.  The
+ * first solve of a handle times blocks of 2, 4, 8 and 16 rows with 1 or 2 planes per thread and
+ * dd read from the per-cell array or summed per cell (a few sweeps each on scratch vectors) and
+ * keeps the fastest; it also times the FP64 CalcAX with either dd source (the same bits in every
+ * case).  The choices are cached per grid size and smoother precision for the process;
+ * H2G_RB_ROWS, H2G_RB_PLANES, H2G_RB_DD and H2G_AX_DD (0/1) in the environment force them (all
+ * four: no timing at all).  h2g_autotune runs the tuner now and reports its choices (each
+ * pointer nullable): the colour pass's rows and planes, whether it reads dd (*rb_dd) and whether
+ * CalcAX does (*ax_dd).  h2g_set_tuning forces a shape (rows 2, 4, 8 or 16 and planes 1 or 2;
+ * rows = 0: tune again on the next solve). */
+int h2g_autotune(h2g_solver *h, int *rows, int *planes, int *rb_dd, int *ax_dd);
 int h2g_set_tuning(h2g_solver *h, int rows, int planes);
 
 /* ---- kernels of the path, callable one at a time (host arrays in and out) ---------------

@@ -53,7 +53,7 @@ def test_bad_arguments_rejected_on_host(lib):
     assert lib.h2g_adjoint(None, None, 8.0, 1e-6, 10, 1, C.byref(J), None, None, None, None) == L.H2G_BAD_ARG
     assert lib.h2g_adjoint_transient(None, bcs, 3, None, 8.0, 1e-6, 10, 1, 2, C.byref(J), None, None,
                                      None) == L.H2G_BAD_ARG
-    assert lib.h2g_autotune(None, None, None) == L.H2G_BAD_ARG
+    assert lib.h2g_autotune(None, None, None, None, None) == L.H2G_BAD_ARG
     assert lib.h2g_set_tuning(None, 4, 2) == L.H2G_BAD_ARG
     hs = (C.c_void_p * 1)()
     assert lib.h2g_batch_solve(0, hs, 0, 1e-6, 10, 1, 1, (L.Result * 1)()) == L.H2G_BAD_ARG
