@@ -177,7 +177,7 @@ class BatchSolver:
         for s in self.solvers:
             s.snapshot(restore=True)
 
-    def solve(self, method="pbicgstab", tol=1e-8, maxItr=20_000, smoother="gs", threads=16):
+    def solve(self, method="pbicgstab", tol=1e-8, maxItr=20_000, smoother="gs", threads=2):
         """All members at once; returns (status, list of Result)."""
         from .nonuniform import smoother_selector
         L, C = self.L, self.C

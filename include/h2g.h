@@ -155,7 +155,7 @@ int h2g_release_cached(void);
  * Solve n independent systems at once (many power maps and grids of uneven size): every handle
  * keeps its own grid, fields, θ and b (set beforehand), gets its own non-blocking stream for the
  * batch, and its whole solve (a CUDA graph looping on the device) is issued from one of
- * `threads` host threads (<= 0: 16), so the solves run concurrently on the GPU.  method 0
+ * `threads` host threads (<= 0: 2), so the solves run concurrently on the GPU.  method 0
  * PBiCGSTAB, 1 CG, 2 RB-SOR with omega = 1.  outs[q] receives handle q's result (the same values
  * as a lone h2g_pbicgstab/h2g_cg on that handle: kernels are deterministic).  Returns H2G_OK
  * when every member converged, else the first non-OK member status (H2G_BAD_ARG /
