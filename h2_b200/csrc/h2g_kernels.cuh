@@ -190,7 +190,10 @@ __device__ void finish_stage(int stage, SolverState* st, double s1, double s2) {
   }
 }
 
-template <int NV>
+// COND: the kernel may set the loop condition of a device-side WHILE node.  Kernels compiled
+// without it contain no device graph call (the host-loop path launches those; profilers can
+// then see them too).
+template <int NV, bool COND = false>
 __device__ __forceinline__ void reduce_finish(double (&v)[NV], double* __restrict__ partials, SolverState* st,
                                               int stage, cudaGraphConditionalHandle hc, int use_cond) {
   __shared__ double sm[32][NV];
@@ -232,7 +235,7 @@ __device__ __forceinline__ void reduce_finish(double (&v)[NV], double* __restric
     st->ticket = 0;
     finish_stage(stage, st, acc[0], NV > 1 ? acc[NV > 1 ? 1 : 0] : 0.0);
     // the loop continues only while the solve runs and the pass count is within maxItr + 1
-    set_cond(hc, use_cond, !st->stop && st->passes <= st->maxItr + 1);
+    if constexpr (COND) set_cond(hc, use_cond, !st->stop && st->passes <= st->maxItr + 1);
   }
 }
 
@@ -528,6 +531,7 @@ __global__ void __launch_bounds__(kBX * BY, (H2G_MINB * kBY) / BY)
 // colour `color` updated with relaxation omega, sum of r^2 -> stage (kStageSorHalf after colour
 // 0, kStageSorIter after colour 1).  The colour-1 launch ends a WHILE-body pass: block 0 counts
 // the pass and ends the loop provisionally; only the finisher can continue it.
+template <bool COND>
 __global__ void __launch_bounds__(kThreads) k_sor_pass(OpParams<double> op, double* x,
                                                        const double* __restrict__ bb, int color, double omega,
                                                        SolverState* st, double* __restrict__ partials, int stage,
@@ -535,7 +539,7 @@ __global__ void __launch_bounds__(kThreads) k_sor_pass(OpParams<double> op, doub
   pdl_enter();
   if (color == 1 && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.x == 0 && threadIdx.y == 0) {
     st->passes += 1;
-    set_cond(hc, use_cond, 0);
+    if constexpr (COND) set_cond(hc, use_cond, 0);
   }
   if (st->stop) return;
   const int lane = threadIdx.x, p = blockIdx.x * kBX + lane;
@@ -543,7 +547,7 @@ __global__ void __launch_bounds__(kThreads) k_sor_pass(OpParams<double> op, doub
   const int k0 = 1 + 2 * blockIdx.z;
   double v[1] = {0.0};
   if (j <= op.g.NY) v[0] = rb_pass_column<double, true>(op, x, bb, color, omega, lane, p, j, k0);
-  reduce_finish<1>(v, partials, st, stage, hc, color == 1 ? use_cond : 0);
+  reduce_finish<1, COND>(v, partials, st, stage, hc, color == 1 ? use_cond : 0);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -947,7 +951,7 @@ __device__ __forceinline__ void st16(T* p, const T (&a)[Vec16<T>::n]) {
 
 // BICG2! + Triad! + Fdot1/Fdot2 (NonUniform.jl:328-331 and the next 289):
 //   x += alpha*ph + omega*sh;  r = (-omega)*t + s;  d1 = (r,r), d2 = (r,r0) -> kStageUpdate
-template <typename T, typename TX, typename TP = T>
+template <typename T, typename TX, typename TP = T, bool COND = true>
 __global__ void __launch_bounds__(256) k_bicg_update(long long n, TX* __restrict__ x, const TP* __restrict__ ph,
                                                       const TP* __restrict__ sh, T* __restrict__ r,
                                                       const T* __restrict__ s, const T* __restrict__ t,
@@ -959,7 +963,7 @@ __global__ void __launch_bounds__(256) k_bicg_update(long long n, TX* __restrict
   // finisher of this kernel (which runs after block 0 has arrived) can continue it.
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     st->passes += 1;
-    set_cond(hc, use_cond, 0);
+    if constexpr (COND) set_cond(hc, use_cond, 0);
   }
   if (st->stop) return;
   constexpr int V = Vec16<T>::n;
@@ -983,7 +987,7 @@ __global__ void __launch_bounds__(256) k_bicg_update(long long n, TX* __restrict
     }
     st16(r + o, a_r);
   }
-  reduce_finish<2>(v, partials, st, kStageUpdate, hc, use_cond);
+  reduce_finish<2, COND>(v, partials, st, kStageUpdate, hc, use_cond);
 }
 
 // CG! fused update (NonUniform.jl:179-182) + Fdot1 (185): x += alpha*p; r -= alpha*q; (r,r)
@@ -1037,14 +1041,14 @@ __global__ void __launch_bounds__(256) k_dot(long long n, const T* __restrict__ 
 }
 
 // CG! p = z + beta*p (NonUniform.jl:218-220); sets the loop condition.
-template <typename T, typename TP = T>
+template <typename T, typename TP = T, bool COND = true>
 __global__ void __launch_bounds__(256) k_cg_pupd(long long n, T* __restrict__ p, const TP* __restrict__ z,
                                                   SolverState* st, cudaGraphConditionalHandle hc, int use_cond) {
   pdl_enter();
   const int stop = st->stop;
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     st->passes += 1;
-    set_cond(hc, use_cond, !stop && st->passes <= st->maxItr + 1);
+    if constexpr (COND) set_cond(hc, use_cond, !stop && st->passes <= st->maxItr + 1);
   }
   if (stop) return;
   constexpr int V = Vec16<T>::n;

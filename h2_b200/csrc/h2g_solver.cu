@@ -500,8 +500,12 @@ static void launch_pbicg_body(Solver* s, cudaStream_t cs, const OpParams<T>& opA
   // t = A s_; omega = (t,s)/(t,t)                               NonUniform.jl:317-326
   launch_ax<T, 2, TP>(s, cs, opA, t, sh, nullptr, sv, st, kStageOmega);
   // x += alpha p_ + omega s_; r = s - omega t; res; next rho    NonUniform.jl:328-346
-  launch(s, k_bicg_update<T, TX, TP>, elementwise_blocks(s), 256, cs, g.n, x, ph, sh, r, sv, t, r0, st, s->partials, hc,
-                                                                  use_cond);
+  if (use_cond)
+    launch(s, k_bicg_update<T, TX, TP, true>, elementwise_blocks(s), 256, cs, g.n, x, ph, sh, r, sv, t, r0, st,
+           s->partials, hc, use_cond);
+  else
+    launch(s, k_bicg_update<T, TX, TP, false>, elementwise_blocks(s), 256, cs, g.n, x, ph, sh, r, sv, t, r0, st,
+           s->partials, hc, use_cond);
 }
 
 // z = M^-1 r with the first pass reading r (VM 0) and, for TP != T, writing bb32
@@ -537,7 +541,8 @@ static void launch_cg_body(Solver* s, cudaStream_t cs, const OpParams<T>& opA, c
   // rho_new = (r,z); beta                                       NonUniform.jl:206-215
   launch(s, k_dot<T, TP>, nb, 256, cs, g.n, r, z, nullptr, st, s->partials, kStageCgBeta);
   // p = z + beta p                                              NonUniform.jl:218-220
-  launch(s, k_cg_pupd<T, TP>, nb, 256, cs, g.n, p, z, st, hc, use_cond);
+  if (use_cond) launch(s, k_cg_pupd<T, TP, true>, nb, 256, cs, g.n, p, z, st, hc, use_cond);
+  else launch(s, k_cg_pupd<T, TP, false>, nb, 256, cs, g.n, p, z, st, hc, use_cond);
 }
 
 template <typename T, typename TP>
@@ -1020,10 +1025,14 @@ static int solve_sor(Solver* s, double omega, double tol, int maxItr, int verbos
   memcpy(sig.data() + sizeof op, &omega, sizeof omega);
   if (!G.exec || G.sig != sig) {
     rc = make_loop_graph(s, G, [&](cudaStream_t cs, cudaGraphConditionalHandle hc, int use_cond) {
-      launch(s, k_sor_pass, rg, blk, cs, op, s->th, (const double*)s->b, 0, omega, st, s->partials,
+      launch(s, k_sor_pass<false>, rg, blk, cs, op, s->th, (const double*)s->b, 0, omega, st, s->partials,
              (int)kStageSorHalf, hc, 0);
-      launch(s, k_sor_pass, rg, blk, cs, op, s->th, (const double*)s->b, 1, omega, st, s->partials,
-             (int)kStageSorIter, hc, use_cond);
+      if (use_cond)
+        launch(s, k_sor_pass<true>, rg, blk, cs, op, s->th, (const double*)s->b, 1, omega, st, s->partials,
+               (int)kStageSorIter, hc, use_cond);
+      else
+        launch(s, k_sor_pass<false>, rg, blk, cs, op, s->th, (const double*)s->b, 1, omega, st, s->partials,
+               (int)kStageSorIter, hc, use_cond);
     });
     if (rc) return rc;
     G.sig = sig;
