@@ -85,3 +85,17 @@ def test_workbuffers_layout():
     wk = h2_b200.WorkBuffers.allocate(7, 6, 5)
     assert wk.theta.flags.f_contiguous and wk.theta.shape == (7, 6, 5)
     assert wk.mask.min() == 1.0 and wk.lam.min() == 1.0 and wk.cp.min() == 1.0 and wk.rho.max() == 0.0
+
+
+def test_header_is_plain_c():
+    """include/h2g.h is a C header (plain pointers and sizes, no C++ or torch types): it compiles
+    as C99, so cgo, ccall, JNI or ctypes bindings can use it as it is."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    hdr = os.path.join(os.path.dirname(L.LIB_PATH), "..", "include", "h2g.h")
+    r = subprocess.run([cc, "-std=c99", "-Wall", "-Werror", "-fsyntax-only", "-x", "c", hdr], capture_output=True,
+                       text=True)
+    assert r.returncode == 0, r.stderr
