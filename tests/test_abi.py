@@ -99,3 +99,29 @@ def test_header_is_plain_c():
     r = subprocess.run([cc, "-std=c99", "-Wall", "-Werror", "-fsyntax-only", "-x", "c", hdr], capture_output=True,
                        text=True)
     assert r.returncode == 0, r.stderr
+
+
+def _build_c_caller(tmp_path):
+    """Compiles tests/abi_harness.c, a plain-C caller that sees only include/h2g.h, and links it
+    against the in-tree libh2g.so the way a foreign-language binding loads it."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    libdir = os.path.dirname(L.LIB_PATH)
+    exe = str(tmp_path / "abi_harness")
+    r = subprocess.run([cc, "-std=c99", "-Wall", "-Wextra", "-Werror", "-O1", "-I", os.path.join(root, "include"),
+                        os.path.join(root, "tests", "abi_harness.c"), "-L", libdir, "-lh2g",
+                        "-Wl,-rpath," + libdir, "-lm", "-o", exe], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    return exe
+
+
+def test_c_caller_host_checks(lib, tmp_path):
+    import subprocess
+    exe = _build_c_caller(tmp_path)
+    r = subprocess.run([exe, "host"], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert r.stdout.startswith("host checks ok")
