@@ -59,6 +59,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch", type=int, default=64, help="members of the batched workload (0 = skip)")
     ap.add_argument("--batch-steps", type=int, default=2)
+    ap.add_argument("--cg", type=int, default=1,
+                    help="1 = also time CG + RB-GS on the symmetric variant (adiabatic instead of convective faces)")
     ap.add_argument("--adjoint-steps", type=int, default=200,
                     help="implicit steps of the timed transient adjoint (0 = skip the adjoint section)")
     return ap.parse_args()
@@ -373,6 +375,7 @@ def run_ours(a, dist: Dist):
     except Exception as e:  # pragma: no cover
         log("e2e failed:", e)
 
+    cg_sym = run_cg_symmetric(a, dist, torch, stream, flush) if a.cg else None
     batch = run_batch(a, dist, torch, stream, flush) if a.batch > 0 else None
     adjoint = run_adjoint(a, dist, torch, stream) if a.adjoint_steps > 0 else None
 
@@ -421,6 +424,7 @@ def run_ours(a, dist: Dist):
                      "kernel": "k_rb_pass<double>: one RB-GS sweep (colour 0 then colour 1) of the FP64 smoother",
                      "algorithmic_bytes": rm["bytes"], "seconds": rm["seconds"], "peak_kind": peak_kind},
         "kernels": {f"{k[0]}_{k[1]}": v for k, v in roof.items()},
+        "cg_symmetric": cg_sym,
         "batch": batch,
         "adjoint": adjoint,
         "cpu_baseline": cpu,
@@ -433,6 +437,60 @@ def run_ours(a, dist: Dist):
     for s in solvers.values():
         s.close()
     dist.close()
+
+
+def run_cg_symmetric(a, dist, torch, stream, flush):
+    """CG + RB-GS(5) on the symmetric variant of the same stack: the convective faces replaced by
+    adiabatic ones (heat_flux_bc(0.0)), which leaves the operator symmetric positive definite.
+    FP64 and mixed precision from theta = 300 K to a.tol; CUDA events around each solve, L2
+    flushed before each; max over ranks."""
+    import h2_b200
+    from h2_b200 import model as M
+
+    m = M.build_mode3(a.nx, a.nx, a.nz, symmetric=True)
+    w = m.wk
+    out, solvers, local = {}, {}, {}
+    try:
+        for name in ("fp64", "mixed"):
+            s = h2_b200.Solver(*m.shape, precision=name, stream=stream.cuda_stream)
+            solvers[name] = s
+            s.set_grid(m.ZC, m.dZ, m.dx, m.dy, m.dt, m.HC, True)
+            s.set_fields(w.lam, w.mask)
+            s.set_rhs(w.b)
+            s.set_theta(w.theta)
+            s.snapshot()
+            ts, res = [], None
+            for r in range(a.warmup + a.steps):
+                s.snapshot(restore=True)
+                with torch.cuda.stream(stream):
+                    flush.zero_()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                st, res = s.solve("cg", tol=a.tol, maxItr=20000, smoother="gs")
+                e1.record(stream)
+                e1.synchronize()
+                if st != 0:
+                    raise RuntimeError(f"CG ({name}) did not converge: status {st}")
+                if r >= a.warmup:
+                    ts.append(e0.elapsed_time(e1) * 1e-3)
+            local[name] = float(np.mean(ts))
+            out[name] = {"iterations": res.itr, "restarts": res.outer, "final_rel_residual": res.res}
+        th = {k: v.get_theta()[1:-1, 1:-1, 1:-1] for k, v in solvers.items()}
+        out["mixed"]["max_abs_dtheta_vs_fp64_K"] = float(np.abs(th["mixed"] - th["fp64"]).max())
+    except Exception as e:  # pragma: no cover
+        log("CG on the symmetric variant failed:", e)
+        out = {"error": str(e)}
+    finally:
+        for s in solvers.values():
+            s.close()
+    # every rank takes the same collectives, whatever happened above
+    for name in ("fp64", "mixed"):
+        t_ = dist.max(local.get(name, float("nan")))
+        if name in out:
+            out[name]["seconds"] = t_
+    out["workload"] = (f"{a.nx}x{a.nx}x{a.nz} Mode-3 stack with adiabatic instead of convective faces, steady, "
+                       f"CG + RB-GS(5 sweeps), to ||r||/||r0|| <= {a.tol:g}")
+    return out
 
 
 def run_batch(a, dist, torch, stream, flush):
