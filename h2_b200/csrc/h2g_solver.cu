@@ -1339,7 +1339,8 @@ static int adjoint_transient(Solver* s, const FaceBC& f, int nt, const double* w
 // handle's grid (three interleaved rounds of two warm-up and ten timed sweeps each, on scratch
 // vectors) and keeps the fastest.  CalcAX is timed with dd summed and read from the array.
 // Choices are cached per (grid, smoother precision) for the process; H2G_RB_ROWS,
-// H2G_RB_PLANES, H2G_RB_DD and H2G_AX_DD in the environment force them (all four: no timing).
+// H2G_RB_PLANES, H2G_RB_DD and H2G_AX_DD in the environment force them (all four: no timing; a
+// forced H2G_RB_DD also restricts the timed variants to that dd source).
 static std::mutex g_tune_mu;
 static std::map<std::array<int, 4>, int> g_tune_cache;
 
@@ -1349,8 +1350,9 @@ static bool valid_rows(int r) {
   return false;
 }
 
+// only_dd: -1 = time dd read and summed, 0 / 1 = only that source (forced by the environment)
 template <typename T>
-static int tune_rows_t(Solver* s, const OpParams<T>& op, int* best_rows) {
+static int tune_rows_t(Solver* s, const OpParams<T>& op, int only_dd, int* best_rows) {
   const size_t n = (size_t)s->g.n, bytes = sizeof(double) * n;
   for (auto& p : s->hook)
     if (!p) CK(cudaMalloc(&p, bytes));
@@ -1382,6 +1384,7 @@ static int tune_rows_t(Solver* s, const OpParams<T>& op, int* best_rows) {
   for (int round = 0; round < kRounds && rc == H2G_OK; ++round)
   for (int shape = 0; shape < 16; ++shape) {
     const int by = kRbRows[shape & 3], np = 1 + ((shape >> 2) & 1), dd = shape >> 3;
+    if (only_dd >= 0 && dd != only_dd) continue;
     s->rb_rows = by;
     s->rb_planes = np;
     s->rb_dd = dd != 0;
@@ -1460,7 +1463,8 @@ static int autotune(Solver* s) {
   if (const char* e = getenv("H2G_RB_DD")) rbdd = atoi(e) ? 1 : 0;
   if (const char* e = getenv("H2G_AX_DD")) dd = atoi(e) ? 1 : 0;
   if (rows < 0 || planes < 0 || rbdd < 0 || dd < 0) {
-    const std::array<int, 4> key = {s->g.MX, s->g.MY, s->g.MZ, s->precision == H2G_FP64 ? 64 : 32};
+    // cached per grid, smoother precision and the dd source the environment restricts it to
+    const std::array<int, 4> key = {s->g.MX, s->g.MY, s->g.MZ, (s->precision == H2G_FP64 ? 64 : 32) * 4 + rbdd + 1};
     int cached = 0;
     {
       // held while tuning, so that handles of one grid solved concurrently (h2g_batch_solve) tune
@@ -1470,8 +1474,8 @@ static int autotune(Solver* s) {
       if (it != g_tune_cache.end()) cached = it->second;
       if (!cached) {
         int r2 = 0, d2 = 0;
-        int rc = s->precision == H2G_FP64 ? tune_rows_t<double>(s, op_params<double>(s, s->t64), &r2)
-                                          : tune_rows_t<float>(s, op_params<float>(s, s->t32), &r2);
+        int rc = s->precision == H2G_FP64 ? tune_rows_t<double>(s, op_params<double>(s, s->t64), rbdd, &r2)
+                                          : tune_rows_t<float>(s, op_params<float>(s, s->t32), rbdd, &r2);
         if (!rc) rc = tune_ax(s, &d2);
         if (rc) return rc;
         cached = r2 | (d2 << 8);
