@@ -230,16 +230,17 @@ static void launch_rb_np(const Solver* s, cudaStream_t cs, const OpParams<T>& op
       break;
   }
 }
+template <typename T, bool DD>
+static void launch_rb_dd(const Solver* s, cudaStream_t cs, const OpParams<T>& op, T* x, const T* bb, int color,
+                         T omega, const SolverState* st) {
+  if (s->rb_planes == 1) launch_rb_np<T, 1, DD>(s, cs, op, x, bb, color, omega, st);
+  else launch_rb_np<T, 2, DD>(s, cs, op, x, bb, color, omega, st);
+}
 template <typename T>
 static void launch_rb(const Solver* s, cudaStream_t cs, const OpParams<T>& op, T* x, const T* bb, int color, T omega,
                       const SolverState* st) {
-  if (s->rb_dd) {
-    if (s->rb_planes == 1) launch_rb_np<T, 1, true>(s, cs, op, x, bb, color, omega, st);
-    else launch_rb_np<T, 2, true>(s, cs, op, x, bb, color, omega, st);
-  } else {
-    if (s->rb_planes == 1) launch_rb_np<T, 1, false>(s, cs, op, x, bb, color, omega, st);
-    else launch_rb_np<T, 2, false>(s, cs, op, x, bb, color, omega, st);
-  }
+  if (s->rb_dd) launch_rb_dd<T, true>(s, cs, op, x, bb, color, omega, st);
+  else launch_rb_dd<T, false>(s, cs, op, x, bb, color, omega, st);
 }
 
 static size_t partials_needed(const Solver* s) {
@@ -1340,7 +1341,7 @@ static int adjoint_transient(Solver* s, const FaceBC& f, int nt, const double* w
 // vectors) and keeps the fastest.  CalcAX is timed with dd summed and read from the array.
 // Choices are cached per (grid, smoother precision) for the process; H2G_RB_ROWS,
 // H2G_RB_PLANES, H2G_RB_DD and H2G_AX_DD in the environment force them (all four: no timing; a
-// forced H2G_RB_DD also restricts the timed variants to that dd source).
+// forced rows, planes or dd source also restricts the timed variants to it).
 static std::mutex g_tune_mu;
 static std::map<std::array<int, 4>, int> g_tune_cache;
 
@@ -1350,9 +1351,10 @@ static bool valid_rows(int r) {
   return false;
 }
 
-// only_dd: -1 = time dd read and summed, 0 / 1 = only that source (forced by the environment)
+// only_rows / only_np / only_dd: -1 = time every value, else only that one (forced by the
+// environment)
 template <typename T>
-static int tune_rows_t(Solver* s, const OpParams<T>& op, int only_dd, int* best_rows) {
+static int tune_rows_t(Solver* s, const OpParams<T>& op, int only_rows, int only_np, int only_dd, int* best_rows) {
   const size_t n = (size_t)s->g.n, bytes = sizeof(double) * n;
   for (auto& p : s->hook)
     if (!p) CK(cudaMalloc(&p, bytes));
@@ -1378,13 +1380,15 @@ static int tune_rows_t(Solver* s, const OpParams<T>& op, int only_dd, int* best_
     launch_rb<T>(s, s->stream, op, xa, (const T*)xb, 0, T(1), nullptr);
     launch_rb<T>(s, s->stream, op, xa, (const T*)xb, 1, T(1), nullptr);
   }
-  float tbest[16];
-  for (int q = 0; q < 16; ++q) tbest[q] = 1e30f;
+  constexpr int kShapes = 16;  // 4 block heights x 2 plane counts x 2 dd sources
+  float tbest[kShapes];
+  for (int q = 0; q < kShapes; ++q) tbest[q] = 1e30f;
   constexpr int kRounds = 3;
   for (int round = 0; round < kRounds && rc == H2G_OK; ++round)
-  for (int shape = 0; shape < 16; ++shape) {
+  for (int shape = 0; shape < kShapes; ++shape) {
     const int by = kRbRows[shape & 3], np = 1 + ((shape >> 2) & 1), dd = shape >> 3;
-    if (only_dd >= 0 && dd != only_dd) continue;
+    if ((only_rows >= 0 && by != only_rows) || (only_np >= 0 && np != only_np) || (only_dd >= 0 && dd != only_dd))
+      continue;
     s->rb_rows = by;
     s->rb_planes = np;
     s->rb_dd = dd != 0;
@@ -1407,9 +1411,10 @@ static int tune_rows_t(Solver* s, const OpParams<T>& op, int only_dd, int* best_
     tbest[shape] = std::min(tbest[shape], ms);
     if (round == kRounds - 1 && tbest[shape] < best) {
       best = tbest[shape];
-      *best_rows = by | (np << 5) | (dd << 7);
+      *best_rows = by | (np << 5) | (dd << 8);
     }
   }
+  if (best == 1e30f) *best_rows = kBY | (2 << 5) | (1 << 8);  // nothing timed: the defaults
   s->rb_rows = saved;
   s->rb_planes = saved_np;
   s->rb_dd = saved_dd;
@@ -1463,8 +1468,9 @@ static int autotune(Solver* s) {
   if (const char* e = getenv("H2G_RB_DD")) rbdd = atoi(e) ? 1 : 0;
   if (const char* e = getenv("H2G_AX_DD")) dd = atoi(e) ? 1 : 0;
   if (rows < 0 || planes < 0 || rbdd < 0 || dd < 0) {
-    // cached per grid, smoother precision and the dd source the environment restricts it to
-    const std::array<int, 4> key = {s->g.MX, s->g.MY, s->g.MZ, (s->precision == H2G_FP64 ? 64 : 32) * 4 + rbdd + 1};
+    // cached per grid, smoother precision and the choices the environment restricts it to
+    const int forced = (rows + 1) + 18 * ((planes + 1) + 6 * (rbdd + 1));  // 0 .. 323
+    const std::array<int, 4> key = {s->g.MX, s->g.MY, s->g.MZ, (s->precision == H2G_FP64 ? 64 : 32) * 512 + forced};
     int cached = 0;
     {
       // held while tuning, so that handles of one grid solved concurrently (h2g_batch_solve) tune
@@ -1474,18 +1480,19 @@ static int autotune(Solver* s) {
       if (it != g_tune_cache.end()) cached = it->second;
       if (!cached) {
         int r2 = 0, d2 = 0;
-        int rc = s->precision == H2G_FP64 ? tune_rows_t<double>(s, op_params<double>(s, s->t64), rbdd, &r2)
-                                          : tune_rows_t<float>(s, op_params<float>(s, s->t32), rbdd, &r2);
+        int rc = s->precision == H2G_FP64
+                     ? tune_rows_t<double>(s, op_params<double>(s, s->t64), rows, planes, rbdd, &r2)
+                     : tune_rows_t<float>(s, op_params<float>(s, s->t32), rows, planes, rbdd, &r2);
         if (!rc) rc = tune_ax(s, &d2);
         if (rc) return rc;
-        cached = r2 | (d2 << 8);
+        cached = r2 | (d2 << 9);
         g_tune_cache[key] = cached;
       }
     }
     if (rows < 0) rows = cached & 0x1f;
-    if (planes < 0) planes = (cached >> 5) & 3;
-    if (rbdd < 0) rbdd = (cached >> 7) & 1;
-    if (dd < 0) dd = (cached >> 8) & 1;
+    if (planes < 0) planes = (cached >> 5) & 7;
+    if (rbdd < 0) rbdd = (cached >> 8) & 1;
+    if (dd < 0) dd = (cached >> 9) & 1;
   }
   if (rows != s->rb_rows || planes != s->rb_planes || (rbdd != 0) != s->rb_dd || (dd != 0) != s->ax_dd)
     invalidate_graphs(s);

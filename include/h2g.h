@@ -215,7 +215,7 @@ int h2g_transient(h2g_solver *h, const h2g_bc *bc, int nt, int method, double to
  * keeps the fastest; it also times the FP64 CalcAX with either dd source (the same bits in every
  * case).  The choices are cached per grid size and smoother precision for the process;
  * H2G_RB_ROWS, H2G_RB_PLANES, H2G_RB_DD and H2G_AX_DD (0/1) in the environment force them (all
- * four: no timing at all; a forced H2G_RB_DD times only the shapes with that dd source).  h2g_autotune runs the tuner now and reports its choices (each
+ * four: no timing at all; a forced rows, planes or dd source restricts the timing to it).  h2g_autotune runs the tuner now and reports its choices (each
  * pointer nullable): the colour pass's rows and planes, whether it reads dd (*rb_dd) and whether
  * CalcAX does (*ax_dd).  h2g_set_tuning forces a shape (rows 2, 4, 8 or 16 and planes 1 or 2;
  * rows = 0: tune again on the next solve). */

@@ -66,3 +66,20 @@ def test_dd_source_gives_identical_results(oracle, monkeypatch):
     assert outs[0][:2] == outs[1][:2]
     assert np.array_equal(outs[0][2], outs[1][2]) and np.array_equal(outs[0][3], outs[1][3])
     assert os.environ.get("H2G_AX_DD") == "1" and os.environ.get("H2G_RB_DD") == "1"
+
+
+def test_forced_choices_restrict_the_tuner(oracle, monkeypatch):
+    """A forced plane count or dd source is kept and the other choices are tuned around it."""
+    prob = mode3_model(oracle, 32)
+    for planes, dd in (("1", None), ("2", "0"), ("1", "1")):
+        monkeypatch.setenv("H2G_RB_PLANES", planes)
+        if dd is None:
+            monkeypatch.delenv("H2G_RB_DD", raising=False)
+        else:
+            monkeypatch.setenv("H2G_RB_DD", dd)
+        s = make_solver(prob)
+        rows, p, rb_dd, _ = s.tuning()
+        assert rows in (2, 4, 8, 16) and p == int(planes)
+        if dd is not None:
+            assert rb_dd == (dd == "1")
+        s.close()
