@@ -134,6 +134,33 @@ def test_nonfinite_and_unsupported_fields(oracle):
     s.close()
 
 
+def test_most_materials(oracle):
+    """127 distinct conductivities, the most a 7-bit material key holds: CalcAX and the 5-sweep
+    preconditioner stay bit-identical to the oracle.  A 128th distinct value is rejected on the
+    host (H2G_UNSUPPORTED) before any solve."""
+    prob = mode3_model(oracle, 20)
+    lam = prob.wk["lam"]
+    have = len(np.unique(lam))
+    rng = np.random.default_rng(3)
+    inner = np.argwhere(prob.wk["mask"] == 1.0)
+    pick = inner[rng.choice(len(inner), 128 - have, replace=False)]
+    vals = rng.uniform(0.5, 400.0, len(pick))
+    for (i, j, k), v in zip(pick[:-1], vals[:-1]):
+        lam[i, j, k] = v
+    assert len(np.unique(lam)) == 127
+    s = make_solver(prob)
+    x = random_interior(prob.shape, 5)
+    assert np.array_equal(s.calc_ax(x)[1:-1, 1:-1, 1:-1], oracle.calc_ax(prob, x)[1:-1, 1:-1, 1:-1])
+    bb = random_interior(prob.shape, 6)
+    assert np.array_equal(s.preconditioner(bb, "gs"), oracle.preconditioner(prob, bb, "gs"))
+    i, j, k = pick[-1]
+    lam[i, j, k] = vals[-1]
+    with pytest.raises(h2_b200.H2GError) as e:
+        s.set_fields(lam, prob.wk["mask"])
+    assert e.value.status == 7  # H2G_UNSUPPORTED
+    s.close()
+
+
 @pytest.mark.parametrize("case", CASES, ids=["mode3", "adiabatic", "odd", "transient"])
 def test_calcax_symmetric(oracle, case):
     """(A x, y) = (x, A y) to rounding on the GPU operator (test_symmetry.jl:11-81 restated): the
