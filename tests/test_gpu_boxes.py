@@ -1,0 +1,94 @@
+"""Kernels and solves on hand-built boxes against the oracle: tiny and odd grid sizes (one cell
+wide, a half-row spanning two warps), odd and small NZ (the two-planes-per-thread colour pass
+then has a last plane pair with one plane outside the grid), a non-uniform Z grid, five
+materials at random, and all three boundary types on the six faces (isothermal at two
+temperatures, convection at two coefficients, heat flux, adiabatic).  Every launch shape of the
+colour pass must give the oracle's bits."""
+import numpy as np
+import pytest
+
+from test_gpu_kernels import make_solver, random_interior
+
+pytestmark = pytest.mark.gpu
+
+GRIDS = [(1, 1, 3), (6, 5, 7), (3, 2, 5), (33, 31, 9), (65, 4, 4), (70, 9, 1)]
+SHAPES = [(8, 2), (2, 1), (16, 2), (4, 1)]
+
+
+def box_problem(O, NX, NY, NZ, seed, transient=False):
+    """A box with random materials and mixed boundary conditions, set up with the oracle's own
+    boundary routine (apply_boundary_conditions! / set_BC_coef) and calRHS!."""
+    MX, MY, MZ = NX + 2, NY + 2, NZ + 2
+    shape = (MX, MY, MZ)
+    rng = np.random.default_rng(seed)
+    dz = rng.uniform(2e-6, 2e-5, NZ)
+    zf = np.concatenate([[0.0], np.cumsum(dz)])
+    ZC = np.empty(MZ)
+    ZC[0], ZC[-1] = zf[0], zf[-1]  # guards on the faces, as genZ!
+    ZC[1:-1] = 0.5 * (zf[1:] + zf[:-1])
+    dZ = np.concatenate([[dz[0]], dz, [dz[-1]]])
+    Z = np.concatenate([[2 * zf[0] - zf[min(1, NZ)]], zf, [2 * zf[-1] - zf[-2]]])
+    wk = {n: O.zeros(shape) for n in O._WK_NAMES}
+    mats = np.array([0.4, 1.5, 50.0, 149.0, 386.0])
+    wk["lam"][...] = mats[rng.integers(0, len(mats), shape)]
+    wk["rho"][...] = rng.uniform(1e3, 9e3, shape)
+    wk["cp"][...] = rng.uniform(300.0, 900.0, shape)
+    wk["mask"][...] = 1.0
+    wk["theta"][...] = 300.0
+    bcs = [O.isothermal_bc(300.0), O.convection_bc(5.0, 290.0), O.heat_flux_bc(2.0e4), O.adiabatic_bc(),
+           O.isothermal_bc(320.0), O.convection_bc(12.0, 300.0)]
+    bca = O.bc_array(bcs)
+    L = O.lib()
+    L.h2o_apply_bc(MX, MY, MZ, bca, O._p(wk["theta"]), O._p(wk["lam"]), O._p(wk["rho"]), O._p(wk["cp"]),
+                   O._p(wk["mask"]))
+    HC = np.zeros(6)
+    L.h2o_set_bc_coef(bca, O._p(HC))
+    wk["hsrc"][1:-1, 1:-1, 1:-1] = rng.uniform(0.0, 1.0e12, (NX, NY, NZ))
+    ID = np.zeros(shape, dtype=np.uint8, order="F")
+    prob = O.Problem(NX, NY, NZ, 1.0e-5, 1.3e-5, 1.0e-4 if transient else 1.0, not transient, Z, ZC, dZ, HC, bcs,
+                     ID, wk)
+    O.calRHS(prob)
+    return prob
+
+
+@pytest.mark.parametrize("transient", [False, True], ids=["steady", "transient"])
+@pytest.mark.parametrize("grid", GRIDS, ids=["x".join(map(str, g)) for g in GRIDS])
+def test_box_kernels_bit_exact(oracle, grid, transient):
+    prob = box_problem(oracle, *grid, seed=sum(grid), transient=transient)
+    s = make_solver(prob)
+    x = random_interior(prob.shape, 1)
+    assert np.array_equal(s.calc_ax(x)[1:-1, 1:-1, 1:-1], oracle.calc_ax(prob, x)[1:-1, 1:-1, 1:-1])
+    r, res = s.calc_rk()
+    r_ref, res_ref = oracle.calc_rk(prob)
+    assert np.array_equal(r[1:-1, 1:-1, 1:-1], r_ref[1:-1, 1:-1, 1:-1])
+    assert abs(res - res_ref) <= 1e-13 * res_ref
+    b = random_interior(prob.shape, 2)
+    bb = random_interior(prob.shape, 3)
+    pre_ref = oracle.preconditioner(prob, bb, "gs")
+    for rows, planes in SHAPES:
+        s.set_tuning(rows, planes)
+        for color, omega in ((0, 1.0), (1, 1.0), (0, 1.7)):
+            xr = x.copy(order="F")
+            oracle.rbsor_core(prob, xr, b, color, omega=omega)
+            assert np.array_equal(s.rbsor_pass(x.copy(order="F"), b, color, omega), xr), (rows, planes, color)
+        assert np.array_equal(s.preconditioner(bb, "gs"), pre_ref), (rows, planes)
+    s.close()
+
+
+@pytest.mark.parametrize("method", ["pbicgstab", "cg"])
+@pytest.mark.parametrize("grid", [(6, 5, 7), (33, 31, 9), (70, 9, 1)], ids=["6x5x7", "33x31x9", "70x9x1"])
+def test_box_solve(oracle, grid, method):
+    """The solve on a box converges like the oracle's (iterations within 10 %, at least 2) to the
+    same field (1e-3 K)."""
+    prob = box_problem(oracle, *grid, seed=7)
+    ref = box_problem(oracle, *grid, seed=7)
+    fn = oracle.pbicgstab if method == "pbicgstab" else oracle.cg
+    conv, itr, res0, _ = fn(ref, tol=1e-10, maxItr=20000, smoother="gs")
+    assert conv
+    s = make_solver(prob)
+    st, res = s.solve(method, tol=1e-10, maxItr=20000, smoother="gs")
+    assert st == 0 and res.isconverged
+    assert abs(res.res0 - res0) <= 1e-12 * res0
+    assert abs(res.itr - itr) <= max(2, itr // 10), (res.itr, itr)
+    assert np.abs(s.get_theta() - ref.wk["theta"]).max() <= 1e-3
+    s.close()
