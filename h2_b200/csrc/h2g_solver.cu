@@ -1012,7 +1012,6 @@ static int solve_sor(Solver* s, double omega, double tol, int maxItr, int verbos
   const Geo& g = s->g;
   int rc = ensure_hist(s, maxItr);
   if (rc) return rc;
-  if (rc) return rc;
   const OpParams<double> op = op_params<double>(s, s->t64);
   SolverState* st = s->st;
   if ((rc = prime_state(s, st, tol, maxItr, s->hist, maxItr))) return rc;
