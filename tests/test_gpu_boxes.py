@@ -117,3 +117,43 @@ def test_box_sor_bit_exact(oracle, grid):
     assert np.allclose(hist, hist_r, rtol=1e-12, atol=0)
     assert np.array_equal(s.get_theta(), ref.wk["theta"])
     s.close()
+
+
+@pytest.mark.parametrize("transient", [False, True], ids=["steady", "transient"])
+@pytest.mark.parametrize("grid", GRIDS, ids=["x".join(map(str, g)) for g in GRIDS])
+def test_box_calrhs_bit_exact(oracle, grid, transient):
+    """calRHS! on a box with every boundary type and a random temperature field."""
+    prob = box_problem(oracle, *grid, seed=11, transient=transient)
+    rng = np.random.default_rng(5)
+    prob.wk["theta"][1:-1, 1:-1, 1:-1] = 300.0 + 40.0 * rng.random(grid)
+    prob.wk["b"][...] = 0.0
+    oracle.calRHS(prob)
+    s = make_solver(prob)
+    s.set_hsrc(prob.wk["hsrc"])
+    s.calrhs(prob.bcs, zero_b=True)
+    assert np.array_equal(s.get_rhs(), prob.wk["b"])
+    s.close()
+
+
+@pytest.mark.parametrize("grid", [(6, 5, 7), (33, 31, 9)], ids=["6x5x7", "33x31x9"])
+def test_box_time_loop(oracle, grid):
+    """Four implicit steps (dt = 1e-4 s) of the time loop on a box with every boundary type:
+    b rebuilt from zero each step, the solve from the previous field, against the oracle's loop."""
+    nt, tol = 4, 1e-10
+    prob = box_problem(oracle, *grid, seed=13, transient=True)
+    ref = box_problem(oracle, *grid, seed=13, transient=True)
+    s = make_solver(prob)
+    s.set_hsrc(prob.wk["hsrc"])
+    st, res, stats = s.transient(prob.bcs, nt, tol=tol, smoother="gs")
+    assert st == 0 and res.isconverged and res.outer == nt
+    w = ref.wk
+    for step in range(nt):
+        w["b"][...] = 0.0
+        oracle.calRHS(ref)
+        conv, itr, _, _ = oracle.pbicgstab(ref, tol=tol, maxItr=20000, smoother="gs")
+        assert conv
+        inner = w["theta"][1:-1, 1:-1, 1:-1]
+        assert abs(stats[step, 3] - itr) <= max(2, 0.1 * itr)
+        assert abs(stats[step, 0] - inner.min()) <= 1e-3 and abs(stats[step, 1] - inner.max()) <= 1e-3
+    assert np.abs(s.get_theta() - w["theta"]).max() <= 1e-3
+    s.close()
