@@ -157,3 +157,36 @@ def test_box_time_loop(oracle, grid):
         assert abs(stats[step, 0] - inner.min()) <= 1e-3 and abs(stats[step, 1] - inner.max()) <= 1e-3
     assert np.abs(s.get_theta() - w["theta"]).max() <= 1e-3
     s.close()
+
+
+def test_box_steady_adjoint(oracle):
+    """h2g_adjoint on a box with every boundary type (heat-flux and convective guards carry
+    lambda = 0, isothermal guards a copy of their neighbour's): J and both gradient fields against
+    the oracle's FP64 forward and adjoint solves with the numpy restatement of the gradient."""
+    from oracle import adjoint as OA
+
+    from h2_b200 import adjoint as A
+    grid, P = (33, 31, 9), 8.0
+    prob = box_problem(oracle, *grid, seed=17)
+    w = np.zeros(prob.shape, order="F")
+    w[1:-1, 1:-1, 1:-1] = (prob.dx * prob.dy) * prob.dZ[None, None, 1:-1]
+    s = make_solver(prob)
+    J, gh, gl, rf, ra = A.steady_gradient(s, w, P, tol=1e-12)
+    assert rf.isconverged and ra.isconverged
+    th = s.get_theta()
+    s.close()
+    fwd = box_problem(oracle, *grid, seed=17)
+    assert oracle.pbicgstab(fwd, tol=1e-12, maxItr=20000, smoother="gs")[0]
+    th_ref = fwd.wk["theta"]
+    assert np.abs(th - th_ref).max() <= 1e-6
+    J_ref = OA.objective(th_ref, w, P)
+    assert abs(J - J_ref) <= 1e-12 * J_ref
+    adj = box_problem(oracle, *grid, seed=17)
+    adj.wk["theta"][...] = 0.0
+    adj.wk["b"][...] = OA.adj_rhs(th_ref, w, P)
+    assert oracle.pbicgstab(adj, tol=1e-12, maxItr=20000, smoother="gs")[0]
+    w_ = prob.wk
+    gh_ref, gl_ref = OA.gradients(w_["lam"], w_["mask"], th_ref, adj.wk["theta"], prob.dx, prob.dy, prob.ZC,
+                                  prob.dZ)
+    assert np.abs(gh - gh_ref).max() <= 1e-6 * np.abs(gh_ref).max()
+    assert np.abs(gl - gl_ref).max() <= 1e-6 * np.abs(gl_ref).max()
