@@ -35,7 +35,7 @@ extern "C" {
 #define H2G_BAD_ARG 4         /* rejected on the host before any launch */
 #define H2G_CUDA_ERROR 5      /* a CUDA runtime call failed */
 #define H2G_TIMEOUT 6         /* a bounded device wait ran out */
-#define H2G_UNSUPPORTED 7     /* input outside what this build implements (message says what) */
+#define H2G_UNSUPPORTED 7     /* input outside what the library implements (message says what) */
 
 /* ---- precision ---------------------------------------------------------------------- */
 #define H2G_FP64 0     /* FP64 throughout, same arithmetic as the reference */
