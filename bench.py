@@ -5,8 +5,9 @@ One step = one steady solve from theta = 300 K to ||r||/||r0|| <= 1e-8 on inputs
 HBM.  The headline `value` is the FP64 GPU solver (every kernel bit-identical per cell to the
 reference's FP64 arithmetic).  The mixed variant (FP32 RB-GS preconditioner inside the FP64
 PBiCGSTAB, restarted on the FP64 true residual) is timed on the same inputs and reported beside
-it with its max |theta - theta_FP64|; on this operator it needs ~5x the iterations, so it is
-slower (the measured evidence is in the JSON line).
+it with its max |theta - theta_FP64|; on this operator it needs about twice the iterations, so
+it is slower (the measured evidence is in the JSON line).  CG + RB-GS on the symmetric variant of
+the stack (adiabatic instead of convective faces) is timed in FP64 and mixed precision too.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
