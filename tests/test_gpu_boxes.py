@@ -190,3 +190,40 @@ def test_box_steady_adjoint(oracle):
                                   prob.dZ)
     assert np.abs(gh - gh_ref).max() <= 1e-6 * np.abs(gh_ref).max()
     assert np.abs(gl - gl_ref).max() <= 1e-6 * np.abs(gl_ref).max()
+
+
+def singular_box(O, NX, NY, NZ, seed=21):
+    """A steady box with every face adiabatic and a heat source: A is singular (pure Neumann)
+    and the system has no solution (the net heat input is not zero)."""
+    p = box_problem(O, NX, NY, NZ, seed)
+    MX, MY, MZ = p.shape
+    w = p.wk
+    rng = np.random.default_rng(seed)
+    w["lam"][...] = np.array([0.4, 1.5, 50.0, 149.0, 386.0])[rng.integers(0, 5, p.shape)]
+    w["mask"][...] = 1.0
+    w["theta"][...] = 300.0
+    w["b"][...] = 0.0
+    p.bcs = [O.adiabatic_bc()] * 6
+    O.lib().h2o_apply_bc(MX, MY, MZ, O.bc_array(p.bcs), O._p(w["theta"]), O._p(w["lam"]), O._p(w["rho"]),
+                         O._p(w["cp"]), O._p(w["mask"]))
+    p.HC[...] = 0.0
+    O.calRHS(p)
+    return p
+
+
+@pytest.mark.parametrize("method", ["pbicgstab", "cg"])
+@pytest.mark.parametrize("grid", [(6, 5, 7), (33, 31, 9)], ids=["6x5x7", "33x31x9"])
+def test_box_singular_system(oracle, grid, method):
+    """No solution: the oracle runs to maxItr without converging.  The GPU solve ends within
+    maxItr with a failure status: NOT_CONVERGED after maxItr iterations, or BREAKDOWN or
+    NONFINITE earlier if its rounding takes it there first."""
+    ref = singular_box(oracle, *grid)
+    fn = oracle.pbicgstab if method == "pbicgstab" else oracle.cg
+    conv, itr, res0, _ = fn(ref, tol=1e-10, maxItr=500, smoother="gs")
+    assert not conv and itr == 500
+    s = make_solver(singular_box(oracle, *grid))
+    st, res = s.solve(method, tol=1e-10, maxItr=500, smoother="gs")
+    assert st in (1, 2, 3) and st == res.status and not res.isconverged
+    assert res.itr <= 500 and (st != 1 or res.itr == 500)
+    assert abs(res.res0 - res0) <= 1e-12 * res0
+    s.close()
