@@ -34,7 +34,7 @@ extern "C" {
 #define H2G_NONFINITE 3       /* NaN/Inf in an input array or in the iteration */
 #define H2G_BAD_ARG 4         /* rejected on the host before any launch */
 #define H2G_CUDA_ERROR 5      /* a CUDA runtime call failed */
-#define H2G_TIMEOUT 6         /* a bounded device wait ran out */
+#define H2G_TIMEOUT 6         /* a bounded device wait ran out (reserved: no kernel here waits) */
 #define H2G_UNSUPPORTED 7     /* input outside what the library implements (message says what) */
 
 /* ---- precision ---------------------------------------------------------------------- */
