@@ -37,6 +37,14 @@ namespace h2g {
 #ifndef H2G_NKEY
 #define H2G_NKEY 1
 #endif
+// CalcAX asks the compiler for 5 resident blocks of 256 threads per SM (48 registers; the
+// variants that read dd spill 4-12 bytes).  Per FP64 solve, with the same bits: equal at
+// 240x240x30 and -3 % at 480x480x60 against no request (58-72 registers); -4 % and -11 %
+// against an explicit 1-block request (66-88 registers).  A 6-block cap (40 registers) spills
+// more and gains less.
+#ifndef H2G_AX_MINB
+#define H2G_AX_MINB 5
+#endif
 
 constexpr int kBX = 32;       // threads along the half-row
 constexpr int kBY = H2G_BY;   // rows per block
@@ -708,7 +716,7 @@ __device__ __forceinline__ void load_pair(const Geo& g, const TI* x, const uint8
 // DD: read dd from the per-cell array (FP64 only; the FP32 operator uses the difference form).
 // Which is faster depends on whether the vectors stay in L2; the launch-shape tuner decides.
 template <typename T, int NDOT, typename TI = T, bool DD = false>
-__global__ void __launch_bounds__(kThreads) k_ax(OpParams<T> op, T* __restrict__ y, const TI* __restrict__ x,
+__global__ void __launch_bounds__(kThreads, H2G_AX_MINB) k_ax(OpParams<T> op, T* __restrict__ y, const TI* __restrict__ x,
                                                   const T* __restrict__ u, const T* __restrict__ w,
                                                   SolverState* st, double* __restrict__ partials, int stage) {
   pdl_enter();
