@@ -22,15 +22,6 @@ def test_fill_id_refined_z(oracle):
     assert np.array_equal(model.fill_id(48, 48, 60), oracle.fill_id(48, 48, 60))
 
 
-def test_zgrid_and_pitch(oracle):
-    from h2_b200 import model
-    for nz in (30, 60, 120):
-        for a, b in zip(model.zgrid(nz), oracle.genz(nz)):
-            assert np.array_equal(a, b)
-    for n in (20, 40, 120, 180, 240, 480, 960):
-        assert model.pitch(n) == oracle.pitch(n)
-
-
 @pytest.mark.parametrize("kw", [dict(), dict(symmetric=True), dict(is_steady=False, dt=1e-4)])
 def test_build_mode3_bit_exact(oracle, kw):
     from h2_b200 import model
