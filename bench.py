@@ -281,13 +281,13 @@ def run_ours(a, dist: Dist):
 
     solvers = {"fp64": make("fp64"), "mixed": make("mixed")}
 
-    def one(s, timed: bool):
+    def one(s, timed: bool, tol=None):
         s.snapshot(restore=True)
         with torch.cuda.stream(stream):
             flush.zero_()
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ev0.record(stream)
-        st, res = s.solve("pbicgstab", tol=a.tol, maxItr=20000, smoother="gs")
+        st, res = s.solve("pbicgstab", tol=a.tol if tol is None else tol, maxItr=20000, smoother="gs")
         ev1.record(stream)
         ev1.synchronize()
         if st != 0:
@@ -317,6 +317,18 @@ def run_ours(a, dist: Dist):
 
     th = {k: solvers[k].get_theta()[1:-1, 1:-1, 1:-1] for k in solvers}
     max_dtheta = float(np.abs(th["mixed"] - th["fp64"]).max())
+
+    # ---- the case the reference publishes a solve time for: the same solve to eps = 1e-4
+    readme = None
+    if a.nx == 240 and a.nz == 30:  # the same decision on every rank
+        ts_r, res_r = [], None
+        for r in range(2 + a.steps):
+            dt_, res_r = one(solvers["fp64"], True, tol=1e-4)
+            if r >= 2:
+                ts_r.append(dt_)
+        readme = {"tol": 1e-4, "seconds": dist.max(float(np.mean(ts_r))), "iterations": res_r.itr,
+                  "reference_published": {"seconds": 183.0, "iterations": 208, "hardware": "not stated",
+                                          "source": "the reference's README.md:174-182 (Julia; compute time of this solve)"}}
 
     # ---- roofline of the dominant kernel: one RB-GS sweep (2 launches of the colour pass)
     peak, peak_kind = measured_peaks()
@@ -429,6 +441,7 @@ def run_ours(a, dist: Dist):
                      "kernel": "k_rb_pass<double>: one RB-GS sweep (colour 0 then colour 1) of the FP64 smoother",
                      "algorithmic_bytes": rm["bytes"], "seconds": rm["seconds"], "peak_kind": peak_kind},
         "kernels": {f"{k[0]}_{k[1]}": v for k, v in roof.items()},
+        "readme_case": readme,
         "cg_symmetric": cg_sym,
         "batch": batch,
         "adjoint": adjoint,
