@@ -190,6 +190,10 @@ class BatchSolver:
         return st, list(outs)
 
     def solve_sequential(self, method="pbicgstab", tol=1e-8, maxItr=20_000, smoother="gs"):
+        """The same members one after another through the single-solve calls (method "sor":
+        solveSOR! with omega = 1, as h2g_batch_solve runs it)."""
+        if method == "sor":
+            return [s.sor(omega=1.0, tol=tol, maxItr=maxItr)[1] for s in self.solvers]
         return [s.solve(method, tol=tol, maxItr=maxItr, smoother=smoother)[1] for s in self.solvers]
 
     def close(self):

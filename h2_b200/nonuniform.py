@@ -153,7 +153,10 @@ class Solver:
         L.check(self.lib.h2g_set_mixed_params(self.h, float(inner_tol), int(max_outer)))
 
     def solve(self, method="pbicgstab", tol=1e-6, maxItr=20_000, smoother="gs", verbose=False, hist=None):
-        """Returns (status, Result); the status is also Result.status."""
+        """Returns (status, Result); the status is also Result.status.  method: "pbicgstab" or
+        "cg" (solveSOR! is Solver.sor)."""
+        if method not in ("pbicgstab", "cg"):
+            raise ValueError(f"unknown method {method!r}: use 'pbicgstab' or 'cg' (or Solver.sor)")
         sm = smoother_selector(smoother)
         res = L.Result()
         fn = self.lib.h2g_pbicgstab if method == "pbicgstab" else self.lib.h2g_cg

@@ -56,3 +56,27 @@ def test_batch_rejects_duplicates(small_batch):
     hs = (C.c_void_p * 2)(s.h.value, s.h.value)
     outs = (L.Result * 2)()
     assert L.load().h2g_batch_solve(2, hs, 0, 1e-8, 100, 1, 2, outs) == L.H2G_BAD_ARG
+
+
+@pytest.mark.parametrize("method", ["cg", "sor"])
+def test_batch_other_methods_equal_sequential(method):
+    """h2g_batch_solve with CG and with solveSOR! (omega = 1): each member gets the results of its
+    lone solve through the single-solve call."""
+    ms = B.draw_batch(3, 1000, sizes=(24, 32))
+    bs = B.BatchSolver(ms)
+    try:
+        tol, maxItr = (1e-8, 20000) if method == "cg" else (1e-4, 400)
+        bs.restore()
+        st, res = bs.solve(method=method, tol=tol, maxItr=maxItr)
+        th = [s.get_theta() for s in bs.solvers]
+        bs.restore()
+        seq = bs.solve_sequential(method=method, tol=tol, maxItr=maxItr)
+        for r, q, s, t in zip(res, seq, bs.solvers, th):
+            assert (r.itr, r.res0, r.res, r.status) == (q.itr, q.res0, q.res, q.status)
+            assert np.array_equal(s.get_theta(), t)
+        if method == "cg":
+            assert all(r.isconverged for r in res)
+        with pytest.raises(ValueError):
+            bs.solvers[0].solve("sor")
+    finally:
+        bs.close()
