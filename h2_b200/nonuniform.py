@@ -41,6 +41,17 @@ def _ptr(a):
     return None if a is None else a.ctypes.data_as(C.POINTER(C.c_double))
 
 
+def _hist(hist, maxItr):
+    """The residual-history buffer: the library writes up to maxItr doubles into it."""
+    if hist is None:
+        return None
+    if not isinstance(hist, np.ndarray) or hist.dtype != np.float64 or not hist.flags.c_contiguous:
+        raise TypeError("hist: expected a contiguous Float64 array")
+    if hist.size < int(maxItr):
+        raise ValueError(f"hist holds {hist.size} values; the solve may write maxItr = {int(maxItr)}")
+    return _ptr(hist)
+
+
 def smoother_selector(s) -> int:
     """smoother_selector (NonUniform.jl:36-41): :none / :gs, anything else is an ArgumentError."""
     key = s.lstrip(":") if isinstance(s, str) else s
@@ -160,7 +171,7 @@ class Solver:
         sm = smoother_selector(smoother)
         res = L.Result()
         fn = self.lib.h2g_pbicgstab if method == "pbicgstab" else self.lib.h2g_cg
-        st = fn(self.h, float(tol), int(maxItr), sm, int(bool(verbose)), _ptr(hist), C.byref(res))
+        st = fn(self.h, float(tol), int(maxItr), sm, int(bool(verbose)), _hist(hist, maxItr), C.byref(res))
         L.check(st, allowed=(L.H2G_OK, L.H2G_NOT_CONVERGED, L.H2G_BREAKDOWN, L.H2G_NONFINITE))
         return st, res
 
@@ -190,7 +201,7 @@ class Solver:
     def sor(self, omega=1.0, tol=1e-6, maxItr=20_000, verbose=False, hist=None):
         """solveSOR! on the handle's theta and b (FP64).  Returns (status, Result)."""
         res = L.Result()
-        st = self.lib.h2g_sor(self.h, float(omega), float(tol), int(maxItr), int(bool(verbose)), _ptr(hist),
+        st = self.lib.h2g_sor(self.h, float(omega), float(tol), int(maxItr), int(bool(verbose)), _hist(hist, maxItr),
                               C.byref(res))
         L.check(st, allowed=(L.H2G_OK, L.H2G_NOT_CONVERGED, L.H2G_NONFINITE))
         return st, res
@@ -264,11 +275,12 @@ def _oneshot(method, wk, dh, dt, ZC, dZ, HC, tol, maxItr, smoother, par, verbose
     HC = np.ascontiguousarray(HC, dtype=np.float64)
     if ZC.size != MZ or dZ.size != MZ or HC.size != 6:
         raise ValueError("ZC needs MZ entries, dZ MZ (or MZ-1), HC 6")
+    hp = _hist(hist, maxItr)
     res = L.Result()
     fn = lib.h2g_PBiCGSTAB if method == "pbicgstab" else lib.h2g_CG
     st = fn(MX, MY, MZ, _ptr(wk.theta), _ptr(wk.b), _ptr(wk.lam), _ptr(wk.mask), _ptr(wk.rho), _ptr(wk.cp), dx, dy,
             float(dt), _ptr(ZC), _ptr(dZ), _ptr(HC), float(tol), int(maxItr), sm, int(bool(verbose)),
-            int(bool(is_steady)), _PRECISION[precision], _ptr(hist), C.byref(res))
+            int(bool(is_steady)), _PRECISION[precision], hp, C.byref(res))
     L.check(st, allowed=(L.H2G_OK, L.H2G_NOT_CONVERGED, L.H2G_BREAKDOWN, L.H2G_NONFINITE))
     return bool(res.isconverged), int(res.itr), float(res.res0)
 
@@ -314,7 +326,7 @@ def solveSOR(theta, lam, b, mask, rho, cp, dh, dt, omega, ZC, dZ, HC, F=None, to
     res = L.Result()
     st = lib.h2g_SolveSOR(MX, MY, MZ, _ptr(theta), _ptr(b), _ptr(lam), _ptr(mask), _ptr(rho), _ptr(cp), dx, dy,
                           float(dt), float(omega), _ptr(ZC), _ptr(dZ), _ptr(HC), float(tol), int(maxItr),
-                          int(bool(verbose)), int(bool(is_steady)), _ptr(hist), C.byref(res))
+                          int(bool(verbose)), int(bool(is_steady)), _hist(hist, maxItr), C.byref(res))
     L.check(st, allowed=(L.H2G_OK, L.H2G_NOT_CONVERGED, L.H2G_NONFINITE))
     if F is not None:
         for n in range(int(res.itr)):

@@ -125,3 +125,16 @@ def test_c_caller_host_checks(lib, tmp_path):
     r = subprocess.run([exe, "host"], capture_output=True, text=True, timeout=120)
     assert r.returncode == 0, r.stdout + r.stderr
     assert r.stdout.startswith("host checks ok")
+
+
+def test_history_buffer_checked_on_host(lib):
+    """The library writes up to maxItr residuals into the caller's history buffer: a shorter or
+    non-Float64 buffer is refused before any call reaches the device."""
+    wk = h2_b200.WorkBuffers.allocate(6, 6, 6)
+    z6, hc = np.linspace(0.0, 1e-3, 6), np.zeros(6)
+    for bad, err in ((np.zeros(9), ValueError), (np.zeros(10, dtype=np.float32), TypeError)):
+        with pytest.raises(err):
+            h2_b200.PBiCGSTAB(wk, (1e-5, 1e-5, 1.0), 1.0, z6, np.full(6, 2e-4), hc, maxItr=10, hist=bad)
+        with pytest.raises(err):
+            h2_b200.solveSOR(wk.theta, wk.lam, wk.b, wk.mask, wk.rho, wk.cp, (1e-5, 1e-5, 1.0), 1.0, 1.5, z6,
+                             np.full(6, 2e-4), hc, None, 1e-6, maxItr=10, hist=bad)
