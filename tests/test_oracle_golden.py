@@ -144,3 +144,18 @@ def test_sor_solver_reaches_tolerance(oracle):
     n, res0, hist = oracle.solve_sor(prob, omega=1.5, tol=1e-3, maxItr=300)
     assert n == -300 and res0 > 0
     assert hist[-1] < hist[100] < hist[1]
+
+
+def test_threaded_oracle_tracks_sequential(oracle):
+    """The CPU baseline runs the oracle with OpenMP reductions on every core.  Its solve on the
+    60x60x30 Mode-3 stack converges like the sequential (Julia-order) one: iterations within
+    10 % and the same field within 1e-6 K at 1e-10."""
+    a = mode3_model(oracle, 60)
+    b = mode3_model(oracle, 60)
+    conv_s, itr_s, res0_s, _ = oracle.pbicgstab(a, tol=1e-10, maxItr=20000, smoother="gs", red_mode=oracle.RED_SEQ)
+    conv_t, itr_t, res0_t, _ = oracle.pbicgstab(b, tol=1e-10, maxItr=20000, smoother="gs", red_mode=oracle.RED_OMP,
+                                                threads=4)
+    assert conv_s and conv_t
+    assert abs(itr_t - itr_s) <= max(1, itr_s // 10), (itr_t, itr_s)
+    assert abs(res0_t - res0_s) <= 1e-13 * res0_s
+    assert np.abs(a.wk["theta"] - b.wk["theta"]).max() <= 1e-6
