@@ -484,7 +484,7 @@ static void launch_pbicg_body(Solver* s, cudaStream_t cs, const OpParams<T>& opA
   TP* sh = kvec<TP>(s, KSH);
   T* t = kvec<T>(s, KT);
   TP* bbm = std::is_same<T, TP>::value ? nullptr : kvec<TP>(s, KBB);
-  const dim3 rg = rb_grid(g), ag = ax_grid(g), blk(kBX, kBY);
+  const dim3 blk(kBX, kBY);
   const int none = smoother == H2G_SMOOTHER_NONE;
   // p = r + beta (p - omega q); p_ = M^-1 p                     NonUniform.jl:296-305
   launch(s, k_rb_first<TP, T, 1>, first_grid(g), blk, cs, opM, ph, p, bbm, r, q, st, none);
@@ -514,7 +514,7 @@ template <typename T, typename TP>
 static void launch_precond_r(Solver* s, cudaStream_t cs, const OpParams<TP>& opM, TP* z, T* r, SolverState* st,
                              int smoother) {
   const Geo& g = s->g;
-  const dim3 rg = rb_grid(g), blk(kBX, kBY);
+  const dim3 blk(kBX, kBY);
   const int none = smoother == H2G_SMOOTHER_NONE;
   TP* bbm = std::is_same<T, TP>::value ? nullptr : kvec<TP>(s, KBB);
   launch(s, k_rb_first<TP, T, 0>, first_grid(g), blk, cs, opM, z, r, bbm, nullptr, nullptr, st, none);
@@ -531,7 +531,7 @@ static void launch_cg_body(Solver* s, cudaStream_t cs, const OpParams<T>& opA, c
   T* p = kvec<T>(s, KP);
   T* q = kvec<T>(s, KQ);
   TP* z = kvec<TP>(s, KPH);  // z (pcg_s in NonUniform.jl:146) in the preconditioner-output buffer
-  const dim3 ag = ax_grid(g), blk(kBX, kBY);
+  const dim3 blk(kBX, kBY);
   const int nb = elementwise_blocks(s);
   // q = A p; alpha = rho_old / (p,q)                             NonUniform.jl:164-176
   launch_ax<T, 1, T>(s, cs, opA, q, p, p, nullptr, st, kStageCgAlpha);
@@ -1726,7 +1726,7 @@ static int precond_t(Solver* s, const double* bb, double* xx, int smoother, cons
   T* xd = static_cast<T*>(ha);
   T* bd = static_cast<T*>(hb);
   if ((rc = upload<T>(s, bb, bd, 1))) return rc;
-  const dim3 rg = rb_grid(s->g), blk(kBX, kBY);
+  const dim3 blk(kBX, kBY);
   const int none = smoother == H2G_SMOOTHER_NONE;
   launch(s, k_rb_first<T, T, 0>, first_grid(s->g), blk, s->stream, op, xd, bd, nullptr, nullptr, nullptr, nullptr, none);
   if (!none)
@@ -1753,7 +1753,7 @@ static int bench_t(Solver* s, int kind, int reps, int* launches, const h2g::OpPa
     CK(cudaStreamSynchronize(s->stream));
     s->hook_filled = true;
   }
-  const dim3 rg = rb_grid(s->g), ag = ax_grid(s->g), blk(kBX, kBY);
+  const dim3 blk(kBX, kBY);
   int n = 0;
   for (int r = 0; r < reps; ++r) {
     if (kind == 0) {
