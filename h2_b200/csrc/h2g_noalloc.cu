@@ -2,10 +2,11 @@
 // memory.
 //
 // Who needs it: a caller whose device memory is owned by someone else -- a Julia program whose
-// arrays live in CUDA.jl's pool, a time-stepping loop that must not stall on cudaMalloc/cudaFree
-// (both can synchronise the device), or code between the steps of a CUDA stream capture, where
-// cudaFree is not allowed.  Such a caller already holds the fields in device memory and only
-// wants the residual r = b - A theta and its norm, without a solver handle (h2g_create allocates).
+// arrays live in CUDA.jl's pool, or a time-stepping loop that must not stall on
+// cudaMalloc/cudaFree (both can synchronise the device).  Such a caller already holds the fields
+// in device memory and only wants the residual r = b - A theta and its norm, without a solver
+// handle (h2g_create allocates).  The call ends by copying ||r|| to the host and synchronising
+// its stream, so it must not be issued while that stream is capturing a CUDA graph.
 //
 // The reduction of ||r|| needs scratch: one partial sum per row (j, k) of the interior, a ticket
 // counter and the result.  They live in g_noalloc_scratch, a file-scope device array: every GPU
@@ -16,7 +17,7 @@
 //     the start of every call, and calls that overlap on the GPU (several host threads, or
 //     several streams) race on it -- serialise them;
 //   * the first call on a device looks up the array's device address (cudaGetSymbolAddress) with
-//     that device current; make that first call before any stream capture.
+//     that device current.
 #include <cuda_runtime.h>
 
 #include <cmath>

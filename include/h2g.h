@@ -242,8 +242,8 @@ int h2g_bench_kernel(h2g_solver *h, int kind, int reps, int *launches);
 /* ---- CalcRK! without device allocation -------------------------------------------------
  * No counterpart in the reference.  For callers that cannot allocate device memory: the device
  * memory belongs to someone else (a Julia program's CUDA.jl pool, a framework's caching
- * allocator), or the caller runs a time-stepping loop that must not stall on cudaMalloc/cudaFree,
- * or it is between steps of a CUDA stream capture, where cudaFree is not allowed.  Computes
+ * allocator), or the caller runs a time-stepping loop that must not stall on cudaMalloc/cudaFree.
+ * Computes
  * r = b - A theta over the interior and *res = ||r||_2 exactly as h2g_calcrk, from the
  * reference's column-major arrays already in device memory (theta, b, lambda, mask, rho, cp: MX*MY*MZ
  * doubles; ZC, dZ: MZ doubles; rho and cp may be NULL when is_steady) and HC[6] on the host;
@@ -251,8 +251,9 @@ int h2g_bench_kernel(h2g_solver *h, int kind, int reps, int *launches);
  * the reduction uses a 512 KiB device array inside the library that every GPU loading it keeps
  * until exit, so grids with more than 65536 interior rows (NY*NZ) are rejected (H2G_BAD_ARG).
  * Calls share that array: calls that overlap on the GPU race and must be serialised.  The first
- * call on a device looks up the array's address; make it before any stream capture.  stream may
- * be NULL (legacy default stream); the call returns after *res is on the host. */
+ * call on a device looks up the array's address.  stream may be NULL (legacy default stream); the
+ * call copies *res to the host and synchronises the stream before it returns, so it must not be
+ * issued while that stream is capturing a CUDA graph. */
 int h2g_calcrk_noalloc(int MX, int MY, int MZ, const double *theta, const double *b, const double *lambda,
                        const double *mask, const double *rho, const double *cp, const double *ZC, const double *dZ,
                        double dx, double dy, double dt, const double *HC, int is_steady, double *r, double *res,

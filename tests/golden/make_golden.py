@@ -1,6 +1,8 @@
 """Generate the golden fixtures of tests/golden/.
 
-  python tests/golden/make_golden.py [--reference /path/to/H2] [--only readme|oracle240|...]
+  python tests/golden/make_golden.py [--reference <checkout of kenoogl/H2>] [--only readme|oracle240|...]
+
+(--reference is needed for the readme job only)
 
 readme_240.json      the sample log of the reference README (README.md:166-183), read as text:
                      the initial residual, the relative residuals printed there, the iteration
@@ -99,9 +101,11 @@ def run_oracle(NX, eps, method="pbicgstab", red=O.RED_SEQ, symmetric=False):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=None, help="checkout of the reference (readme job)")
     ap.add_argument("--only", default="")
     a = ap.parse_args()
+    if a.reference is None and (not a.only or "readme" in a.only.split(",")):
+        ap.error("--reference is required for the readme job (or pick others with --only)")
     O.build()
     jobs = {
         "readme": lambda: ("readme_240.json", parse_readme(os.path.join(a.reference, "README.md"))),

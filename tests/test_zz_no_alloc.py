@@ -1,6 +1,6 @@
 """h2g_calcrk_noalloc: CalcRK! for callers that cannot allocate device memory (their memory
 belongs to a pool such as CUDA.jl's, or they run a loop that must not stall on cudaMalloc /
-cudaFree, or they are between steps of a stream capture).  The entry point allocates nothing; its
+cudaFree).  The entry point allocates nothing; its
 reduction scratch is a fixed array inside the library.  It must return the same residual as the
 handle-based h2g_calcrk, on two calls in a row (the shared scratch keeps the last call's
 contents), and refuse grids larger than its scratch.
