@@ -34,12 +34,6 @@ sys.path.insert(0, ROOT)
 
 METRIC = "PBiCGSTAB time-to-eps (s) + stencil HBM GB/s, mixed vs FP64 GPU at 240^2x30"
 L2_FLUSH_BYTES = 256 << 20
-# DRAM bytes (read + write) of one FP64 RB-GS sweep (two k_rb_pass<double> launches) on the
-# 240x240x30 grid, from one ncu capture of `python -m h2_b200.kernel_bench --kind sweep
-# --precision fp64` (dram__bytes_read.sum 37.46 MB and dram__bytes_write.sum < 1 KB per launch;
-# the pass also reads the precomputed dd and the packed stencil keys of the cells it updates,
-# 13.8 MB, beyond the algorithmic bytes).
-SWEEP_TRAFFIC_F64 = {(240, 30): 2 * 37.463e6}
 
 
 def log(*a):
@@ -64,6 +58,9 @@ def parse():
                     help="1 = also time CG + RB-GS on the symmetric variant (adiabatic instead of convective faces)")
     ap.add_argument("--adjoint-steps", type=int, default=200,
                     help="implicit steps of the timed transient adjoint (0 = skip the adjoint section)")
+    ap.add_argument("--scaling", type=int, default=1,
+                    help="1 = also measure the scaling grids (480^2x60: FP64 and mixed solves and sweep rates; "
+                         "960^2x120: sweep rates)")
     return ap.parse_args()
 
 
@@ -79,6 +76,22 @@ def measured_peaks():
 def workload_name(a):
     return (f"{a.nx}x{a.nx}x{a.nz} Mode-3 IC stack, steady, PBiCGSTAB + RB-GS(5 sweeps), FP64, "
             f"to ||r||/||r0|| <= {a.tol:g}")
+
+
+def bench_config(a):
+    """The workload of one step; identical in both arms."""
+    return {"workload": workload_name(a), "grid": [a.nx, a.nx, a.nz], "tol": a.tol, "smoother": "RB-GS, 5 sweeps",
+            "method": "PBiCGSTAB", "precision": "fp64"}
+
+
+def cpu_model() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
 
 
 # ----------------------------------------------------------------------------------------------
@@ -236,17 +249,157 @@ def run_reference(a, dist: Dist):
         "impl": "reference", "metric": METRIC, "value": value, "unit": "s", "n_gpus": a.gpus, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": 1e3 * float(np.mean(times)), "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (reference Mode-3 model)",
-        "config": {"workload": workload_name(a),
-                   "grid": [a.nx, a.nx, a.nz], "tol": a.tol, "parallelism": "host threads"},
-        "cpu_baseline": {"value": value, "unit": "s", "cores": cb.cores, "kind": "port",
+        "config": bench_config(a),
+        "parallelism": f"host threads x{cb.cores}",
+        "cpu_baseline": {"value": value, "unit": "s", "cores": cb.cores, "kind": "port", "cpu_model": cpu_model(),
+                         "extrapolated": True,
                          "sample": f"{per_step} PBiCGSTAB iterations per step (OpenMP reductions, "
-                                   f"{cb.cores} threads), scaled to the {iters_ref} iterations the FP64 "
-                                   f"solve needs"},
+                                   f"{cb.cores} threads); value = mean time per iteration x the {iters_ref} "
+                                   f"iterations the oracle's FP64 solve needs to reach the tolerance "
+                                   f"(extrapolated from the bounded sample, not a full solve)"},
         "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "seconds_per_iteration": t_iter,
     }
     print(json.dumps(line), flush=True)
     dist.close()
+
+
+def cpu_baseline_leg(a, it64: int) -> dict:
+    """The oracle (the reference's algorithm in C, OpenMP on all host cores) on the same workload:
+    one full FP64 solve to the tolerance when it takes under ~40 s, else a bounded sample of
+    iterations scaled to the GPU solve's iteration count (said so in `sample`)."""
+    cb = CpuBaseline(a.nx, a.nz)
+    t1 = cb.time_iters(2) / 2
+    base = {"unit": "s", "cores": cb.cores, "kind": "port", "cpu_model": cpu_model()}
+    if t1 * it64 <= 40.0:
+        import copy
+        prob = copy.deepcopy(cb.prob0)
+        t = time.perf_counter()
+        conv, itr, _, _ = cb.O.pbicgstab(prob, tol=a.tol, maxItr=20000, smoother="gs", red_mode=cb.O.RED_OMP,
+                                         threads=cb.cores)
+        tcpu = time.perf_counter() - t
+        return {"value": tcpu, **base, "extrapolated": False, "iterations": itr, "converged": bool(conv),
+                "sample": f"one full FP64 PBiCGSTAB+RB-GS solve of the oracle to ||r||/||r0|| <= {a.tol:g} "
+                          f"({itr} iterations, OpenMP reductions, {cb.cores} threads)"}
+    iters = a.cpu_sample_iters or cb.calibrate(target_s=10.0)
+    tcpu = cb.time_iters(iters)
+    return {"value": tcpu / iters * it64, **base, "extrapolated": True,
+            "sample": f"{iters} FP64 PBiCGSTAB+RB-GS iterations of the oracle (OpenMP, {cb.cores} threads) in "
+                      f"{tcpu:.2f} s, scaled to the {it64} iterations of the GPU FP64 solve"}
+
+
+# DRAM bytes (read + write) per launch of the dominant kernel, from one ncu capture each (see the
+# profiles/ summaries): key (nx, nz, fused).
+SWEEP_TRAFFIC_F64 = {(240, 30, False): 37.463e6}
+
+
+def kernel_rates(nx, nz, solvers, torch, stream, flush, reps):
+    """Algorithmic GB/s of one RB-GS sweep (one fused launch or two colour passes, whichever the
+    handle's tuner chose) and of CalcAX, per handle: warm = CUDA events around `reps` back-to-back
+    launches on resident data, as inside a solve; cold = the L2 flushed (256 MiB write) before each
+    single launch.  Algorithmic bytes per cell: sweep 3w + 1 (x read and written, b, one key byte),
+    CalcAX 2*8 + 1 (FP64 in both handles)."""
+    N = nx * nx * nz
+    out = {}
+    for name, s in solvers.items():
+        w_elem = 8 if name == "fp64" else 4
+        fused = bool(s.sweep()[0])
+        for kind, bytes_per_cell, label in ((0, 3 * w_elem + 1, "rb_sweep"), (1, 2 * 8 + 1, "calcax")):
+            cold = []
+            for r in range(reps + 3):
+                with torch.cuda.stream(stream):
+                    flush.zero_()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                s.bench_kernel(kind, 1)
+                e1.record(stream)
+                e1.synchronize()
+                if r >= 3:
+                    cold.append(e0.elapsed_time(e1) * 1e-3)
+            s.bench_kernel(kind, 3)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            s.bench_kernel(kind, reps)
+            e1.record(stream)
+            e1.synchronize()
+            warm = e0.elapsed_time(e1) * 1e-3 / reps
+            tc = float(np.mean(cold))
+            nbytes = bytes_per_cell * N
+            out[(name, label)] = {"seconds": warm, "gbs": nbytes / warm / 1e9, "seconds_cold": tc,
+                                  "gbs_cold": nbytes / tc / 1e9, "bytes": nbytes,
+                                  "launches": (1 if fused else 2) if kind == 0 else 1,
+                                  "fused": fused if kind == 0 else None}
+    return out
+
+
+def roofline_object(rm, peak, peak_kind, nx, nz):
+    fused = bool(rm["fused"])
+    name = ("k_rb_sweep<double>: one fused RB-GS sweep (both colours, TMA-staged z-march) of the FP64 smoother"
+            if fused else "k_rb_pass<double>: one RB-GS sweep (colour 0 then colour 1) of the FP64 smoother")
+    traffic = SWEEP_TRAFFIC_F64.get((nx, nz, fused))
+    return {"bound": "hbm", "achieved": rm["gbs"], "peak": peak, "unit": "GB/s", "frac": rm["gbs"] / peak,
+            "traffic": None if traffic is None else traffic * rm["launches"],
+            "traffic_unit": f"DRAM bytes per sweep ({rm['launches']} launch(es)), ncu, L2 flushed",
+            "kernel": name, "algorithmic_bytes": rm["bytes"], "seconds": rm["seconds"],
+            "timing": "warm: CUDA events around back-to-back sweeps on resident data, as inside the solve "
+                      "(at 240^2x30 the working set is L2-resident)",
+            "cold": {"achieved": rm["gbs_cold"], "frac": rm["gbs_cold"] / peak, "seconds": rm["seconds_cold"],
+                     "timing": "L2 flushed before each launch"},
+            "peak_kind": peak_kind}
+
+
+def run_scaling(a, dist, torch, stream, flush, peak):
+    """The scaling grids of the workload (the reference's stack, Z cells split uniformly): at
+    480x480x60 one FP64 and one mixed solve to a.tol (after one untimed solve each) and the sweep
+    rates; at 960x960x120 the sweep rates.  CUDA events; L2 flushed before each solve."""
+    import h2_b200
+    from h2_b200 import model as M
+
+    out = {}
+    for nx, nz, solve in ((480, 60, True), (960, 120, False)):
+        m = M.build_mode3(nx, nx, nz)
+        w = m.wk
+        solvers, entry = {}, {}
+        try:
+            for name in ("fp64", "mixed"):
+                s = h2_b200.Solver(*m.shape, precision=name, stream=stream.cuda_stream)
+                solvers[name] = s
+                s.set_grid(m.ZC, m.dZ, m.dx, m.dy, m.dt, m.HC, True)
+                s.set_fields(w.lam, w.mask)
+                s.set_rhs(w.b)
+                s.set_theta(w.theta)
+                s.snapshot()
+                if solve:
+                    ts, res = [], None
+                    for r in range(2):
+                        s.snapshot(restore=True)
+                        with torch.cuda.stream(stream):
+                            flush.zero_()
+                        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                        e0.record(stream)
+                        st, res = s.solve("pbicgstab", tol=a.tol, maxItr=20000, smoother="gs")
+                        e1.record(stream)
+                        e1.synchronize()
+                        if r:
+                            ts.append(e0.elapsed_time(e1) * 1e-3)
+                    entry[name] = {"seconds": ts[0], "iterations": res.itr, "status": st,
+                                   "final_rel_residual": res.res, "restarts": res.outer}
+            if solve:
+                th = {k: v.get_theta()[1:-1, 1:-1, 1:-1] for k, v in solvers.items()}
+                entry["mixed"]["max_abs_dtheta_vs_fp64_K"] = float(np.abs(th["mixed"] - th["fp64"]).max())
+            rates = kernel_rates(nx, nz, solvers, torch, stream, flush, 10)
+            for (name, label), v in rates.items():
+                v["frac_cold"] = v["gbs_cold"] / peak
+                v["frac"] = v["gbs"] / peak
+                entry[f"{name}_{label}"] = v
+        except Exception as e:  # pragma: no cover
+            log(f"scaling grid {nx}^2x{nz} failed:", e)
+            entry = {"error": str(e)}
+        finally:
+            for s in solvers.values():
+                s.close()
+        out[f"{nx}x{nx}x{nz}"] = entry
+    return out
 
 
 # ----------------------------------------------------------------------------------------------
@@ -330,27 +483,9 @@ def run_ours(a, dist: Dist):
                   "reference_published": {"seconds": 183.0, "iterations": 208, "hardware": "not stated",
                                           "source": "the reference's README.md:174-182 (Julia; compute time of this solve)"}}
 
-    # ---- roofline of the dominant kernel: one RB-GS sweep (2 launches of the colour pass)
+    # ---- roofline of the dominant kernel: one RB-GS sweep (one fused launch, or two colour passes)
     peak, peak_kind = measured_peaks()
-    N = a.nx * a.nx * a.nz
-    roof = {}
-    # the mixed handle sweeps in FP32 (its preconditioner) and applies CalcAX in FP64 (its Krylov solver)
-    for name, w_elem in (("mixed", 4), ("fp64", 8)):
-        s = solvers[name]
-        for kind, bytes_per_cell, label in ((0, 3 * w_elem + 1, "rb_sweep"), (1, 2 * 8 + 1, "calcax")):
-            ts = []
-            for r in range(a.kernel_reps + 3):
-                with torch.cuda.stream(stream):
-                    flush.zero_()
-                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                e0.record(stream)
-                s.bench_kernel(kind, 1)
-                e1.record(stream)
-                e1.synchronize()
-                if r >= 3:
-                    ts.append(e0.elapsed_time(e1) * 1e-3)
-            tk = float(np.mean(ts))
-            roof[(name, label)] = dict(seconds=tk, bytes=bytes_per_cell * N, gbs=bytes_per_cell * N / tk / 1e9)
+    roof = kernel_rates(a.nx, a.nz, solvers, torch, stream, flush, a.kernel_reps)
 
     # ---- end to end through the public drop-in call with pinned host buffers
     e2e, e2e_local = None, float("nan")
@@ -399,17 +534,12 @@ def run_ours(a, dist: Dist):
     cpu = None
     if dist.rank == 0 and dist.world == 1 and not a.no_cpu_baseline:
         try:
-            cb = CpuBaseline(a.nx, a.nz)
-            iters = a.cpu_sample_iters or cb.calibrate(target_s=10.0)
-            tcpu = cb.time_iters(iters)
-            it64 = results["fp64"]["res"].itr
-            cpu = {"value": tcpu / iters * it64, "unit": "s", "cores": cb.cores, "kind": "port",
-                   "sample": f"{iters} FP64 PBiCGSTAB+RB-GS iterations of the oracle (OpenMP, {cb.cores} threads) "
-                             f"in {tcpu:.2f} s, scaled to the {it64} iterations of the FP64 solve"}
+            cpu = cpu_baseline_leg(a, results["fp64"]["res"].itr)
         except Exception as e:  # pragma: no cover
             log("cpu baseline failed:", e)
 
     rm = roof[("fp64", "rb_sweep")]
+    scaling = run_scaling(a, dist, torch, stream, flush, peak) if a.scaling else None
     f64, mx = results["fp64"], results["mixed"]
     out = {
         "metric": METRIC,
@@ -425,22 +555,19 @@ def run_ours(a, dist: Dist):
         "dtype": "f64",
         "data": "synthetic: the reference's Mode-3 IC-stack model (GPU fillID!, heat source 1.6e11 W/m^3 "
                 "on the power grids), theta_init = 300 K",
-        "config": {"workload": workload_name(a), "grid": [a.nx, a.nx, a.nz], "tol": a.tol,
-                   "smoother": "RB-GS, 5 sweeps",
-                   "l2": "flushed (256 MiB write) before every timed solve and kernel launch",
-                   "parallelism": f"replicas x{dist.world}" if dist.world > 1 else "single GPU"},
+        "config": bench_config(a),
+        "l2": "flushed (256 MiB write) before every timed solve; kernels timed warm (back to back, as inside "
+              "the solve) and cold (L2 flushed before each launch)",
+        "parallelism": f"replicas x{dist.world}" if dist.world > 1 else "single GPU",
         "fp64": {"seconds": f64["t"], "iterations": f64["res"].itr, "final_rel_residual": f64["res"].res},
         "mixed": {"seconds": mx["t"], "iterations": mx["res"].itr, "restarts": mx["res"].outer,
                   "final_rel_residual": mx["res"].res, "max_abs_dtheta_vs_fp64_K": max_dtheta,
                   "precision": "FP32 RB-GS preconditioner (tables, smoother vectors); FP64 Krylov vectors, "
                                "inner products, CalcAX and solution"},
         "speedup_mixed_vs_fp64": f64["t"] / mx["t"],
-        "roofline": {"bound": "hbm", "achieved": rm["gbs"], "peak": peak, "unit": "GB/s",
-                     "frac": rm["gbs"] / peak, "traffic": SWEEP_TRAFFIC_F64.get((a.nx, a.nz)),
-                     "traffic_unit": "bytes per sweep (2 launches), ncu",
-                     "kernel": "k_rb_pass<double>: one RB-GS sweep (colour 0 then colour 1) of the FP64 smoother",
-                     "algorithmic_bytes": rm["bytes"], "seconds": rm["seconds"], "peak_kind": peak_kind},
+        "roofline": roofline_object(rm, peak, peak_kind, a.nx, a.nz),
         "kernels": {f"{k[0]}_{k[1]}": v for k, v in roof.items()},
+        "scaling_configs": scaling,
         "readme_case": readme,
         "cg_symmetric": cg_sym,
         "batch": batch,

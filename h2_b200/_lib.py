@@ -84,6 +84,9 @@ _SIGS = {
                                         C.c_int, _dp, _dp, _dp, C.POINTER(Result)]),
     "h2g_autotune": (C.c_int, [_vp, _ip, _ip, _ip, _ip]),
     "h2g_set_tuning": (C.c_int, [_vp, C.c_int, C.c_int]),
+    "h2g_set_sweep": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int]),
+    "h2g_get_sweep": (C.c_int, [_vp, _ip, _ip, _ip]),
+    "h2g_set_wait_limit": (C.c_int, [_vp, C.c_longlong]),
     "h2g_release_cached": (C.c_int, []),
     "h2g_calcax": (C.c_int, [_vp, _dp, _dp]),
     "h2g_calcrk": (C.c_int, [_vp, _dp, _dp]),

@@ -54,7 +54,13 @@ inline Geo make_geo(int MX, int MY, int MZ) {
 }
 
 // Why a solve stopped (SolverState::reason).
-enum Reason { kRunning = 0, kConverged = 1, kBreakdown = 2, kMaxItr = 3, kNonFinite = 4 };
+enum Reason { kRunning = 0, kConverged = 1, kBreakdown = 2, kMaxItr = 3, kNonFinite = 4, kTimeout = 5 };
+
+// Bounded device waits (TMA completion barriers of the fused sweep): the default budget of one
+// wait and the budget of the drain of copies still in flight after a wait ran out, in SM clock
+// cycles (about one second each at 1.965 GHz).
+constexpr long long kWaitCycles = 2000000000LL;
+constexpr long long kDrainCycles = 2000000000LL;
 
 // Finisher stages: what the last block of a reducing kernel does with the reduced sums.
 enum Stage {

@@ -7,6 +7,7 @@
 // and the last kernel of the body sets the loop condition, so the host does not synchronise
 // between iterations.
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <array>
@@ -25,7 +26,7 @@
 #include <vector>
 
 #include "../../include/h2g.h"
-#include "h2g_kernels.cuh"
+#include "h2g_sweep.cuh"
 
 namespace h2g {
 
@@ -131,8 +132,9 @@ struct Solver {
   size_t tstates_cap = 0;      // in vectors
   // Krylov vectors in working precision: r, r0, p, ph, q, s, sh, t (+ e for refinement)
   void* kv[10] = {nullptr};
-  void* hook[2] = {nullptr, nullptr};  // scratch of the single-kernel entry points (never a Krylov vector)
+  void* hook[3] = {nullptr, nullptr, nullptr};  // scratch of the single-kernel entry points (never a Krylov vector)
   bool hook_filled = false;            // hook[] holds the benchmark's non-zero scratch values
+  unsigned bench_parity = 0;           // direction of the next fused benchmark sweep
   size_t elem = 8;
   // column-major staging buffers (MX*MY*MZ doubles each)
   double* stage[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -155,6 +157,19 @@ struct Solver {
   bool rb_dd = true;      // colour pass reads dd from the per-cell array (autotuned)
   bool ax_dd = false;     // CalcAX reads dd from the per-cell array (autotuned)
   bool rb_tuned = false;  // rb_rows chosen (by the tuner or h2g_set_tuning)
+  // fused sweeps (k_rb_sweep): sweeps 2-5 of the preconditioner as one launch each, ping-ponging
+  // between the preconditioner's output and x2 (one per precision; guards zero, never written)
+  bool rb_fused = false;   // autotuned
+  int sw_chunks = 1;       // z chunks of the fused sweep's grid (autotuned)
+  bool sw_dda = false;     // the fused sweep reads dd from the array (autotuned)
+  int sweep_forced = -1;   // h2g_set_sweep: -1 tuner, 0 colour passes, 1 fused
+  double* x2_64 = nullptr;
+  float* x2_32 = nullptr;
+  int* sweep_err = nullptr;            // set by a fused sweep whose bounded wait ran out
+  long long wait_limit = kWaitCycles;  // budget of one bounded wait (clock cycles)
+  std::map<std::pair<const void*, int>, CUtensorMap> xmaps;  // TMA maps of x buffers (pointer, bytes/element)
+  CUtensorMap kmap;                    // TMA map of the key array
+  bool kmap_ok = false;
 
   long long nfort() const { return (long long)g.MX * g.MY * g.MZ; }
 };
@@ -243,6 +258,148 @@ static void launch_rb(const Solver* s, cudaStream_t cs, const OpParams<T>& op, T
   else launch_rb_dd<T, false>(s, cs, op, x, bb, color, omega, st);
 }
 
+// ---- fused sweep (k_rb_sweep) ---------------------------------------------------------------
+// cuTensorMapEncodeTiled from the driver, looked up through the runtime (the library does not
+// link libcuda itself).
+static PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+static std::once_flag g_encode_once;
+
+static int tensor_encoder() {
+  std::call_once(g_encode_once, [] {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    cudaGetLastError();
+  });
+  return g_encode ? H2G_OK : fail(H2G_CUDA_ERROR, "cuTensorMapEncodeTiled is not available");
+}
+
+// 3-D map over a device-layout vector: (positions HP, half-rows 2*MY, planes MZ); the box is one
+// staged plane of k_rb_sweep.  Out-of-range coordinates read as zero.
+static int encode_map(const Solver* s, const void* base, int esize, CUtensorMap* m) {
+  if (int rc = tensor_encoder()) return rc;
+  const Geo& g = s->g;
+  const cuuint64_t dims[3] = {(cuuint64_t)g.HP, (cuuint64_t)(2 * g.MY), (cuuint64_t)g.MZ};
+  const cuuint64_t strides[2] = {(cuuint64_t)g.HP * esize, (cuuint64_t)(2 * g.MY) * g.HP * esize};
+  const cuuint32_t box[3] = {(cuuint32_t)(esize == 8 ? SwCfg<double>::WX : esize == 4 ? SwCfg<float>::WX : kSwWK),
+                             (cuuint32_t)kSwRR, 1u};
+  const cuuint32_t es[3] = {1u, 1u, 1u};
+  const CUtensorMapDataType dt = esize == 8   ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64
+                                 : esize == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+                                              : CU_TENSOR_MAP_DATA_TYPE_UINT8;
+  const CUresult r = g_encode(m, dt, 3, const_cast<void*>(base), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(H2G_CUDA_ERROR, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+  return H2G_OK;
+}
+
+template <typename T>
+static int xmap(Solver* s, const T* base, const CUtensorMap** out) {
+  const auto key = std::make_pair((const void*)base, (int)sizeof(T));
+  auto it = s->xmaps.find(key);
+  if (it == s->xmaps.end()) {
+    CUtensorMap m;
+    if (int rc = encode_map(s, base, (int)sizeof(T), &m)) return rc;
+    it = s->xmaps.emplace(key, m).first;
+  }
+  *out = &it->second;
+  return H2G_OK;
+}
+
+static int kmap(Solver* s, const CUtensorMap** out) {
+  if (!s->kmap_ok) {
+    if (int rc = encode_map(s, s->key, 1, &s->kmap)) return rc;
+    s->kmap_ok = true;
+  }
+  *out = &s->kmap;
+  return H2G_OK;
+}
+
+// the fused sweep's dynamic shared memory (above the 48 KiB default), once per process
+static int sweep_attrs() {
+  static std::once_flag once;
+  static cudaError_t e = cudaSuccess;
+  std::call_once(once, [] {
+    cudaError_t r[4] = {
+        cudaFuncSetAttribute(k_rb_sweep<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, SwCfg<double>::SMEM),
+        cudaFuncSetAttribute(k_rb_sweep<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SwCfg<double>::SMEM),
+        cudaFuncSetAttribute(k_rb_sweep<float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, SwCfg<float>::SMEM),
+        cudaFuncSetAttribute(k_rb_sweep<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SwCfg<float>::SMEM)};
+    for (cudaError_t x : r)
+      if (x != cudaSuccess) e = x;
+  });
+  if (e != cudaSuccess) return fail(H2G_CUDA_ERROR, "fused sweep attributes: %s", cudaGetErrorString(e));
+  return H2G_OK;
+}
+
+static dim3 sweep_grid(const Geo& g, int chunks) {
+  const int kc = (g.NZ + chunks - 1) / chunks;
+  return dim3((g.HI + kSwTPX - 3) / (kSwTPX - 2), (g.NY + kSwTJ - 3) / (kSwTJ - 2), (g.NZ + kc - 1) / kc);
+}
+
+// One fused RB-GS sweep xout <- sweep(xin) with right-hand side bb.  The tensor maps are encoded
+// on the host when a buffer is first seen (also during stream capture: no stream work).
+template <typename T>
+static int launch_sweep(Solver* s, cudaStream_t cs, const OpParams<T>& op, const T* xin, T* xout, const T* bb,
+                        SolverState* st) {
+  const CUtensorMap *mx = nullptr, *mk = nullptr;
+  if (int rc = xmap<T>(s, xin, &mx)) return rc;
+  if (int rc = kmap(s, &mk)) return rc;
+  const Geo& g = op.g;
+  const int kc = (g.NZ + s->sw_chunks - 1) / s->sw_chunks;
+  const dim3 grid = sweep_grid(g, s->sw_chunks), blk(kSwTPX, kSwTJ);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = blk;
+  cfg.dynamicSmemBytes = SwCfg<T>::SMEM;
+  cfg.stream = cs;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = s->pdl ? 1 : 0;
+  if (s->sw_dda)
+    cudaLaunchKernelEx(&cfg, k_rb_sweep<T, true>, op, *mx, *mk, xout, bb, kc, st, s->sweep_err, s->wait_limit);
+  else
+    cudaLaunchKernelEx(&cfg, k_rb_sweep<T, false>, op, *mx, *mk, xout, bb, kc, st, s->sweep_err, s->wait_limit);
+  return H2G_OK;
+}
+
+// H2G_TIMEOUT (and the flag cleared) if a fused sweep's bounded wait ran out since the last check.
+static int sweep_status(Solver* s) {
+  int e = 0;
+  CK(cudaMemcpy(&e, s->sweep_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (!e) return H2G_OK;
+  CK(cudaMemset(s->sweep_err, 0, sizeof(int)));
+  return fail(H2G_TIMEOUT, "a bounded wait of the fused RB-GS sweep ran out");
+}
+
+template <typename T>
+static T* x2buf(Solver* s);
+template <>
+double* x2buf<double>(Solver* s) { return s->x2_64; }
+template <>
+float* x2buf<float>(Solver* s) { return s->x2_32; }
+
+// Preconditioner! after its first colour pass (k_rb_first wrote xx): colour 1 of sweep 1, then
+// sweeps 2..5, either as colour passes in place or as fused sweeps xx -> x2 -> xx -> x2 -> xx.
+template <typename T>
+static int launch_precond_tail(Solver* s, cudaStream_t cs, const OpParams<T>& op, T* xx, const T* bb,
+                               SolverState* st) {
+  launch_rb<T>(s, cs, op, xx, bb, 1, T(1), st);
+  if (s->rb_fused) {
+    T* x2 = x2buf<T>(s);
+    for (int sw = 1; sw < kSweeps; ++sw)
+      if (int rc = launch_sweep<T>(s, cs, op, (sw & 1) ? xx : x2, (sw & 1) ? x2 : xx, bb, st)) return rc;
+  } else {
+    for (int pass = 2; pass < 2 * kSweeps; ++pass) launch_rb<T>(s, cs, op, xx, bb, pass & 1, T(1), st);
+  }
+  return H2G_OK;
+}
+
 static size_t partials_needed(const Solver* s) {
   dim3 a = ax_grid(s->g);
   size_t nb = (size_t)a.x * a.y * a.z;
@@ -325,6 +482,7 @@ static void destroy(Solver* s) {
   for (auto& p : s->kv) cudaFree(p);
   for (auto& p : s->hook) cudaFree(p);
   for (auto& p : s->stage) cudaFree(p);
+  cudaFree(s->x2_64); cudaFree(s->x2_32); cudaFree(s->sweep_err);
   cudaFree(s->st); cudaFree(s->st_in); cudaFree(s->partials); cudaFree(s->hist);
   if (s->st_host) cudaFreeHost(s->st_host);
   if (s->cap) cudaStreamDestroy(s->cap);
@@ -472,8 +630,8 @@ static int build_tables(Solver* s) {
 // CalcAX (opA); TP: the preconditioner's precision (opM) and of its outputs p_, s_ (z for CG).
 // With TP != T the first pass also writes the smoother's copy of its right-hand side (bb32).
 template <typename T, typename TX, typename TP>
-static void launch_pbicg_body(Solver* s, cudaStream_t cs, const OpParams<T>& opA, const OpParams<TP>& opM, TX* x,
-                              SolverState* st, int smoother, cudaGraphConditionalHandle hc, int use_cond) {
+static int launch_pbicg_body(Solver* s, cudaStream_t cs, const OpParams<T>& opA, const OpParams<TP>& opM, TX* x,
+                             SolverState* st, int smoother, cudaGraphConditionalHandle hc, int use_cond) {
   const Geo& g = s->g;
   T* r = kvec<T>(s, KR);
   T* r0 = kvec<T>(s, KR0);
@@ -489,15 +647,13 @@ static void launch_pbicg_body(Solver* s, cudaStream_t cs, const OpParams<T>& opA
   // p = r + beta (p - omega q); p_ = M^-1 p                     NonUniform.jl:296-305
   launch(s, k_rb_first<TP, T, 1>, first_grid(g), blk, cs, opM, ph, p, bbm, r, q, st, none);
   if (!none)
-    for (int pass = 1; pass < 2 * kSweeps; ++pass)
-      launch_rb<TP>(s, cs, opM, ph, bbm ? bbm : reinterpret_cast<TP*>(p), pass & 1, TP(1), st);
+    if (int rc = launch_precond_tail<TP>(s, cs, opM, ph, bbm ? bbm : reinterpret_cast<TP*>(p), st)) return rc;
   // q = A p_;  alpha = rho / (q, r0)                            NonUniform.jl:307-309
   launch_ax<T, 1, TP>(s, cs, opA, q, ph, r0, nullptr, st, kStageAlpha);
   // s = r - alpha q; s_ = M^-1 s                                NonUniform.jl:310-315
   launch(s, k_rb_first<TP, T, 2>, first_grid(g), blk, cs, opM, sh, sv, bbm, r, q, st, none);
   if (!none)
-    for (int pass = 1; pass < 2 * kSweeps; ++pass)
-      launch_rb<TP>(s, cs, opM, sh, bbm ? bbm : reinterpret_cast<TP*>(sv), pass & 1, TP(1), st);
+    if (int rc = launch_precond_tail<TP>(s, cs, opM, sh, bbm ? bbm : reinterpret_cast<TP*>(sv), st)) return rc;
   // t = A s_; omega = (t,s)/(t,t)                               NonUniform.jl:317-326
   launch_ax<T, 2, TP>(s, cs, opA, t, sh, nullptr, sv, st, kStageOmega);
   // x += alpha p_ + omega s_; r = s - omega t; res; next rho    NonUniform.jl:328-346
@@ -507,25 +663,25 @@ static void launch_pbicg_body(Solver* s, cudaStream_t cs, const OpParams<T>& opA
   else
     launch(s, k_bicg_update<T, TX, TP, false>, elementwise_blocks(s), 256, cs, g.n, x, ph, sh, r, sv, t, r0, st,
            s->partials, hc, use_cond);
+  return H2G_OK;
 }
 
 // z = M^-1 r with the first pass reading r (VM 0) and, for TP != T, writing bb32
 template <typename T, typename TP>
-static void launch_precond_r(Solver* s, cudaStream_t cs, const OpParams<TP>& opM, TP* z, T* r, SolverState* st,
-                             int smoother) {
+static int launch_precond_r(Solver* s, cudaStream_t cs, const OpParams<TP>& opM, TP* z, T* r, SolverState* st,
+                            int smoother) {
   const Geo& g = s->g;
   const dim3 blk(kBX, kBY);
   const int none = smoother == H2G_SMOOTHER_NONE;
   TP* bbm = std::is_same<T, TP>::value ? nullptr : kvec<TP>(s, KBB);
   launch(s, k_rb_first<TP, T, 0>, first_grid(g), blk, cs, opM, z, r, bbm, nullptr, nullptr, st, none);
-  if (!none)
-    for (int pass = 1; pass < 2 * kSweeps; ++pass)
-      launch_rb<TP>(s, cs, opM, z, bbm ? bbm : reinterpret_cast<TP*>(r), pass & 1, TP(1), st);
+  if (!none) return launch_precond_tail<TP>(s, cs, opM, z, bbm ? bbm : reinterpret_cast<TP*>(r), st);
+  return H2G_OK;
 }
 
 template <typename T, typename TX, typename TP>
-static void launch_cg_body(Solver* s, cudaStream_t cs, const OpParams<T>& opA, const OpParams<TP>& opM, TX* x,
-                           SolverState* st, int smoother, cudaGraphConditionalHandle hc, int use_cond) {
+static int launch_cg_body(Solver* s, cudaStream_t cs, const OpParams<T>& opA, const OpParams<TP>& opM, TX* x,
+                          SolverState* st, int smoother, cudaGraphConditionalHandle hc, int use_cond) {
   const Geo& g = s->g;
   T* r = kvec<T>(s, KR);
   T* p = kvec<T>(s, KP);
@@ -538,12 +694,13 @@ static void launch_cg_body(Solver* s, cudaStream_t cs, const OpParams<T>& opA, c
   // x += alpha p; r -= alpha q; res                              NonUniform.jl:179-198
   launch(s, k_cg_update<T, TX>, nb, 256, cs, g.n, x, p, r, q, st, s->partials);
   // z = M^-1 r                                                  NonUniform.jl:201-203
-  launch_precond_r<T, TP>(s, cs, opM, z, r, st, smoother);
+  if (int rc = launch_precond_r<T, TP>(s, cs, opM, z, r, st, smoother)) return rc;
   // rho_new = (r,z); beta                                       NonUniform.jl:206-215
   launch(s, k_dot<T, TP>, nb, 256, cs, g.n, r, z, nullptr, st, s->partials, kStageCgBeta);
   // p = z + beta p                                              NonUniform.jl:218-220
   if (use_cond) launch(s, k_cg_pupd<T, TP, true>, nb, 256, cs, g.n, p, z, st, hc, use_cond);
   else launch(s, k_cg_pupd<T, TP, false>, nb, 256, cs, g.n, p, z, st, hc, use_cond);
+  return H2G_OK;
 }
 
 template <typename T, typename TP>
@@ -622,17 +779,20 @@ static int get_graph(Solver* s, int kind, int smoother, const OpParams<T>& op, c
     return H2G_OK;
   }
   const bool cg = (kind == kGCg64 || kind == kGCg32 || kind == kGCgMx);
+  int berr = H2G_OK;
   int rc = make_loop_graph(s, G, [&](cudaStream_t cs, cudaGraphConditionalHandle hc, int use_cond) {
     // kUnroll iterations per WHILE-body pass: the device re-evaluates the loop condition
     // kUnroll times less often.  Every kernel returns at once when the state says stop, and the
     // last update kernel of the body sets the condition, so an iteration that converges in the
     // middle of a pass only leaves the rest of the pass as empty launches.
-    for (int u = 0; u < kUnroll; ++u) {
-      if (cg) launch_cg_body<T, TX, TP>(s, cs, op, opM, x, st, smoother, hc, use_cond);
-      else launch_pbicg_body<T, TX, TP>(s, cs, op, opM, x, st, smoother, hc, use_cond);
+    for (int u = 0; u < kUnroll && berr == H2G_OK; ++u) {
+      if (cg) berr = launch_cg_body<T, TX, TP>(s, cs, op, opM, x, st, smoother, hc, use_cond);
+      else berr = launch_pbicg_body<T, TX, TP>(s, cs, op, opM, x, st, smoother, hc, use_cond);
     }
   });
+  if (rc == H2G_OK && berr != H2G_OK) G.reset();
   if (rc) return rc;
+  if (berr) return berr;
   G.sig = sig;
   *out = &G;
   return H2G_OK;
@@ -679,6 +839,7 @@ static int status_of(const SolverState& st) {
     case kConverged: return H2G_OK;
     case kBreakdown: return H2G_BREAKDOWN;
     case kNonFinite: return H2G_NONFINITE;
+    case kTimeout: return H2G_TIMEOUT;
     default: return H2G_NOT_CONVERGED;
   }
 }
@@ -716,9 +877,16 @@ static void print_log(const SolverState& st, const double* hist, int nhist, int 
   fflush(stdout);
 }
 
+// Kernels of one preconditioner call: the first pass, then 9 colour passes or 1 colour pass and
+// 4 fused sweeps.
+static int precond_kernels(const Solver* s, int smoother) {
+  if (smoother == H2G_SMOOTHER_NONE) return 1;
+  return s->rb_fused ? 2 + (kSweeps - 1) : 2 * kSweeps;
+}
+
 // Kernels in one WHILE-body pass (one Krylov iteration).
-static long long body_kernels(bool cg, int smoother) {
-  const int pc = smoother == H2G_SMOOTHER_NONE ? 1 : 2 * kSweeps;  // passes per preconditioner call
+static long long body_kernels(const Solver* s, bool cg, int smoother) {
+  const int pc = precond_kernels(s, smoother);
   return cg ? (1 + 1 + pc + 1 + 1) : (2 * pc + 2 + 1);
 }
 
@@ -744,7 +912,7 @@ static int solve_krylov(Solver* s, bool cg, double tol, int maxItr, int smoother
   if (cg) {
     // z = M^-1 r; p = z; rho_old = (r,z)                          NonUniform.jl:147-155
     TP* z = kvec<TP>(s, KPH);
-    launch_precond_r<double, TP>(s, s->stream, opM, z, r, st, smoother);
+    if ((rc = launch_precond_r<double, TP>(s, s->stream, opM, z, r, st, smoother))) return rc;
     launch(s, k_dot<double, TP>, elementwise_blocks(s), 256, s->stream, g.n, r, z, kvec<double>(s, KP), st, s->partials,
                                                                      kStageCgInit);
     CKL();
@@ -768,8 +936,8 @@ static int solve_krylov(Solver* s, bool cg, double tol, int maxItr, int smoother
   const int nprint = (fin.reason == kBreakdown || fin.reason == kNonFinite) ? std::min(nh, std::max(0, fin.itr - 1)) : nh;
   if (verbose) print_log(fin, hh.data(), nprint, fin.converged);
   if (out) {
-    const long long body = body_kernels(cg, smoother);
-    const long long pre = 2 + (cg ? (smoother == H2G_SMOOTHER_NONE ? 2 : 2 * kSweeps + 1) : 0);
+    const long long body = body_kernels(s, cg, smoother);
+    const long long pre = 2 + (cg ? precond_kernels(s, smoother) + 1 : 0);
     out->launches = pre + body * std::max(1, fin.itr);
     out->isconverged = fin.converged;
     out->itr = fin.itr;
@@ -827,7 +995,7 @@ static int solve_ir(Solver* s, bool cg, double tol, int maxItr, int smoother, in
       CKL();
       if (cg) {
         float* z = kvec<float>(s, KPH);
-        launch_precond_r<float, float>(s, s->stream, op32, z, kvec<float>(s, KR), si, smoother);
+        if ((rc = launch_precond_r<float, float>(s, s->stream, op32, z, kvec<float>(s, KR), si, smoother))) return rc;
         launch(s, k_dot<float>, nb, 256, s->stream, g.n, kvec<float>(s, KR), z, kvec<float>(s, KP), si, s->partials,
                                                  kStageCgInit);
         CKL();
@@ -843,6 +1011,10 @@ static int solve_ir(Solver* s, bool cg, double tol, int maxItr, int smoother, in
       CK(cudaMemcpyAsync(s->st_host, si, sizeof(SolverState), cudaMemcpyDeviceToHost, s->stream));
       CK(cudaStreamSynchronize(s->stream));
       inner = *s->st_host;
+      if (inner.reason == kTimeout) {
+        status = H2G_TIMEOUT;
+        break;
+      }
       CK(cudaMemcpyAsync(s->st_host, st, sizeof(SolverState), cudaMemcpyDeviceToHost, s->stream));
       CK(cudaStreamSynchronize(s->stream));
       const double new_scale = s->st_host->scale;
@@ -873,8 +1045,8 @@ static int solve_ir(Solver* s, bool cg, double tol, int maxItr, int smoother, in
     print_log(fake, hist_all.data(), (int)std::min<size_t>(hist_all.size(), (size_t)maxItr), converged);
   }
   if (out) {
-    const long long body = body_kernels(cg, smoother);
-    const long long pre_inner = 2 + (cg ? (smoother == H2G_SMOOTHER_NONE ? 2 : 2 * kSweeps + 1) : 0);
+    const long long body = body_kernels(s, cg, smoother);
+    const long long pre_inner = 2 + (cg ? precond_kernels(s, smoother) + 1 : 0);
     out->launches = 2 + (long long)outer * (pre_inner + 2) + body * std::max(total, outer);
     out->isconverged = converged;
     out->itr = total;
@@ -919,7 +1091,7 @@ static int solve_mixed(Solver* s, bool cg, double tol, int maxItr, int smoother,
     memset(&r, 0, sizeof r);
     const int st = solve_krylov<float>(s, cg, tol_cur, maxItr - total, smoother, verbose && restart == 0,
                                        res_hist ? res_hist + total : nullptr, &r);
-    if (st == H2G_BAD_ARG || st == H2G_CUDA_ERROR) return st;
+    if (st == H2G_BAD_ARG || st == H2G_CUDA_ERROR || st == H2G_TIMEOUT) return st;
     ++passes;
     launches += r.launches + 3;
     total += r.itr;
@@ -954,7 +1126,7 @@ static int solve_mixed(Solver* s, bool cg, double tol, int maxItr, int smoother,
       memset(&r, 0, sizeof r);
       const int st = solve_krylov<double>(s, cg, tol / res, maxItr - total, smoother, 0,
                                           res_hist ? res_hist + total : nullptr, &r);
-      if (st == H2G_BAD_ARG || st == H2G_CUDA_ERROR) return st;
+      if (st == H2G_BAD_ARG || st == H2G_CUDA_ERROR || st == H2G_TIMEOUT) return st;
       ++passes;
       launches += r.launches + 1;
       total += r.itr;
@@ -992,9 +1164,21 @@ static int solve(Solver* s, bool cg, double tol, int maxItr, int smoother, int v
   if (!(tol >= 0.0) || !std::isfinite(tol)) return fail(H2G_BAD_ARG, "bad tolerance");
   CK(cudaSetDevice(s->device));
   if (int rc = autotune(s)) return rc;
-  if (s->precision == H2G_MIXED_IR) return solve_ir(s, cg, tol, maxItr, smoother, verbose, res_hist, out);
-  if (s->precision == H2G_MIXED) return solve_mixed(s, cg, tol, maxItr, smoother, verbose, res_hist, out);
-  return solve_krylov<double>(s, cg, tol, maxItr, smoother, verbose, res_hist, out);
+  int rc;
+  if (s->precision == H2G_MIXED_IR) rc = solve_ir(s, cg, tol, maxItr, smoother, verbose, res_hist, out);
+  else if (s->precision == H2G_MIXED) rc = solve_mixed(s, cg, tol, maxItr, smoother, verbose, res_hist, out);
+  else rc = solve_krylov<double>(s, cg, tol, maxItr, smoother, verbose, res_hist, out);
+  if (rc == H2G_BAD_ARG || rc == H2G_CUDA_ERROR) return rc;
+  // a fused sweep whose bounded wait ran out stopped the solve: report it as such
+  const int e = sweep_status(s);
+  if (e != H2G_OK) {
+    if (out) {
+      out->status = e;
+      out->isconverged = 0;
+    }
+    return e;
+  }
+  return rc;
 }
 
 // ------------------------------------------------------------------------------------------
@@ -1121,7 +1305,7 @@ static int transient(Solver* s, const FaceBC& f, int nt, int method, double tol,
     int rc = calrhs(s, f, 1);
     if (rc) return rc;
     const int st = solve(s, method == 1, tol, maxItr, smoother, verbose, nullptr, &r);
-    if (st == H2G_BAD_ARG || st == H2G_CUDA_ERROR) return st;
+    if (st == H2G_BAD_ARG || st == H2G_CUDA_ERROR || st == H2G_TIMEOUT) return st;
     k_theta_stats1<<<nb1, 256, 0, s->stream>>>(s->g, s->th, part);
     k_theta_stats2<<<1, 32, 0, s->stream>>>(part, nb1, s->stats + 3 * (size_t)step);
     CKL();
@@ -1342,7 +1526,7 @@ static int adjoint_transient(Solver* s, const FaceBC& f, int nt, const double* w
 // H2G_RB_PLANES, H2G_RB_DD and H2G_AX_DD in the environment force them (all four: no timing; a
 // forced rows, planes or dd source also restricts the timed variants to it).
 static std::mutex g_tune_mu;
-static std::map<std::array<int, 4>, int> g_tune_cache;
+static std::map<std::array<int, 11>, int> g_tune_cache;
 
 static bool valid_rows(int r) {
   for (int q : kRbRows)
@@ -1353,7 +1537,8 @@ static bool valid_rows(int r) {
 // only_rows / only_np / only_dd: -1 = time every value, else only that one (forced by the
 // environment)
 template <typename T>
-static int tune_rows_t(Solver* s, const OpParams<T>& op, int only_rows, int only_np, int only_dd, int* best_rows) {
+static int tune_rows_t(Solver* s, const OpParams<T>& op, int only_rows, int only_np, int only_dd, int* best_rows,
+                       float* best_ms) {
   const size_t n = (size_t)s->g.n, bytes = sizeof(double) * n;
   for (auto& p : s->hook)
     if (!p) CK(cudaMalloc(&p, bytes));
@@ -1414,11 +1599,91 @@ static int tune_rows_t(Solver* s, const OpParams<T>& op, int only_rows, int only
     }
   }
   if (best == 1e30f) *best_rows = kBY | (2 << 5) | (1 << 8);  // nothing timed: the defaults
+  *best_ms = best;
   s->rb_rows = saved;
   s->rb_planes = saved_np;
   s->rb_dd = saved_dd;
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  return rc;
+}
+
+// Chunk counts along z worth timing for the fused sweep: each distinct planes-per-chunk value with
+// at least 3 planes per chunk and at most 16 blocks per SM in all.
+static std::vector<int> sweep_chunk_candidates(const Solver* s) {
+  const dim3 g1 = sweep_grid(s->g, 1);
+  const long long tiles = (long long)g1.x * g1.y;
+  std::vector<int> out;
+  int last_kc = -1;
+  for (int c : {1, 2, 3, 4, 5, 6, 8, 10, 12, 16}) {
+    const int kc = (s->g.NZ + c - 1) / c;
+    if (kc == last_kc || (kc < 3 && c > 1) || tiles * c > 16LL * s->num_sms) continue;
+    out.push_back(c);
+    last_kc = kc;
+  }
+  if (out.empty()) out.push_back(1);
+  return out;
+}
+
+// Fused sweep against the colour passes: times 10 fused sweeps (x ping-ponging between two
+// scratch vectors) per (chunk count, dd source) and keeps the fastest if it beats unfused_ms, the
+// best 10 unfused sweeps.  *choice: bit 0 fused, bit 1 dd read, bits 2-9 chunk count.
+// only_fused / only_chunks / only_dda: -1 = free, else forced by the environment.
+template <typename T>
+static int tune_sweep_t(Solver* s, const OpParams<T>& op, float unfused_ms, int only_fused, int only_chunks,
+                        int only_dda, int* choice) {
+  *choice = 0;
+  if (only_fused == 0) return H2G_OK;
+  if (int rc = sweep_attrs()) return rc;
+  const size_t bytes = sizeof(double) * (size_t)s->g.n;
+  for (auto& p : s->hook)
+    if (!p) CK(cudaMalloc(&p, bytes));
+  T* xa = static_cast<T*>(s->hook[0]);
+  T* xb = static_cast<T*>(s->hook[1]);
+  T* xc = static_cast<T*>(s->hook[2]);
+  k_fill_const<T><<<elementwise_blocks(s), 256, 0, s->stream>>>((long long)s->g.n, xa, T(300));
+  k_fill_const<T><<<elementwise_blocks(s), 256, 0, s->stream>>>((long long)s->g.n, xb, T(-1.0e-3));
+  k_fill_const<T><<<elementwise_blocks(s), 256, 0, s->stream>>>((long long)s->g.n, xc, T(300));
+  CKL();
+  s->hook_filled = false;
+  std::vector<int> cands = sweep_chunk_candidates(s);
+  if (only_chunks > 0) cands = {only_chunks};
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return fail(H2G_CUDA_ERROR, "event creation failed");
+  }
+  const int saved_c = s->sw_chunks;
+  const bool saved_d = s->sw_dda;
+  float best = only_fused == 1 ? 1e30f : unfused_ms;
+  int rc = H2G_OK;
+  for (int round = 0; round < 2 && rc == H2G_OK; ++round)
+    for (int c : cands)
+      for (int d = 0; d < 2 && rc == H2G_OK; ++d) {
+        if (only_dda >= 0 && d != only_dda) continue;
+        s->sw_chunks = c;
+        s->sw_dda = d != 0;
+        for (int r = 0; r < 2 && rc == H2G_OK; ++r) rc = launch_sweep<T>(s, s->stream, op, (r & 1) ? xc : xa,
+                                                                         (r & 1) ? xa : xc, xb, nullptr);
+        cudaEventRecord(e0, s->stream);
+        for (int r = 0; r < 10 && rc == H2G_OK; ++r) rc = launch_sweep<T>(s, s->stream, op, (r & 1) ? xc : xa,
+                                                                          (r & 1) ? xa : xc, xb, nullptr);
+        cudaEventRecord(e1, s->stream);
+        float ms = 0.f;
+        if (rc == H2G_OK && (cudaGetLastError() != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+                             cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess))
+          rc = fail(H2G_CUDA_ERROR, "fused-sweep tuning failed");
+        if (rc == H2G_OK && round == 1 && ms < best) {
+          best = ms;
+          *choice = 1 | (d << 1) | (c << 2);
+        }
+      }
+  s->sw_chunks = saved_c;
+  s->sw_dda = saved_d;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc == H2G_OK) rc = sweep_status(s);
   return rc;
 }
 
@@ -1460,16 +1725,27 @@ static int tune_ax(Solver* s, int* use_dd) {
 
 static int autotune(Solver* s) {
   if (s->rb_tuned) return H2G_OK;
-  // choices forced by the environment (-1: not forced)
-  int rows = -1, planes = -1, rbdd = -1, dd = -1;
+  // choices forced by the environment or h2g_set_sweep (-1: not forced)
+  int rows = -1, planes = -1, rbdd = -1, dd = -1, fused = -1, chunks = -1, swdd = -1;
   if (const char* e = getenv("H2G_RB_ROWS")) rows = valid_rows(atoi(e)) ? atoi(e) : -1;
   if (const char* e = getenv("H2G_RB_PLANES")) planes = (atoi(e) == 1 || atoi(e) == 2) ? atoi(e) : -1;
   if (const char* e = getenv("H2G_RB_DD")) rbdd = atoi(e) ? 1 : 0;
   if (const char* e = getenv("H2G_AX_DD")) dd = atoi(e) ? 1 : 0;
-  if (rows < 0 || planes < 0 || rbdd < 0 || dd < 0) {
+  if (const char* e = getenv("H2G_RB_FUSED")) fused = atoi(e) ? 1 : 0;
+  if (const char* e = getenv("H2G_SW_CHUNKS")) chunks = (atoi(e) >= 1 && atoi(e) <= 255) ? atoi(e) : -1;
+  if (const char* e = getenv("H2G_SW_DD")) swdd = atoi(e) ? 1 : 0;
+  if (s->sweep_forced >= 0) {
+    fused = s->sweep_forced;
+    chunks = s->sweep_forced ? s->sw_chunks : -1;
+    swdd = s->sweep_forced ? (s->sw_dda ? 1 : 0) : -1;
+  }
+  if (chunks > s->g.NZ) chunks = s->g.NZ;
+  const bool sweep_known = fused == 0 || (fused == 1 && chunks > 0 && swdd >= 0);
+  if (rows < 0 || planes < 0 || rbdd < 0 || dd < 0 || !sweep_known) {
     // cached per grid, smoother precision and the choices the environment restricts it to
-    const int forced = (rows + 1) + 18 * ((planes + 1) + 6 * (rbdd + 1));  // 0 .. 323
-    const std::array<int, 4> key = {s->g.MX, s->g.MY, s->g.MZ, (s->precision == H2G_FP64 ? 64 : 32) * 512 + forced};
+    const std::array<int, 11> key = {s->g.MX, s->g.MY,  s->g.MZ, s->precision == H2G_FP64 ? 64 : 32,
+                                     rows,    planes,   rbdd,    dd,
+                                     fused,   chunks,   swdd};
     int cached = 0;
     {
       // held while tuning, so that handles of one grid solved concurrently (h2g_batch_solve) tune
@@ -1478,13 +1754,28 @@ static int autotune(Solver* s) {
       auto it = g_tune_cache.find(key);
       if (it != g_tune_cache.end()) cached = it->second;
       if (!cached) {
-        int r2 = 0, d2 = 0;
+        int r2 = 0, d2 = 0, sw = 0;
+        float unfused_ms = 1e30f;
         int rc = s->precision == H2G_FP64
-                     ? tune_rows_t<double>(s, op_params<double>(s, s->t64), rows, planes, rbdd, &r2)
-                     : tune_rows_t<float>(s, op_params<float>(s, s->t32), rows, planes, rbdd, &r2);
+                     ? tune_rows_t<double>(s, op_params<double>(s, s->t64), rows, planes, rbdd, &r2, &unfused_ms)
+                     : tune_rows_t<float>(s, op_params<float>(s, s->t32), rows, planes, rbdd, &r2, &unfused_ms);
         if (!rc) rc = tune_ax(s, &d2);
+        if (!rc && !sweep_known) {
+          // the fused sweep is timed with the colour-pass shape just chosen for its first pass
+          const int sr = s->rb_rows, sp = s->rb_planes;
+          const bool sd = s->rb_dd;
+          s->rb_rows = r2 & 0x1f;
+          s->rb_planes = (r2 >> 5) & 7;
+          s->rb_dd = (r2 >> 8) & 1;
+          rc = s->precision == H2G_FP64
+                   ? tune_sweep_t<double>(s, op_params<double>(s, s->t64), unfused_ms, fused, chunks, swdd, &sw)
+                   : tune_sweep_t<float>(s, op_params<float>(s, s->t32), unfused_ms, fused, chunks, swdd, &sw);
+          s->rb_rows = sr;
+          s->rb_planes = sp;
+          s->rb_dd = sd;
+        }
         if (rc) return rc;
-        cached = r2 | (d2 << 9);
+        cached = r2 | (d2 << 9) | (sw << 10) | (1 << 30);
         g_tune_cache[key] = cached;
       }
     }
@@ -1492,13 +1783,29 @@ static int autotune(Solver* s) {
     if (planes < 0) planes = (cached >> 5) & 7;
     if (rbdd < 0) rbdd = (cached >> 8) & 1;
     if (dd < 0) dd = (cached >> 9) & 1;
+    if (!sweep_known) {
+      const int sw = (cached >> 10) & 0x3ff;
+      fused = sw & 1;
+      swdd = (sw >> 1) & 1;
+      chunks = std::max(1, (sw >> 2) & 0xff);
+    }
   }
-  if (rows != s->rb_rows || planes != s->rb_planes || (rbdd != 0) != s->rb_dd || (dd != 0) != s->ax_dd)
+  if (fused == 1) {
+    if (int rc = sweep_attrs()) return rc;
+  } else {
+    chunks = s->sw_chunks;
+    swdd = s->sw_dda ? 1 : 0;
+  }
+  if (rows != s->rb_rows || planes != s->rb_planes || (rbdd != 0) != s->rb_dd || (dd != 0) != s->ax_dd ||
+      (fused == 1) != s->rb_fused || chunks != s->sw_chunks || (swdd != 0) != s->sw_dda)
     invalidate_graphs(s);
   s->rb_rows = rows;
   s->rb_planes = planes;
   s->rb_dd = rbdd != 0;
   s->ax_dd = dd != 0;
+  s->rb_fused = fused == 1;
+  s->sw_chunks = chunks;
+  s->sw_dda = swdd != 0;
   s->rb_tuned = true;
   return H2G_OK;
 }
@@ -1539,6 +1846,9 @@ static int create(int MX, int MY, int MZ, int precision, Solver** out) {
   const size_t kvb = s->elem * (size_t)g.n;
   for (int i = 0; i < 8; ++i) AL(s->kv[i], kvb);
   if (precision == H2G_MIXED) AL(s->kv[KBB], sizeof(float) * (size_t)g.n);
+  AL(s->x2_64, nb);
+  if (precision != H2G_FP64) AL(s->x2_32, sizeof(float) * (size_t)g.n);
+  AL(s->sweep_err, sizeof(int));
   if (precision == H2G_MIXED_IR) {
     AL(s->kv[KE], kvb);
     AL(s->r64, nb);
@@ -1680,8 +1990,7 @@ static int hook_buffers(Solver* s, void** a, void** b) {
   const size_t bytes = sizeof(double) * (size_t)s->g.n;
   for (auto& p : s->hook)
     if (!p) CK(cudaMalloc(&p, bytes));
-  CK(cudaMemsetAsync(s->hook[0], 0, bytes, s->stream));
-  CK(cudaMemsetAsync(s->hook[1], 0, bytes, s->stream));
+  for (auto& p : s->hook) CK(cudaMemsetAsync(p, 0, bytes, s->stream));
   s->hook_filled = false;
   *a = s->hook[0];
   *b = s->hook[1];
@@ -1722,6 +2031,7 @@ static int precond_t(Solver* s, const double* bb, double* xx, int smoother, cons
   using namespace h2g;
   void *ha, *hb;
   int rc;
+  if ((rc = autotune(s))) return rc;  // before the hook buffers are filled: the tuner uses them
   if ((rc = hook_buffers(s, &ha, &hb))) return rc;
   T* xd = static_cast<T*>(ha);
   T* bd = static_cast<T*>(hb);
@@ -1729,10 +2039,22 @@ static int precond_t(Solver* s, const double* bb, double* xx, int smoother, cons
   const dim3 blk(kBX, kBY);
   const int none = smoother == H2G_SMOOTHER_NONE;
   launch(s, k_rb_first<T, T, 0>, first_grid(s->g), blk, s->stream, op, xd, bd, nullptr, nullptr, nullptr, nullptr, none);
-  if (!none)
-    for (int pass = 1; pass < 2 * kSweeps; ++pass) launch_rb<T>(s, s->stream, op, xd, (const T*)bd, pass & 1, T(1), nullptr);
+  if (!none) {
+    // the fused sweeps ping-pong through the third (zeroed) hook buffer, not the solvers' x2
+    T* x2 = static_cast<T*>(s->hook[2]);
+    launch_rb<T>(s, s->stream, op, xd, (const T*)bd, 1, T(1), nullptr);
+    if (s->rb_fused) {
+      for (int sw = 1; sw < kSweeps; ++sw)
+        if ((rc = launch_sweep<T>(s, s->stream, op, (sw & 1) ? xd : x2, (sw & 1) ? x2 : xd, (const T*)bd, nullptr)))
+          return rc;
+    } else {
+      for (int pass = 2; pass < 2 * kSweeps; ++pass)
+        launch_rb<T>(s, s->stream, op, xd, (const T*)bd, pass & 1, T(1), nullptr);
+    }
+  }
   CKL();
-  return download<T>(s, xd, xx);
+  if ((rc = download<T>(s, xd, xx))) return rc;
+  return sweep_status(s);
 }
 
 template <typename T>
@@ -1749,14 +2071,22 @@ static int bench_t(Solver* s, int kind, int reps, int* launches, const h2g::OpPa
   if (!s->hook_filled) {  // once, outside the caller's timed repetitions
     k_fill_const<T><<<elementwise_blocks(s), 256, 0, s->stream>>>((long long)s->g.n, xa, T(300));
     k_fill_const<T><<<elementwise_blocks(s), 256, 0, s->stream>>>((long long)s->g.n, xb, T(-1.0e-3));
+    k_fill_const<T><<<elementwise_blocks(s), 256, 0, s->stream>>>((long long)s->g.n, static_cast<T*>(s->hook[2]),
+                                                                  T(300));
     CKL();
     CK(cudaStreamSynchronize(s->stream));
     s->hook_filled = true;
   }
   const dim3 blk(kBX, kBY);
   int n = 0;
+  T* xc = static_cast<T*>(s->hook[2]);
   for (int r = 0; r < reps; ++r) {
-    if (kind == 0) {
+    if (kind == 0 && s->rb_fused) {
+      // one fused sweep; consecutive calls alternate between the two scratch vectors
+      const bool fwd = (s->bench_parity++ & 1) == 0;
+      if (int rc = launch_sweep<T>(s, s->stream, op, fwd ? xa : xc, fwd ? xc : xa, (const T*)xb, nullptr)) return rc;
+      n += 1;
+    } else if (kind == 0) {
       launch_rb<T>(s, s->stream, op, xa, (const T*)xb, 0, T(1), nullptr);
       launch_rb<T>(s, s->stream, op, xa, (const T*)xb, 1, T(1), nullptr);
       n += 2;
@@ -2069,6 +2399,43 @@ int h2g_set_tuning(h2g_solver* h, int rows, int planes) {
   s->rb_rows = rows;
   s->rb_planes = planes;
   s->rb_tuned = true;
+  return H2G_OK;
+}
+
+int h2g_set_sweep(h2g_solver* h, int fused, int chunks, int dd_array) {
+  if (int rc = h2g::check_handle(h)) return rc;
+  Solver* s = S(h);
+  if (fused < -1 || fused > 1) return fail(H2G_BAD_ARG, "fused must be -1 (tune), 0 or 1");
+  if (fused == 1 && (chunks < 1 || chunks > 255)) return fail(H2G_BAD_ARG, "chunks must be in 1..255");
+  if (fused == 1 && dd_array != 0 && dd_array != 1) return fail(H2G_BAD_ARG, "dd_array must be 0 or 1");
+  s->sweep_forced = fused;
+  if (fused == 1) {
+    s->sw_chunks = std::min(chunks, s->g.NZ);
+    s->sw_dda = dd_array != 0;
+  }
+  s->rb_tuned = false;  // the next solve applies the choice (and tunes what is left free)
+  h2g::invalidate_graphs(s);
+  return H2G_OK;
+}
+
+int h2g_get_sweep(h2g_solver* h, int* fused, int* chunks, int* dd_array) {
+  if (int rc = h2g::check_handle(h)) return rc;
+  Solver* s = S(h);
+  if (!s->grid_set || !s->fields_set) return fail(H2G_BAD_ARG, "h2g_set_grid and h2g_set_fields must come first");
+  CK(cudaSetDevice(s->device));
+  if (int rc = h2g::autotune(s)) return rc;
+  if (fused) *fused = s->rb_fused ? 1 : 0;
+  if (chunks) *chunks = s->sw_chunks;
+  if (dd_array) *dd_array = s->sw_dda ? 1 : 0;
+  return H2G_OK;
+}
+
+int h2g_set_wait_limit(h2g_solver* h, long long cycles) {
+  if (int rc = h2g::check_handle(h)) return rc;
+  Solver* s = S(h);
+  if (cycles < 0) return fail(H2G_BAD_ARG, "cycles must be >= 0");
+  s->wait_limit = cycles == 0 ? 0 : cycles;
+  h2g::invalidate_graphs(s);  // the limit is a kernel argument captured in the graphs
   return H2G_OK;
 }
 

@@ -244,6 +244,21 @@ class Solver:
         """Force the colour pass's shape (rows 2, 4, 8, 16; planes 1, 2); rows = 0 tunes again."""
         L.check(self.lib.h2g_set_tuning(self.h, int(rows), int(planes)))
 
+    def set_sweep(self, fused: int, chunks: int = 1, dd_array: bool = False):
+        """Force the preconditioner's sweeps 2-5: fused=1 one fused launch per sweep (with `chunks`
+        z chunks and dd read or summed), 0 two colour passes per sweep, -1 let the tuner choose."""
+        L.check(self.lib.h2g_set_sweep(self.h, int(fused), int(chunks), int(bool(dd_array))))
+
+    def sweep(self) -> tuple:
+        """(fused, chunks, dd read) that the next solve uses (running the tuner if needed)."""
+        f, c, d = C.c_int(0), C.c_int(0), C.c_int(0)
+        L.check(self.lib.h2g_get_sweep(self.h, C.byref(f), C.byref(c), C.byref(d)))
+        return bool(f.value), c.value, bool(d.value)
+
+    def set_wait_limit(self, cycles: int):
+        """Budget of one bounded device wait in clock cycles (0: every wait gives up at once)."""
+        L.check(self.lib.h2g_set_wait_limit(self.h, int(cycles)))
+
     def bench_kernel(self, kind: int, reps: int) -> int:
         n = C.c_int()
         L.check(self.lib.h2g_bench_kernel(self.h, int(kind), int(reps), C.byref(n)))

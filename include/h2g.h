@@ -34,7 +34,7 @@ extern "C" {
 #define H2G_NONFINITE 3       /* NaN/Inf in an input array or in the iteration */
 #define H2G_BAD_ARG 4         /* rejected on the host before any launch */
 #define H2G_CUDA_ERROR 5      /* a CUDA runtime call failed */
-#define H2G_TIMEOUT 6         /* a bounded device wait ran out (reserved: no kernel here waits) */
+#define H2G_TIMEOUT 6         /* a bounded device wait ran out (the fused sweep's TMA waits) */
 #define H2G_UNSUPPORTED 7     /* input outside what the library implements (message says what) */
 
 /* ---- precision ---------------------------------------------------------------------- */
@@ -221,6 +221,22 @@ int h2g_transient(h2g_solver *h, const h2g_bc *bc, int nt, int method, double to
  * rows = 0: tune again on the next solve). */
 int h2g_autotune(h2g_solver *h, int *rows, int *planes, int *rb_dd, int *ax_dd);
 int h2g_set_tuning(h2g_solver *h, int rows, int planes);
+/* The preconditioner's sweeps 2-5 as one fused launch each (k_rb_sweep: both colours of a sweep,
+ * planes of x and keys staged in shared memory by TMA, z-marching, results bit-identical to the
+ * colour passes) or as two colour passes each.  The tuner times the fused sweep for several
+ * numbers of z chunks, with dd summed or read, against the best colour-pass shape and keeps the
+ * faster (H2G_RB_FUSED, H2G_SW_CHUNKS, H2G_SW_DD in the environment force it).  h2g_set_sweep forces
+ * the choice on a handle: fused 0 (colour passes), 1 (fused, with `chunks` z chunks, 1..255, and
+ * dd read from the per-cell array if dd_array) or -1 (tune again); h2g_get_sweep reports what the
+ * next solve uses.  No reference counterpart (rbsor!, NonUniform.jl:936-957, runs the colours one
+ * after another over the whole grid). */
+int h2g_set_sweep(h2g_solver *h, int fused, int chunks, int dd_array);
+int h2g_get_sweep(h2g_solver *h, int *fused, int *chunks, int *dd_array);
+/* Budget of one bounded device wait (the fused sweep's waits for its TMA copies), in SM clock
+ * cycles; default about one second.  0 makes every such wait give up at once: the solve then ends
+ * with H2G_TIMEOUT, the copies in flight are drained and the context stays usable (the failure
+ * path of the bounded waits, exercised by the tests without a GPU fault). */
+int h2g_set_wait_limit(h2g_solver *h, long long cycles);
 
 /* ---- kernels of the path, callable one at a time (host arrays in and out) ---------------
  * CalcAX! (NonUniform.jl:454-511): ax = A x over the interior; guard cells of ax are 0. */
