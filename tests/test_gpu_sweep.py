@@ -10,6 +10,8 @@ the fused sweep must equal the colour-pass solves bit for bit, iteration count i
 bounded waits of the kernel are exercised with a zero budget: the solve ends with H2G_TIMEOUT and
 the handle keeps working.
 """
+import ctypes
+
 import numpy as np
 import pytest
 
@@ -116,8 +118,15 @@ def test_fused_wait_timeout_is_reported(oracle):
     s.set_sweep(1, 2, False)
     s.snapshot()
     s.set_wait_limit(0)
-    st, res = s.solve("pbicgstab", tol=1e-8, maxItr=200, smoother="gs")
+    # through the C ABI: the status is returned and copied into the result
+    from h2_b200 import _lib as L
+    res = L.Result()
+    st = L.load().h2g_pbicgstab(s.h, 1e-8, 200, 1, 0, None, ctypes.byref(res))
     assert st == H2G_TIMEOUT and res.status == H2G_TIMEOUT and not res.isconverged
+    # the Python mirror raises it, as it does every hard error
+    with pytest.raises(h2_b200.H2GError) as e:
+        s.solve("pbicgstab", tol=1e-8, maxItr=200, smoother="gs")
+    assert e.value.status == H2G_TIMEOUT
     with pytest.raises(h2_b200.H2GError) as e:
         s.preconditioner(random_interior(prob.shape, 1), "gs")
     assert e.value.status == H2G_TIMEOUT
