@@ -9,8 +9,11 @@ reference's operator.
 
 backward returns dJ/dhsrc and dJ/dlnlam per cell (zero on the guards, which the model does not
 use) times the incoming gradient.  Inputs and gradients are float64 tensors of the grid's shape
-(MX, MY, MZ) indexed [i, j, k] like the reference's arrays.  The Julia counterpart is the
-ChainRulesCore rrule in julia/H2GPURules.jl.
+(MX, MY, MZ) indexed [i, j, k] like the reference's arrays.  The library keys every cell's
+conductivity in 7 bits, so lambda may take at most 127 distinct values over the grid: per-band or
+per-material parameters fit (the 13 log-scales of h2_b200.adjoint give at most 84), a field of
+per-cell values does not (H2GError, status UNSUPPORTED).  The gradient is per cell either way.
+The Julia counterpart is the ChainRulesCore rrule in julia/H2GPURules.jl.
 """
 from __future__ import annotations
 

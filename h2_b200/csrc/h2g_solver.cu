@@ -75,6 +75,7 @@ struct SolveGraph {
 #define H2G_UNROLL 4
 #endif
 constexpr int kUnroll = H2G_UNROLL;  // Krylov iterations per captured loop-body pass
+static_assert(kUnroll % 2 == 0, "p ping-pongs between two buffers: an even number of iterations per pass");
 
 enum GraphKind {
   kGPbicg64 = 0, kGCg64 = 1, kGPbicg32 = 2, kGCg32 = 3, kGPbicgMx = 4, kGCgMx = 5, kGSor = 6, kGNum = 7
@@ -130,8 +131,10 @@ struct Solver {
   double* lamv = nullptr;      // lambda value of every material key (adjoint gradient)
   double* tstates = nullptr;   // transient adjoint: checkpoints, segment states, final state
   size_t tstates_cap = 0;      // in vectors
-  // Krylov vectors in working precision: r, r0, p, ph, q, s, sh, t (+ e for refinement)
-  void* kv[10] = {nullptr};
+  // Krylov vectors in working precision: r, r0, p, ph, q, s, sh, t (+ e for refinement, the FP32
+  // right-hand side of the mixed smoother, and p's second buffer: the fused first sweep reads the
+  // old p at its overlap cells, so p ping-pongs between two buffers from iteration to iteration)
+  void* kv[11] = {nullptr};
   void* hook[3] = {nullptr, nullptr, nullptr};  // scratch of the single-kernel entry points (never a Krylov vector)
   bool hook_filled = false;            // hook[] holds the benchmark's non-zero scratch values
   unsigned bench_parity = 0;           // direction of the next fused benchmark sweep
@@ -384,19 +387,55 @@ double* x2buf<double>(Solver* s) { return s->x2_64; }
 template <>
 float* x2buf<float>(Solver* s) { return s->x2_32; }
 
-// Preconditioner! after its first colour pass (k_rb_first wrote xx): colour 1 of sweep 1, then
-// sweeps 2..5, either as colour passes in place or as fused sweeps xx -> x2 -> xx -> x2 -> xx.
-template <typename T>
-static int launch_precond_tail(Solver* s, cudaStream_t cs, const OpParams<T>& op, T* xx, const T* bb,
-                               SolverState* st) {
-  launch_rb<T>(s, cs, op, xx, bb, 1, T(1), st);
-  if (s->rb_fused) {
-    T* x2 = x2buf<T>(s);
+
+// k_rb_sweep_first with the handle's chunking and dd source.
+template <typename T, typename TV, int VM>
+static int launch_sweep_first(Solver* s, cudaStream_t cs, const OpParams<T>& op, T* xout, TV* vout, const TV* vin,
+                              T* bbT, const TV* r, const TV* q, SolverState* st) {
+  const CUtensorMap* mk = nullptr;
+  if (int rc = kmap(s, &mk)) return rc;
+  const Geo& g = op.g;
+  const int kc = (g.NZ + s->sw_chunks - 1) / s->sw_chunks;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = sweep_grid(g, s->sw_chunks);
+  cfg.blockDim = dim3(kSwTPX, kSwTJ);
+  cfg.dynamicSmemBytes = sweep_first_smem<T>();
+  cfg.stream = cs;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = s->pdl ? 1 : 0;
+  if (s->sw_dda)
+    cudaLaunchKernelEx(&cfg, k_rb_sweep_first<T, TV, VM, true>, op, *mk, xout, vout, vin, bbT, r, q, kc, st,
+                       s->sweep_err, s->wait_limit);
+  else
+    cudaLaunchKernelEx(&cfg, k_rb_sweep_first<T, TV, VM, false>, op, *mk, xout, vout, vin, bbT, r, q, kc, st,
+                       s->sweep_err, s->wait_limit);
+  return H2G_OK;
+}
+
+// Preconditioner! (NonUniform.jl:531-559) fused with the Krylov update that makes its right-hand
+// side (VM as in k_rb_first): xx = M^-1 bb from xx = 0.  VM 0: bb = vin; VM 1: bb = p written to
+// vout from p = vin (the same buffer on the colour-pass path); VM 2: bb = s written to vout.
+// Fused path: one k_rb_sweep_first (sweep 1) and 4 fused sweeps; colour-pass path: k_rb_first and
+// 9 colour passes.  x2 is the fused sweeps' ping-pong partner (zero guards).
+template <typename T, typename TV, int VM>
+static int launch_precond(Solver* s, cudaStream_t cs, const OpParams<T>& op, T* xx, T* x2, TV* vin, TV* vout,
+                          T* bbT, const TV* r, const TV* q, SolverState* st, int smoother) {
+  const int none = smoother == H2G_SMOOTHER_NONE;
+  const T* bb = bbT ? bbT : reinterpret_cast<const T*>(VM == 0 ? vin : vout);
+  if (s->rb_fused && !none) {
+    if (int rc = launch_sweep_first<T, TV, VM>(s, cs, op, xx, vout, vin, bbT, r, q, st)) return rc;
     for (int sw = 1; sw < kSweeps; ++sw)
       if (int rc = launch_sweep<T>(s, cs, op, (sw & 1) ? xx : x2, (sw & 1) ? x2 : xx, bb, st)) return rc;
-  } else {
-    for (int pass = 2; pass < 2 * kSweeps; ++pass) launch_rb<T>(s, cs, op, xx, bb, pass & 1, T(1), st);
+    return H2G_OK;
   }
+  // k_rb_first updates v in place (VM 1 reads and writes p there)
+  TV* v = VM == 0 ? vin : vout;
+  launch(s, k_rb_first<T, TV, VM>, first_grid(op.g), dim3(kBX, kBY), cs, op, xx, v, bbT, r, q, st, none);
+  if (none) return H2G_OK;
+  for (int pass = 1; pass < 2 * kSweeps; ++pass) launch_rb<T>(s, cs, op, xx, bb, pass & 1, T(1), st);
   return H2G_OK;
 }
 
@@ -411,7 +450,7 @@ template <typename T>
 static T* kvec(Solver* s, int i) {
   return reinterpret_cast<T*>(s->kv[i]);
 }
-enum { KR = 0, KR0 = 1, KP = 2, KPH = 3, KQ = 4, KS = 5, KSH = 6, KT = 7, KE = 8, KBB = 9 };
+enum { KR = 0, KR0 = 1, KP = 2, KPH = 3, KQ = 4, KS = 5, KSH = 6, KT = 7, KE = 8, KBB = 9, KP2 = 10 };
 
 template <typename T>
 static OpParams<T> op_params(const Solver* s, const OpTables<T>& t);
@@ -631,29 +670,27 @@ static int build_tables(Solver* s) {
 // With TP != T the first pass also writes the smoother's copy of its right-hand side (bb32).
 template <typename T, typename TX, typename TP>
 static int launch_pbicg_body(Solver* s, cudaStream_t cs, const OpParams<T>& opA, const OpParams<TP>& opM, TX* x,
-                             SolverState* st, int smoother, cudaGraphConditionalHandle hc, int use_cond) {
+                             SolverState* st, int smoother, cudaGraphConditionalHandle hc, int use_cond, int u) {
   const Geo& g = s->g;
   T* r = kvec<T>(s, KR);
   T* r0 = kvec<T>(s, KR0);
-  T* p = kvec<T>(s, KP);
+  // p of this iteration is read from p_in and written to p_out; they alternate on the fused path
+  const bool pp = s->rb_fused && smoother != H2G_SMOOTHER_NONE;
+  T* p_in = kvec<T>(s, pp && (u & 1) ? KP2 : KP);
+  T* p_out = kvec<T>(s, pp && !(u & 1) ? KP2 : KP);
   TP* ph = kvec<TP>(s, KPH);
   T* q = kvec<T>(s, KQ);
   T* sv = kvec<T>(s, KS);
   TP* sh = kvec<TP>(s, KSH);
   T* t = kvec<T>(s, KT);
   TP* bbm = std::is_same<T, TP>::value ? nullptr : kvec<TP>(s, KBB);
-  const dim3 blk(kBX, kBY);
-  const int none = smoother == H2G_SMOOTHER_NONE;
+  TP* x2 = x2buf<TP>(s);
   // p = r + beta (p - omega q); p_ = M^-1 p                     NonUniform.jl:296-305
-  launch(s, k_rb_first<TP, T, 1>, first_grid(g), blk, cs, opM, ph, p, bbm, r, q, st, none);
-  if (!none)
-    if (int rc = launch_precond_tail<TP>(s, cs, opM, ph, bbm ? bbm : reinterpret_cast<TP*>(p), st)) return rc;
+  if (int rc = launch_precond<TP, T, 1>(s, cs, opM, ph, x2, p_in, p_out, bbm, r, q, st, smoother)) return rc;
   // q = A p_;  alpha = rho / (q, r0)                            NonUniform.jl:307-309
   launch_ax<T, 1, TP>(s, cs, opA, q, ph, r0, nullptr, st, kStageAlpha);
   // s = r - alpha q; s_ = M^-1 s                                NonUniform.jl:310-315
-  launch(s, k_rb_first<TP, T, 2>, first_grid(g), blk, cs, opM, sh, sv, bbm, r, q, st, none);
-  if (!none)
-    if (int rc = launch_precond_tail<TP>(s, cs, opM, sh, bbm ? bbm : reinterpret_cast<TP*>(sv), st)) return rc;
+  if (int rc = launch_precond<TP, T, 2>(s, cs, opM, sh, x2, sv, sv, bbm, r, q, st, smoother)) return rc;
   // t = A s_; omega = (t,s)/(t,t)                               NonUniform.jl:317-326
   launch_ax<T, 2, TP>(s, cs, opA, t, sh, nullptr, sv, st, kStageOmega);
   // x += alpha p_ + omega s_; r = s - omega t; res; next rho    NonUniform.jl:328-346
@@ -670,13 +707,8 @@ static int launch_pbicg_body(Solver* s, cudaStream_t cs, const OpParams<T>& opA,
 template <typename T, typename TP>
 static int launch_precond_r(Solver* s, cudaStream_t cs, const OpParams<TP>& opM, TP* z, T* r, SolverState* st,
                             int smoother) {
-  const Geo& g = s->g;
-  const dim3 blk(kBX, kBY);
-  const int none = smoother == H2G_SMOOTHER_NONE;
   TP* bbm = std::is_same<T, TP>::value ? nullptr : kvec<TP>(s, KBB);
-  launch(s, k_rb_first<TP, T, 0>, first_grid(g), blk, cs, opM, z, r, bbm, nullptr, nullptr, st, none);
-  if (!none) return launch_precond_tail<TP>(s, cs, opM, z, bbm ? bbm : reinterpret_cast<TP*>(r), st);
-  return H2G_OK;
+  return launch_precond<TP, T, 0>(s, cs, opM, z, x2buf<TP>(s), r, r, bbm, nullptr, nullptr, st, smoother);
 }
 
 template <typename T, typename TX, typename TP>
@@ -787,7 +819,7 @@ static int get_graph(Solver* s, int kind, int smoother, const OpParams<T>& op, c
     // middle of a pass only leaves the rest of the pass as empty launches.
     for (int u = 0; u < kUnroll && berr == H2G_OK; ++u) {
       if (cg) berr = launch_cg_body<T, TX, TP>(s, cs, op, opM, x, st, smoother, hc, use_cond);
-      else berr = launch_pbicg_body<T, TX, TP>(s, cs, op, opM, x, st, smoother, hc, use_cond);
+      else berr = launch_pbicg_body<T, TX, TP>(s, cs, op, opM, x, st, smoother, hc, use_cond, u);
     }
   });
   if (rc == H2G_OK && berr != H2G_OK) G.reset();
@@ -877,11 +909,11 @@ static void print_log(const SolverState& st, const double* hist, int nhist, int 
   fflush(stdout);
 }
 
-// Kernels of one preconditioner call: the first pass, then 9 colour passes or 1 colour pass and
-// 4 fused sweeps.
+// Kernels of one preconditioner call: the first pass and 9 colour passes, or 5 fused sweeps (the
+// first one with the Krylov update).
 static int precond_kernels(const Solver* s, int smoother) {
   if (smoother == H2G_SMOOTHER_NONE) return 1;
-  return s->rb_fused ? 2 + (kSweeps - 1) : 2 * kSweeps;
+  return s->rb_fused ? kSweeps : 2 * kSweeps;
 }
 
 // Kernels in one WHILE-body pass (one Krylov iteration).
@@ -1119,7 +1151,7 @@ static int solve_mixed(Solver* s, bool cg, double tol, int maxItr, int smoother,
     // values (a NaN step length reaches the guard entries of the linear updates); the FP64
     // kernels need their guards zero, so clear them all first, and again at the end for the FP32
     // layout of the next mixed solve on this handle.
-    for (int i = 0; i < 8; ++i) CK(cudaMemsetAsync(s->kv[i], 0, s->elem * (size_t)s->g.n, s->stream));
+    for (int i : {0, 1, 2, 3, 4, 5, 6, 7, (int)KP2}) CK(cudaMemsetAsync(s->kv[i], 0, s->elem * (size_t)s->g.n, s->stream));
     status = H2G_NOT_CONVERGED;
     for (int pass = 0; pass < 4 && total < maxItr; ++pass) {
       h2g_result r;
@@ -1139,7 +1171,7 @@ static int solve_mixed(Solver* s, bool cg, double tol, int maxItr, int smoother,
       if (st != H2G_OK && st != H2G_NOT_CONVERGED) { status = st; break; }
       if (r.itr == 0) break;
     }
-    for (int i = 0; i < 8; ++i) CK(cudaMemsetAsync(s->kv[i], 0, s->elem * (size_t)s->g.n, s->stream));
+    for (int i : {0, 1, 2, 3, 4, 5, 6, 7, (int)KP2}) CK(cudaMemsetAsync(s->kv[i], 0, s->elem * (size_t)s->g.n, s->stream));
   }
   if (out) {
     out->isconverged = converged;
@@ -1845,6 +1877,7 @@ static int create(int MX, int MY, int MZ, int precision, Solver** out) {
   AL(s->key, (size_t)g.n);
   const size_t kvb = s->elem * (size_t)g.n;
   for (int i = 0; i < 8; ++i) AL(s->kv[i], kvb);
+  AL(s->kv[KP2], kvb);
   if (precision == H2G_MIXED) AL(s->kv[KBB], sizeof(float) * (size_t)g.n);
   AL(s->x2_64, nb);
   if (precision != H2G_FP64) AL(s->x2_32, sizeof(float) * (size_t)g.n);
@@ -2036,22 +2069,10 @@ static int precond_t(Solver* s, const double* bb, double* xx, int smoother, cons
   T* xd = static_cast<T*>(ha);
   T* bd = static_cast<T*>(hb);
   if ((rc = upload<T>(s, bb, bd, 1))) return rc;
-  const dim3 blk(kBX, kBY);
-  const int none = smoother == H2G_SMOOTHER_NONE;
-  launch(s, k_rb_first<T, T, 0>, first_grid(s->g), blk, s->stream, op, xd, bd, nullptr, nullptr, nullptr, nullptr, none);
-  if (!none) {
-    // the fused sweeps ping-pong through the third (zeroed) hook buffer, not the solvers' x2
-    T* x2 = static_cast<T*>(s->hook[2]);
-    launch_rb<T>(s, s->stream, op, xd, (const T*)bd, 1, T(1), nullptr);
-    if (s->rb_fused) {
-      for (int sw = 1; sw < kSweeps; ++sw)
-        if ((rc = launch_sweep<T>(s, s->stream, op, (sw & 1) ? xd : x2, (sw & 1) ? x2 : xd, (const T*)bd, nullptr)))
-          return rc;
-    } else {
-      for (int pass = 2; pass < 2 * kSweeps; ++pass)
-        launch_rb<T>(s, s->stream, op, xd, (const T*)bd, pass & 1, T(1), nullptr);
-    }
-  }
+  // the fused sweeps ping-pong through the third (zeroed) hook buffer, not the solvers' x2
+  if ((rc = launch_precond<T, T, 0>(s, s->stream, op, xd, static_cast<T*>(s->hook[2]), bd, bd, nullptr, nullptr,
+                                    nullptr, nullptr, smoother)))
+    return rc;
   CKL();
   if ((rc = download<T>(s, xd, xx))) return rc;
   return sweep_status(s);

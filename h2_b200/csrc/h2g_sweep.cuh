@@ -326,4 +326,215 @@ __global__ void __launch_bounds__(kSwThreads, 1)
   }
 }
 
+// ------------------------------------------------------------------------------------------
+// The first sweep of Preconditioner! fused with the Krylov update that makes its right-hand side
+// (the work of k_rb_first and the first colour-1 pass in one launch).  x starts at zero
+// (myfill!, NonUniform.jl:303/313), so colour 0 needs only bb and dd, and colour 1 the new colour-0
+// values: no plane of x is read, only the key planes are staged.
+//   VM 0: bb = vin (given);  VM 1: bb = r (first iteration) or r + beta*(vin - omega*q), written
+//   to vout (BiCG1!, NonUniform.jl:296-301);  VM 2: bb = (-alpha)*q + r, written to vout
+//   (Triad!, NonUniform.jl:310-311).
+// Overlap cells compute bb from r, q and vin too, so vout must not be vin (the caller ping-pongs
+// p between iterations).  bbT (when T != TV): the smoother's copy of bb in T, owned cells.  Every
+// cell's arithmetic is that of k_rb_first and rb_pass_column, so the bits are the same.
+// ------------------------------------------------------------------------------------------
+template <typename T, typename TV, int VM>
+__device__ __forceinline__ void first_load(const TV* vin, const TV* r, const TV* q, int ci, TV (&a)[3]) {
+  a[0] = VM == 0 ? __ldg(vin + ci) : __ldg(r + ci);
+  a[1] = VM == 1 ? __ldg(vin + ci) : TV(0);
+  a[2] = VM != 0 ? __ldg(q + ci) : TV(0);
+}
+template <int VM, typename TV>
+__device__ __forceinline__ TV first_bb(const TV (&a)[3], int first, TV beta, TV omg, TV alpha) {
+  if (VM == 0) return a[0];
+  if (VM == 1) return first ? a[0] : add(a[0], mul(beta, sub(a[1], mul(omg, a[2]))));
+  return add(mul(-alpha, a[2]), a[0]);
+}
+
+template <typename T, typename TV, int VM, bool DDA>
+__global__ void __launch_bounds__(kSwThreads, 1)
+    k_rb_sweep_first(OpParams<T> op, const __grid_constant__ CUtensorMap tmk, T* __restrict__ xout,
+                     TV* __restrict__ vout, const TV* __restrict__ vin, T* __restrict__ bbT,
+                     const TV* __restrict__ r, const TV* __restrict__ q, int kc, SolverState* st, int* err,
+                     long long wait_limit) {
+  using C = SwCfg<T>;
+  pdl_enter();
+  if (st && st->stop) return;
+  extern __shared__ __align__(128) unsigned char sm[];
+  const Geo& g = op.g;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + kSwTPX * ty;
+  const int q0 = (int)blockIdx.x * (kSwTPX - 2) - 1, r0 = (int)blockIdx.y * (kSwTJ - 2);
+  const int p = q0 + tx, j = r0 + ty;
+  const int kA = 1 + (int)blockIdx.z * kc, kB = min(kA + kc - 1, g.NZ);
+  const int xk = align_down(q0 - 1, 16), ys = 2 * (r0 - 1);
+  const int first = kA - 2, last = kB + 2;
+  const bool owned = tx >= 1 && tx < kSwTPX - 1 && ty >= 1 && ty < kSwTJ - 1;
+  const bool jin = j >= 1 && j <= g.NY && p >= 0;
+  const int ck = p - xk;
+  const int rr0 = 2 * (ty + 1), rr1 = rr0 + 1;
+  // shared memory: kSwStages key planes, then the colour-0 exchange buffer, then the barriers
+  constexpr int KOFF = kSwStages * C::KBYTES;
+  T* c0b = reinterpret_cast<T*>(sm + KOFF);
+  const int BOFF = KOFF + C::C0BYTES;
+  volatile int* flag = reinterpret_cast<volatile int*>(sm + BOFF + 8 * kSwStages);
+  const uint32_t bar0 = smem_u32(sm + BOFF);
+  auto kbox = [&](int plane) {
+    return reinterpret_cast<const uint8_t*>(sm + ((plane - first) % kSwStages) * C::KBYTES);
+  };
+  auto bar = [&](int plane) { return bar0 + 8u * (uint32_t)((plane - first) % kSwStages); };
+  auto parity = [&](int plane) { return (uint32_t)(((plane - first) / kSwStages) & 1); };
+  auto issue = [&](int plane) {
+    const int qq = (plane - first) % kSwStages;
+    const uint32_t b = bar0 + 8u * qq;
+    mbar_expect_tx(b, (uint32_t)C::KBYTES);
+    tma_load_3d(smem_u32(sm + qq * C::KBYTES), &tmk, xk, ys, plane, b);
+  };
+  auto in0 = [&](int k) {
+    const int i = 2 * p + ((1 + j + k) & 1);
+    return jin && k >= 1 && k <= g.NZ && i >= 1 && i <= g.NX;
+  };
+  auto in1 = [&](int k) {
+    const int i = 2 * p + ((j + k) & 1);
+    return jin && k >= 1 && k <= g.NZ && i >= 1 && i <= g.NX;
+  };
+  auto off0 = [&](int k) { return g.row(0, j, k) + p; };
+  auto off1 = [&](int k) { return g.row(1, j, k) + p; };
+  int firstit = 0;
+  TV beta = TV(0), omg = TV(0), alpha = TV(0);
+  if (VM == 1) {
+    firstit = st->first;
+    beta = (TV)st->beta;
+    omg = (TV)st->omega;
+  } else if (VM == 2) {
+    alpha = (TV)st->alpha;
+  }
+
+  int issued = first - 1, waited = first - 1;
+  if (tid == 0) {
+    for (int qq = 0; qq < kSwStages; ++qq) mbar_init(bar0 + 8u * qq, 1);
+    mbar_fence_init();
+    *flag = 0;
+    for (int pl = first; pl <= min(first + kSwStages - 2, last); ++pl) {
+      issue(pl);
+      issued = pl;
+    }
+    if (mbar_wait_bounded(bar(first), parity(first), wait_limit)) waited = first;
+    if (waited == first && mbar_wait_bounded(bar(first + 1), parity(first + 1), wait_limit)) waited = first + 1;
+    if (waited != first + 1) *flag = 1;
+  }
+  __syncthreads();
+  bool abort = *flag != 0;
+
+  T c0v[3] = {T(0), T(0), T(0)};
+  uint32_t c1k[3] = {0u, 0u, 0u}, c0k[3] = {0u, 0u, 0u};
+  TV a0[3] = {TV(0), TV(0), TV(0)}, a1[3] = {TV(0), TV(0), TV(0)};  // raw operands of bb, a step ahead
+  if (!abort) {
+    c1k[1] = kbox(first)[rr1 * kSwWK + ck];
+    c1k[2] = kbox(first + 1)[rr1 * kSwWK + ck];
+    if (in0(kA - 1)) first_load<T, TV, VM>(vin, r, q, off0(kA - 1), a0);
+  }
+  for (int s = kA - 1; s <= kB + 1 && !abort; ++s) {
+    if (tid == 0) {
+      if (mbar_wait_bounded(bar(s + 1), parity(s + 1), wait_limit)) waited = s + 1;
+      else *flag = 1;
+    }
+    __syncthreads();
+    if (*flag) {
+      abort = true;
+      break;
+    }
+    if (tid == 0 && s + 3 <= last) {
+      issue(s + 3);
+      issued = s + 3;
+    }
+    const uint8_t* K0 = kbox(s);
+    const uint8_t* Km = kbox(s - 1);
+    c1k[0] = c1k[1];
+    c1k[1] = c1k[2];
+    c1k[2] = kbox(s + 1)[rr1 * kSwWK + ck];
+    const bool do1 = owned && s >= kA && s <= kB;
+    TV n0[3] = {TV(0), TV(0), TV(0)}, n1[3] = {TV(0), TV(0), TV(0)};
+    if (s <= kB && in0(s + 1)) first_load<T, TV, VM>(vin, r, q, off0(s + 1), n0);
+    if (do1 && in1(s)) first_load<T, TV, VM>(vin, r, q, off1(s), n1);
+
+    // phase A: colour 0 at plane s from x = 0: ((0 - bb)/dd - 0), then 0 + that
+    {
+      const uint32_t k0 = K0[rr0 * kSwWK + ck];
+      T nv = T(0);
+      const bool in = in0(s);
+      if (in) {
+        const TV bv = first_bb<VM>(a0, firstit, beta, omg, alpha);
+        const T b = (T)bv;
+        if (owned && s >= kA && s <= kB) {
+          if (VM != 0) vout[off0(s)] = bv;
+          if (bbT) bbT[off0(s)] = b;
+        }
+        if (k0 & 0x80u) {
+          const int e = (1 + j + s) & 1, d = e ? 1 : -1;
+          const uint32_t ko = K0[rr1 * kSwWK + ck + d];
+          const uint32_t kym = K0[(rr1 - 2) * kSwWK + ck], kyp = K0[(rr1 + 2) * kSwWK + ck];
+          const uint32_t kxm = e ? c1k[1] : ko, kxp = e ? ko : c1k[1];
+          Coef<T> c;
+          sweep_coef<T, DDA>(op, s, k0, kxm, kxp, kym, kyp, c1k[0], c1k[2], off0(s), c);
+          const T dp = sub(gs_div(sub(T(0), b), c.dd), T(0));
+          nv = add(T(0), dp);
+        }
+      }
+      c0v[0] = c0v[1];
+      c0v[1] = c0v[2];
+      c0v[2] = nv;
+      c0k[0] = c0k[1];
+      c0k[1] = c0k[2];
+      c0k[2] = k0;
+      c0b[((s & 1) * kSwTJ + ty) * kSwTPX + tx] = nv;
+      if (owned && in && s >= kA && s <= kB) xout[off0(s)] = nv;
+    }
+    // phase B: colour 1 at plane s-1 (owned) from x = 0
+    const int sb = s - 1;
+    if (owned && sb >= kA) {
+      const uint32_t k1 = c1k[0];
+      T nv = T(0);
+      const bool in = in1(sb);
+      if (in) {
+        const TV bv = first_bb<VM>(a1, firstit, beta, omg, alpha);
+        const T b = (T)bv;
+        if (VM != 0) vout[off1(sb)] = bv;
+        if (bbT) bbT[off1(sb)] = b;
+        if (k1 & 0x80u) {
+          const int e = (j + sb) & 1, d = e ? 1 : -1;
+          const T* Cr = c0b + ((sb & 1) * kSwTJ + ty) * kSwTPX + tx;
+          const T xo = Cr[d];
+          const uint32_t ko = Km[rr0 * kSwWK + ck + d];
+          const T ym = Cr[-kSwTPX], yp = Cr[kSwTPX];
+          const uint32_t kym = Km[(rr0 - 2) * kSwWK + ck], kyp = Km[(rr0 + 2) * kSwWK + ck];
+          const T xm = e ? c0v[1] : xo, xp = e ? xo : c0v[1];
+          const uint32_t kxm = e ? c0k[1] : ko, kxp = e ? ko : c0k[1];
+          nv = sweep_update<T, DDA>(op, sb, k1, kxm, kxp, kym, kyp, c0k[0], c0k[2], off1(sb), T(0), b, xm, xp, ym,
+                                    yp, c0v[0], c0v[2]);
+        }
+        xout[off1(sb)] = nv;
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 3; ++u) {
+      a0[u] = n0[u];
+      a1[u] = n1[u];
+    }
+  }
+  if (abort && tid == 0) {
+    if (err) atomicExch(err, 1);
+    if (st) {
+      st->stop = 1;
+      st->reason = kTimeout;
+    }
+    for (int pl = waited + 1; pl <= issued; ++pl) mbar_wait_bounded(bar(pl), parity(pl), kDrainCycles);
+  }
+}
+
+// dynamic shared memory of k_rb_sweep_first<T, ...>
+template <typename T>
+constexpr int sweep_first_smem() {
+  return kSwStages * SwCfg<T>::KBYTES + SwCfg<T>::C0BYTES + 8 * kSwStages + 16;
+}
+
 }  // namespace h2g

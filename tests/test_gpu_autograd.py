@@ -1,7 +1,7 @@
 """The differentiable steady solve (h2_b200.autograd.HotspotNorm, a torch.autograd.Function over
 h2g_adjoint) on the 40x40x30 Mode-3 model: J and its gradients through backward() against central
 finite differences of GPU forward solves, and torch.autograd.gradcheck on a three-parameter
-restriction (one heat-source direction, one per-cell and one per-band log-conductivity direction).
+restriction (one heat-source direction and two log-conductivity directions, constant per z-band).
 Solves run to 1e-12, so the difference quotients carry about 1e-7 relative error."""
 import numpy as np
 import pytest
@@ -30,12 +30,17 @@ def problem():
 
 
 def _directions(m, seed):
+    """A heat-source direction on the silicon cells and a log-conductivity direction constant on
+    each z-band of the stack (the 13-parameter mapping; a field of per-cell values would exceed the
+    library's 127 distinct conductivities)."""
     rng = np.random.default_rng(seed)
     inner = (slice(1, -1),) * 3
     dh = np.zeros(m.shape)
     dh[inner] = rng.uniform(0.0, 1.0, (m.NX, m.NY, m.NZ)) * 1e10 * np.isin(m.ID[inner], (2, 7))
+    band = A.band_of_plane(m.ZC)
+    per_band = rng.uniform(-1.0, 1.0, A.NBANDS) * 0.1
     dl = np.zeros(m.shape)
-    dl[inner] = rng.uniform(-1.0, 1.0, (m.NX, m.NY, m.NZ)) * 0.1
+    dl[inner] = np.where(band >= 0, per_band[np.maximum(band, 0)], 0.0)[None, None, 1:-1]
     return dh, dl
 
 
