@@ -120,6 +120,8 @@ struct OpParams {
   const T* rc;         // rho*cp per cell (device layout), transient only
   const T* dzk;        // [MZ] dZ
   const T* ddv;        // dd per cell (device layout), precomputed with the tables; may be null
+  const T* tq;         // [MZ][P][256][4]: the four face tables of one (plane, own key, neighbour key)
+                       // side by side: x, y, z-, z+ (z+ from plane k+1), for the fused sweeps
   const unsigned long long* nkey;  // per cell: own key and the 6 neighbours' keys, one byte each
   T czm, czp;          // convective terms of the z-, z+ faces
   T dx0, dy0, ddt;

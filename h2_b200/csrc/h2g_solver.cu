@@ -89,6 +89,7 @@ struct OpTables {
   T* conv = nullptr;
   T* dzk = nullptr;
   T* ddv = nullptr;  // dd per cell (device layout)
+  T* tq = nullptr;   // interleaved x, y, z-, z+ tables (fused sweeps)
   int pcap = 0;
 };
 
@@ -471,6 +472,7 @@ static OpParams<T> op_params_rc(const Solver* s, const OpTables<T>& t, const T* 
   op.rc = rc;
   op.dzk = t.dzk;
   op.ddv = t.ddv;
+  op.tq = t.tq;
   op.nkey = s->nkey;
   const double dx0 = s->dx, dy0 = s->dy;
   op.czm = (T)((s->HC[4] * dx0) * dy0);
@@ -496,11 +498,11 @@ static OpParams<T> op_params(const Solver* s, const void* tables) {
 }
 
 static void free_tables64(OpTables<double>& t) {
-  cudaFree(t.tx); cudaFree(t.ty); cudaFree(t.tz); cudaFree(t.conv); cudaFree(t.dzk); cudaFree(t.ddv);
+  cudaFree(t.tx); cudaFree(t.ty); cudaFree(t.tz); cudaFree(t.conv); cudaFree(t.dzk); cudaFree(t.ddv); cudaFree(t.tq);
   t = OpTables<double>();
 }
 static void free_tables32(OpTables<float>& t) {
-  cudaFree(t.tx); cudaFree(t.ty); cudaFree(t.tz); cudaFree(t.conv); cudaFree(t.dzk); cudaFree(t.ddv);
+  cudaFree(t.tx); cudaFree(t.ty); cudaFree(t.tz); cudaFree(t.conv); cudaFree(t.dzk); cudaFree(t.ddv); cudaFree(t.tq);
   t = OpTables<float>();
 }
 
@@ -613,6 +615,7 @@ static int build_tables(Solver* s) {
     CK(cudaMalloc(&s->t64.conv, sizeof(double) * 4 * g.MZ));
     CK(cudaMalloc(&s->t64.dzk, sizeof(double) * g.MZ));
     CK(cudaMalloc(&s->t64.ddv, sizeof(double) * (size_t)g.n));
+    CK(cudaMalloc(&s->t64.tq, sizeof(double) * 4 * bytes_t));
     CK(cudaMemsetAsync(s->t64.ddv, 0, sizeof(double) * (size_t)g.n, s->stream));
     s->t64.pcap = pc;
     if (s->precision != H2G_FP64) {
@@ -622,10 +625,21 @@ static int build_tables(Solver* s) {
       CK(cudaMalloc(&s->t32.conv, sizeof(float) * 4 * g.MZ));
       CK(cudaMalloc(&s->t32.dzk, sizeof(float) * g.MZ));
       CK(cudaMalloc(&s->t32.ddv, sizeof(float) * (size_t)g.n));
+      CK(cudaMalloc(&s->t32.tq, sizeof(float) * 4 * bytes_t));
       CK(cudaMemsetAsync(s->t32.ddv, 0, sizeof(float) * (size_t)g.n, s->stream));
       s->t32.pcap = pc;
     }
   }
+  // the same values interleaved per (plane, own key, neighbour key byte): x, y, z-, z+ (the z+
+  // face of plane k is the z- table of plane k+1, zero above the last plane)
+  std::vector<double> tq(4 * bytes_t, 0.0);
+  for (size_t o = 0; o < bytes_t; ++o) {
+    tq[4 * o + 0] = tx[o];
+    tq[4 * o + 1] = ty[o];
+    tq[4 * o + 2] = tz[o];
+    tq[4 * o + 3] = o + lvl < bytes_t ? tz[o + lvl] : 0.0;
+  }
+  CK(cudaMemcpyAsync(s->t64.tq, tq.data(), sizeof(double) * 4 * bytes_t, cudaMemcpyHostToDevice, s->stream));
   CK(cudaMemcpyAsync(s->t64.tx, tx.data(), sizeof(double) * bytes_t, cudaMemcpyHostToDevice, s->stream));
   CK(cudaMemcpyAsync(s->t64.ty, ty.data(), sizeof(double) * bytes_t, cudaMemcpyHostToDevice, s->stream));
   CK(cudaMemcpyAsync(s->t64.tz, tz.data(), sizeof(double) * bytes_t, cudaMemcpyHostToDevice, s->stream));
@@ -637,7 +651,8 @@ static int build_tables(Solver* s) {
       for (size_t i = 0; i < v.size(); ++i) o[i] = (float)v[i];
       return o;
     };
-    std::vector<float> fx = to32(tx), fy = to32(ty), fz = to32(tz), fc = to32(conv), fd = to32(s->dZ);
+    std::vector<float> fx = to32(tx), fy = to32(ty), fz = to32(tz), fc = to32(conv), fd = to32(s->dZ), fq = to32(tq);
+    CK(cudaMemcpyAsync(s->t32.tq, fq.data(), sizeof(float) * 4 * bytes_t, cudaMemcpyHostToDevice, s->stream));
     CK(cudaMemcpyAsync(s->t32.tx, fx.data(), sizeof(float) * bytes_t, cudaMemcpyHostToDevice, s->stream));
     CK(cudaMemcpyAsync(s->t32.ty, fy.data(), sizeof(float) * bytes_t, cudaMemcpyHostToDevice, s->stream));
     CK(cudaMemcpyAsync(s->t32.tz, fz.data(), sizeof(float) * bytes_t, cudaMemcpyHostToDevice, s->stream));

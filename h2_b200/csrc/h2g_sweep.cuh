@@ -94,22 +94,23 @@ __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map
 
 __device__ __forceinline__ int align_down(int v, int a) { return v >= 0 ? v - v % a : -((-v + a - 1) / a) * a; }
 
-// Coefficients of one unmasked cell from its own and its six neighbours' key bytes: the table
-// look-ups of cell_coef, and dd either read (DDA) or summed in NonUniform.jl:501-502's order.  In
-// a steady grid whose cell has six unmasked neighbours every convective term and a_p0 are +0, and
-// adding +0 to the non-negative partial sum changes no bit, so dd is the sum of the six
-// conductances; otherwise the full 13-term chain runs.
+// Coefficients of one unmasked cell from its own and its six neighbours' key bytes, from the
+// interleaved table: `row` is the (plane k, own key) row, whose entry for a neighbour key byte nb
+// holds the x, y, z- and z+ conductances side by side (one multiply-add and one load per face).
+// dd is read (DDA) or summed in NonUniform.jl:501-502's order.  In a steady grid whose cell has six
+// unmasked neighbours every convective term and a_p0 are +0, and adding +0 to the non-negative
+// partial sum changes no bit, so dd is the sum of the six conductances; otherwise the full 13-term
+// chain runs.
 template <typename T, bool DDA>
-__device__ __forceinline__ void sweep_coef(const OpParams<T>& op, int k, uint32_t k0, uint32_t kxm, uint32_t kxp,
-                                           uint32_t kym, uint32_t kyp, uint32_t kzm, uint32_t kzp, int ci,
-                                           Coef<T>& c) {
-  const int bx = (k * op.P + (int)(k0 & 0x7f)) << 8;
-  c.cxm = __ldg(op.tx + (bx | kxm));
-  c.cxp = __ldg(op.tx + (bx | kxp));
-  c.cym = __ldg(op.ty + (bx | kym));
-  c.cyp = __ldg(op.ty + (bx | kyp));
-  c.czm = __ldg(op.tz + (bx | kzm));
-  c.czp = __ldg(op.tz + ((bx + (op.P << 8)) | kzp));
+__device__ __forceinline__ void sweep_coef(const OpParams<T>& op, const T* __restrict__ row, int k, uint32_t kxm,
+                                           uint32_t kxp, uint32_t kym, uint32_t kyp, uint32_t kzm, uint32_t kzp,
+                                           int ci, Coef<T>& c) {
+  c.cxm = __ldg(row + 4 * kxm);
+  c.cxp = __ldg(row + 4 * kxp);
+  c.cym = __ldg(row + 4 * kym + 1);
+  c.cyp = __ldg(row + 4 * kyp + 1);
+  c.czm = __ldg(row + 4 * kzm + 2);
+  c.czp = __ldg(row + 4 * kzp + 3);
   if constexpr (DDA) {
     c.dd = __ldg(op.ddv + ci);
     return;
@@ -142,17 +143,60 @@ __device__ __forceinline__ void sweep_coef(const OpParams<T>& op, int k, uint32_
   c.dd = add(T(0), s);
 }
 
+// the (plane k, own key) row of the interleaved table
+template <typename T>
+__device__ __forceinline__ const T* coef_row(const OpParams<T>& op, int kP, uint32_t k0) {
+  return op.tq + ((size_t)(kP + (int)(k0 & 0x7f)) << 10);
+}
+
 // Gauss-Seidel update of one cell with omega = 1 (NonUniform.jl:903-905): x + ((ss - b)/dd - x).
 template <typename T, bool DDA>
-__device__ __forceinline__ T sweep_update(const OpParams<T>& op, int k, uint32_t k0, uint32_t kxm, uint32_t kxp,
-                                          uint32_t kym, uint32_t kyp, uint32_t kzm, uint32_t kzp, int ci, T pp, T b,
-                                          T xm, T xp, T ym, T yp, T zm, T zp) {
+__device__ __forceinline__ T sweep_update(const OpParams<T>& op, int k, int kP, uint32_t k0, uint32_t kxm,
+                                          uint32_t kxp, uint32_t kym, uint32_t kyp, uint32_t kzm, uint32_t kzp, int ci,
+                                          T pp, T b, T xm, T xp, T ym, T yp, T zm, T zp) {
   Coef<T> c;
-  sweep_coef<T, DDA>(op, k, k0, kxm, kxp, kym, kyp, kzm, kzp, ci, c);
+  sweep_coef<T, DDA>(op, coef_row(op, kP, k0), k, kxm, kxp, kym, kyp, kzm, kzp, ci, c);
   const T ss = nb_sum(c, xp, xm, yp, ym, zp, zm);
   const T dp = sub(gs_div(sub(ss, b), c.dd), pp);
   return relax(pp, T(1), dp);
 }
+
+// Per-thread geometry of a sweep block, computed once: the thread's column (p, j), its offsets in
+// the staged boxes and in the device layout, which of its two cells of a row are interior, and the
+// ring slots of the planes the current step uses (advanced one plane per step).
+struct SweepThread {
+  int p, j, tx, ty;
+  bool owned;
+  bool ok_even, ok_odd;  // interior cell at i = 2p (even) / i = 2p + 1 (odd), row j interior
+  int par;               // parity of colour 0 at plane 0: e0(s) = par ^ (s & 1)
+  int g0;                // offset of colour 0 of (p, j) within a plane; colour 1 is + HP
+  int c0off;             // this thread's entry of one plane of the colour-0 exchange buffer
+  __device__ __forceinline__ bool in0(int s, int NZ) const {
+    return s >= 1 && s <= NZ && ((par ^ (s & 1)) ? ok_odd : ok_even);
+  }
+  __device__ __forceinline__ bool in1(int s, int NZ) const {
+    return s >= 1 && s <= NZ && ((par ^ (s & 1)) ? ok_even : ok_odd);
+  }
+};
+
+__device__ __forceinline__ SweepThread sweep_thread(const Geo& g) {
+  SweepThread t;
+  t.tx = threadIdx.x;
+  t.ty = threadIdx.y;
+  const int q0 = (int)blockIdx.x * (kSwTPX - 2) - 1, r0 = (int)blockIdx.y * (kSwTJ - 2);
+  t.p = q0 + t.tx;
+  t.j = r0 + t.ty;
+  t.owned = t.tx >= 1 && t.tx < kSwTPX - 1 && t.ty >= 1 && t.ty < kSwTJ - 1;
+  const bool jin = t.j >= 1 && t.j <= g.NY && t.p >= 0;
+  t.ok_even = jin && 2 * t.p >= 1 && 2 * t.p <= g.NX;
+  t.ok_odd = jin && 2 * t.p + 1 <= g.NX;
+  t.par = (1 + t.j) & 1;
+  t.g0 = (t.j * 2) * g.HP + t.p;
+  t.c0off = t.ty * kSwTPX + t.tx;
+  return t;
+}
+
+__device__ __forceinline__ int next_slot(int q) { return q == kSwStages - 1 ? 0 : q + 1; }
 
 // One sweep: xout = RB-GS sweep of the x that tmx maps, with right-hand side bb.
 // Grid: (ceil(HI / (TPX-2)), ceil(NY / (TJ-2)), ceil(NZ / kc)); block (kSwTPX, kSwTJ); dynamic
@@ -167,45 +211,30 @@ __global__ void __launch_bounds__(kSwThreads, 1)
   if (st && st->stop) return;
   extern __shared__ __align__(128) unsigned char sm[];
   const Geo& g = op.g;
-  const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + kSwTPX * ty;
+  const SweepThread t = sweep_thread(g);
+  const int tid = t.tx + kSwTPX * t.ty;
   const int q0 = (int)blockIdx.x * (kSwTPX - 2) - 1, r0 = (int)blockIdx.y * (kSwTJ - 2);
-  const int p = q0 + tx, j = r0 + ty;
   const int kA = 1 + (int)blockIdx.z * kc, kB = min(kA + kc - 1, g.NZ);
   const int xs = align_down(q0 - 1, C::A), xk = align_down(q0 - 1, 16), ys = 2 * (r0 - 1);
   const int first = kA - 2, last = kB + 2;  // staged planes
-  const bool owned = tx >= 1 && tx < kSwTPX - 1 && ty >= 1 && ty < kSwTJ - 1;
-  const bool jin = j >= 1 && j <= g.NY && p >= 0;
-  const int cx = p - xs, ck = p - xk;  // this column in the x / key boxes
-  const int rr0 = 2 * (ty + 1), rr1 = rr0 + 1;
+  // this column's colour-0 / colour-1 entries in the staged boxes
+  const int oX0 = (2 * (t.ty + 1)) * C::WX + (t.p - xs), oX1 = oX0 + C::WX;
+  const int oK0 = (2 * (t.ty + 1)) * kSwWK + (t.p - xk), oK1 = oK0 + kSwWK;
   T* c0b = reinterpret_cast<T*>(sm + kSwStages * C::STAGE);
   volatile int* flag = reinterpret_cast<volatile int*>(sm + C::BAR_OFF + 8 * kSwStages);
   const uint32_t bar0 = smem_u32(sm + C::BAR_OFF);
-  auto xbox = [&](int plane) {
-    return reinterpret_cast<const T*>(sm + ((plane - first) % kSwStages) * C::STAGE);
-  };
-  auto kbox = [&](int plane) {
-    return reinterpret_cast<const uint8_t*>(sm + ((plane - first) % kSwStages) * C::STAGE + C::XBYTES);
-  };
-  auto bar = [&](int plane) { return bar0 + 8u * (uint32_t)((plane - first) % kSwStages); };
-  auto parity = [&](int plane) { return (uint32_t)(((plane - first) / kSwStages) & 1); };
-  auto issue = [&](int plane) {  // thread 0
-    const int q = (plane - first) % kSwStages;
+  auto xbox = [&](int q) { return reinterpret_cast<const T*>(sm + q * C::STAGE); };
+  auto kbox = [&](int q) { return reinterpret_cast<const uint8_t*>(sm + q * C::STAGE + C::XBYTES); };
+  auto issue = [&](int plane, int q) {  // thread 0
     const uint32_t b = bar0 + 8u * q;
     mbar_expect_tx(b, (uint32_t)C::STAGE);
     tma_load_3d(smem_u32(sm + q * C::STAGE), &tmx, xs, ys, plane, b);
     tma_load_3d(smem_u32(sm + q * C::STAGE + C::XBYTES), &tmk, xk, ys, plane, b);
   };
-  // colour-0 / colour-1 cells of this column at plane k, interior and inside the grid
-  auto in0 = [&](int k) {
-    const int i = 2 * p + ((1 + j + k) & 1);
-    return jin && k >= 1 && k <= g.NZ && i >= 1 && i <= g.NX;
+  auto wait = [&](int plane) {  // thread 0, bounded
+    const int u = plane - first;
+    return mbar_wait_bounded(bar0 + 8u * (u % kSwStages), (uint32_t)((u / kSwStages) & 1), wait_limit);
   };
-  auto in1 = [&](int k) {
-    const int i = 2 * p + ((j + k) & 1);
-    return jin && k >= 1 && k <= g.NZ && i >= 1 && i <= g.NX;
-  };
-  auto off0 = [&](int k) { return g.row(0, j, k) + p; };
-  auto off1 = [&](int k) { return g.row(1, j, k) + p; };
 
   int issued = first - 1, waited = first - 1;  // thread 0's bookkeeping
   if (tid == 0) {
@@ -213,31 +242,34 @@ __global__ void __launch_bounds__(kSwThreads, 1)
     mbar_fence_init();
     *flag = 0;
     for (int pl = first; pl <= min(first + kSwStages - 2, last); ++pl) {
-      issue(pl);
+      issue(pl, pl - first);
       issued = pl;
     }
-    if (mbar_wait_bounded(bar(first), parity(first), wait_limit)) waited = first;
-    if (waited == first && mbar_wait_bounded(bar(first + 1), parity(first + 1), wait_limit)) waited = first + 1;
+    if (wait(first)) waited = first;
+    if (waited == first && wait(first + 1)) waited = first + 1;
     if (waited != first + 1) *flag = 1;
   }
   __syncthreads();
   bool abort = *flag != 0;
 
+  // ring slots of planes s-1, s, s+1 and of the plane issued at this step (s+3)
+  int qm = 0, q0s = 1, qp = 2, qi = 4;
   // windows along z of this column: colour-1 old values and keys at planes s-1, s, s+1; colour-0
   // new values and keys at planes s-2, s-1, s (after the shift at the top of step s)
   T c1v[3] = {T(0), T(0), T(0)}, c0v[3] = {T(0), T(0), T(0)};
   uint32_t c1k[3] = {0u, 0u, 0u}, c0k[3] = {0u, 0u, 0u};
   T b0 = T(0), b1 = T(0);
+  int pofs = (kA - 1) * (int)g.plane;  // s * plane at the current step
   if (!abort) {
-    c1v[1] = xbox(first)[rr1 * C::WX + cx];
-    c1k[1] = kbox(first)[rr1 * kSwWK + ck];
-    c1v[2] = xbox(first + 1)[rr1 * C::WX + cx];
-    c1k[2] = kbox(first + 1)[rr1 * kSwWK + ck];
-    if (in0(kA - 1)) b0 = __ldg(bb + off0(kA - 1));
+    c1v[1] = xbox(0)[oX1];
+    c1k[1] = kbox(0)[oK1];
+    c1v[2] = xbox(1)[oX1];
+    c1k[2] = kbox(1)[oK1];
+    if (t.in0(kA - 1, g.NZ)) b0 = __ldg(bb + pofs + t.g0);
   }
-  for (int s = kA - 1; s <= kB + 1 && !abort; ++s) {
+  for (int s = kA - 1; s <= kB + 1 && !abort; ++s, pofs += (int)g.plane) {
     if (tid == 0) {
-      if (mbar_wait_bounded(bar(s + 1), parity(s + 1), wait_limit)) waited = s + 1;
+      if (wait(s + 1)) waited = s + 1;
       else *flag = 1;
     }
     __syncthreads();  // step s-1 done everywhere; plane s+1 staged
@@ -246,39 +278,39 @@ __global__ void __launch_bounds__(kSwThreads, 1)
       break;
     }
     if (tid == 0 && s + 3 <= last) {  // the slot of plane s-2 is free now
-      issue(s + 3);
+      issue(s + 3, qi);
       issued = s + 3;
     }
-    const T* X0 = xbox(s);
-    const uint8_t* K0 = kbox(s);
-    const uint8_t* Km = kbox(s - 1);
+    const T* X0 = xbox(q0s);
+    const uint8_t* K0 = kbox(q0s);
+    const uint8_t* Km = kbox(qm);
     c1v[0] = c1v[1];
     c1v[1] = c1v[2];
-    c1v[2] = xbox(s + 1)[rr1 * C::WX + cx];
+    c1v[2] = xbox(qp)[oX1];
     c1k[0] = c1k[1];
     c1k[1] = c1k[2];
-    c1k[2] = kbox(s + 1)[rr1 * kSwWK + ck];
+    c1k[2] = kbox(qp)[oK1];
+    const bool mid = s >= kA && s <= kB;
     // right-hand sides of the next step, in flight during this one
-    const bool do1 = owned && s >= kA && s <= kB;  // phase B of the next step (plane s)
     T nb0 = T(0), nb1 = T(0);
-    if (s <= kB && in0(s + 1)) nb0 = __ldg(bb + off0(s + 1));
-    if (do1 && in1(s)) nb1 = __ldg(bb + off1(s));
+    if (s <= kB && t.in0(s + 1, g.NZ)) nb0 = __ldg(bb + pofs + (int)g.plane + t.g0);
+    if (t.owned && mid && t.in1(s, g.NZ)) nb1 = __ldg(bb + pofs + t.g0 + g.HP);
+    const int e0 = t.par ^ (s & 1);  // colour 0 at plane s sits at i = 2p + e0
+    const int d0 = e0 ? 1 : -1;
 
     // phase A: colour 0 at plane s (tile and overlap)
     {
-      const T pp = X0[rr0 * C::WX + cx];
-      const uint32_t k0 = K0[rr0 * kSwWK + ck];
+      const T pp = X0[oX0];
+      const uint32_t k0 = K0[oK0];
       T nv = pp;
-      const bool in = in0(s);
+      const bool in = t.in0(s, g.NZ);
       if (in && (k0 & 0x80u)) {
-        const int e = (1 + j + s) & 1, d = e ? 1 : -1;
-        const T xo = X0[rr1 * C::WX + cx + d];
-        const uint32_t ko = K0[rr1 * kSwWK + ck + d];
-        const T ym = X0[(rr1 - 2) * C::WX + cx], yp = X0[(rr1 + 2) * C::WX + cx];
-        const uint32_t kym = K0[(rr1 - 2) * kSwWK + ck], kyp = K0[(rr1 + 2) * kSwWK + ck];
-        const T xm = e ? c1v[1] : xo, xp = e ? xo : c1v[1];
-        const uint32_t kxm = e ? c1k[1] : ko, kxp = e ? ko : c1k[1];
-        nv = sweep_update<T, DDA>(op, s, k0, kxm, kxp, kym, kyp, c1k[0], c1k[2], off0(s), pp, b0, xm, xp, ym, yp,
+        const T xo = X0[oX1 + d0];
+        const uint32_t ko = K0[oK1 + d0];
+        const T xm = e0 ? c1v[1] : xo, xp = e0 ? xo : c1v[1];
+        const uint32_t kxm = e0 ? c1k[1] : ko, kxp = e0 ? ko : c1k[1];
+        nv = sweep_update<T, DDA>(op, s, s * op.P, k0, kxm, kxp, K0[oK1 - 2 * kSwWK], K0[oK1 + 2 * kSwWK], c1k[0],
+                                  c1k[2], pofs + t.g0, pp, b0, xm, xp, X0[oX1 - 2 * C::WX], X0[oX1 + 2 * C::WX],
                                   c1v[0], c1v[2]);
       }
       c0v[0] = c0v[1];
@@ -287,32 +319,37 @@ __global__ void __launch_bounds__(kSwThreads, 1)
       c0k[0] = c0k[1];
       c0k[1] = c0k[2];
       c0k[2] = k0;
-      c0b[((s & 1) * kSwTJ + ty) * kSwTPX + tx] = nv;
-      if (owned && in && s >= kA && s <= kB) xout[off0(s)] = nv;
+      c0b[(s & 1) * (kSwTJ * kSwTPX) + t.c0off] = nv;
+      if (t.owned && in && mid) xout[pofs + t.g0] = nv;
     }
     // phase B: colour 1 at plane s-1 (owned cells), its colour-0 neighbours from step s-1
     const int sb = s - 1;
-    if (owned && sb >= kA) {
+    if (t.owned && sb >= kA) {
       const T pp = c1v[0];
       const uint32_t k1 = c1k[0];
       T nv = pp;
-      const bool in = in1(sb);
+      const int pb = pofs - (int)g.plane;
+      const bool in = t.in1(sb, g.NZ);
       if (in && (k1 & 0x80u)) {
-        const int e = (j + sb) & 1, d = e ? 1 : -1;
-        const T* Cr = c0b + ((sb & 1) * kSwTJ + ty) * kSwTPX + tx;
-        const T xo = Cr[d];
-        const uint32_t ko = Km[rr0 * kSwWK + ck + d];
-        const T ym = Cr[-kSwTPX], yp = Cr[kSwTPX];
-        const uint32_t kym = Km[(rr0 - 2) * kSwWK + ck], kyp = Km[(rr0 + 2) * kSwWK + ck];
-        const T xm = e ? c0v[1] : xo, xp = e ? xo : c0v[1];
-        const uint32_t kxm = e ? c0k[1] : ko, kxp = e ? ko : c0k[1];
-        nv = sweep_update<T, DDA>(op, sb, k1, kxm, kxp, kym, kyp, c0k[0], c0k[2], off1(sb), pp, b1, xm, xp, ym, yp,
-                                  c0v[0], c0v[2]);
+        const int e1 = e0;  // colour 1 at plane s-1 sits at i = 2p + e0
+        const int d1 = e1 ? 1 : -1;
+        const T* Cr = c0b + (sb & 1) * (kSwTJ * kSwTPX) + t.c0off;
+        const T xo = Cr[d1];
+        const uint32_t ko = Km[oK0 + d1];
+        const T xm = e1 ? c0v[1] : xo, xp = e1 ? xo : c0v[1];
+        const uint32_t kxm = e1 ? c0k[1] : ko, kxp = e1 ? ko : c0k[1];
+        nv = sweep_update<T, DDA>(op, sb, sb * op.P, k1, kxm, kxp, Km[oK0 - 2 * kSwWK], Km[oK0 + 2 * kSwWK], c0k[0],
+                                  c0k[2], pb + t.g0 + g.HP, pp, b1, xm, xp, Cr[-kSwTPX], Cr[kSwTPX], c0v[0],
+                                  c0v[2]);
       }
-      if (in) xout[off1(sb)] = nv;
+      if (in) xout[pb + t.g0 + g.HP] = nv;
     }
     b0 = nb0;
     b1 = nb1;
+    qm = q0s;
+    q0s = qp;
+    qp = next_slot(qp);
+    qi = next_slot(qi);
   }
   if (abort && tid == 0) {
     // a wait ran out: report it, then let the copies still in flight land before the block's
@@ -322,7 +359,10 @@ __global__ void __launch_bounds__(kSwThreads, 1)
       st->stop = 1;
       st->reason = kTimeout;
     }
-    for (int pl = waited + 1; pl <= issued; ++pl) mbar_wait_bounded(bar(pl), parity(pl), kDrainCycles);
+    for (int pl = waited + 1; pl <= issued; ++pl) {
+      const int u = pl - first;
+      mbar_wait_bounded(bar0 + 8u * (u % kSwStages), (uint32_t)((u / kSwStages) & 1), kDrainCycles);
+    }
   }
 }
 
@@ -362,43 +402,29 @@ __global__ void __launch_bounds__(kSwThreads, 1)
   if (st && st->stop) return;
   extern __shared__ __align__(128) unsigned char sm[];
   const Geo& g = op.g;
-  const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + kSwTPX * ty;
+  const SweepThread t = sweep_thread(g);
+  const int tid = t.tx + kSwTPX * t.ty;
   const int q0 = (int)blockIdx.x * (kSwTPX - 2) - 1, r0 = (int)blockIdx.y * (kSwTJ - 2);
-  const int p = q0 + tx, j = r0 + ty;
   const int kA = 1 + (int)blockIdx.z * kc, kB = min(kA + kc - 1, g.NZ);
   const int xk = align_down(q0 - 1, 16), ys = 2 * (r0 - 1);
   const int first = kA - 2, last = kB + 2;
-  const bool owned = tx >= 1 && tx < kSwTPX - 1 && ty >= 1 && ty < kSwTJ - 1;
-  const bool jin = j >= 1 && j <= g.NY && p >= 0;
-  const int ck = p - xk;
-  const int rr0 = 2 * (ty + 1), rr1 = rr0 + 1;
+  const int oK0 = (2 * (t.ty + 1)) * kSwWK + (t.p - xk), oK1 = oK0 + kSwWK;
   // shared memory: kSwStages key planes, then the colour-0 exchange buffer, then the barriers
   constexpr int KOFF = kSwStages * C::KBYTES;
   T* c0b = reinterpret_cast<T*>(sm + KOFF);
-  const int BOFF = KOFF + C::C0BYTES;
+  constexpr int BOFF = KOFF + C::C0BYTES;
   volatile int* flag = reinterpret_cast<volatile int*>(sm + BOFF + 8 * kSwStages);
   const uint32_t bar0 = smem_u32(sm + BOFF);
-  auto kbox = [&](int plane) {
-    return reinterpret_cast<const uint8_t*>(sm + ((plane - first) % kSwStages) * C::KBYTES);
-  };
-  auto bar = [&](int plane) { return bar0 + 8u * (uint32_t)((plane - first) % kSwStages); };
-  auto parity = [&](int plane) { return (uint32_t)(((plane - first) / kSwStages) & 1); };
-  auto issue = [&](int plane) {
-    const int qq = (plane - first) % kSwStages;
+  auto kbox = [&](int qq) { return reinterpret_cast<const uint8_t*>(sm + qq * C::KBYTES); };
+  auto issue = [&](int plane, int qq) {
     const uint32_t b = bar0 + 8u * qq;
     mbar_expect_tx(b, (uint32_t)C::KBYTES);
     tma_load_3d(smem_u32(sm + qq * C::KBYTES), &tmk, xk, ys, plane, b);
   };
-  auto in0 = [&](int k) {
-    const int i = 2 * p + ((1 + j + k) & 1);
-    return jin && k >= 1 && k <= g.NZ && i >= 1 && i <= g.NX;
+  auto wait = [&](int plane) {
+    const int u = plane - first;
+    return mbar_wait_bounded(bar0 + 8u * (u % kSwStages), (uint32_t)((u / kSwStages) & 1), wait_limit);
   };
-  auto in1 = [&](int k) {
-    const int i = 2 * p + ((j + k) & 1);
-    return jin && k >= 1 && k <= g.NZ && i >= 1 && i <= g.NX;
-  };
-  auto off0 = [&](int k) { return g.row(0, j, k) + p; };
-  auto off1 = [&](int k) { return g.row(1, j, k) + p; };
   int firstit = 0;
   TV beta = TV(0), omg = TV(0), alpha = TV(0);
   if (VM == 1) {
@@ -415,27 +441,29 @@ __global__ void __launch_bounds__(kSwThreads, 1)
     mbar_fence_init();
     *flag = 0;
     for (int pl = first; pl <= min(first + kSwStages - 2, last); ++pl) {
-      issue(pl);
+      issue(pl, pl - first);
       issued = pl;
     }
-    if (mbar_wait_bounded(bar(first), parity(first), wait_limit)) waited = first;
-    if (waited == first && mbar_wait_bounded(bar(first + 1), parity(first + 1), wait_limit)) waited = first + 1;
+    if (wait(first)) waited = first;
+    if (waited == first && wait(first + 1)) waited = first + 1;
     if (waited != first + 1) *flag = 1;
   }
   __syncthreads();
   bool abort = *flag != 0;
 
+  int qm = 0, q0s = 1, qp = 2, qi = 4;
   T c0v[3] = {T(0), T(0), T(0)};
   uint32_t c1k[3] = {0u, 0u, 0u}, c0k[3] = {0u, 0u, 0u};
   TV a0[3] = {TV(0), TV(0), TV(0)}, a1[3] = {TV(0), TV(0), TV(0)};  // raw operands of bb, a step ahead
+  int pofs = (kA - 1) * (int)g.plane;
   if (!abort) {
-    c1k[1] = kbox(first)[rr1 * kSwWK + ck];
-    c1k[2] = kbox(first + 1)[rr1 * kSwWK + ck];
-    if (in0(kA - 1)) first_load<T, TV, VM>(vin, r, q, off0(kA - 1), a0);
+    c1k[1] = kbox(0)[oK1];
+    c1k[2] = kbox(1)[oK1];
+    if (t.in0(kA - 1, g.NZ)) first_load<T, TV, VM>(vin, r, q, pofs + t.g0, a0);
   }
-  for (int s = kA - 1; s <= kB + 1 && !abort; ++s) {
+  for (int s = kA - 1; s <= kB + 1 && !abort; ++s, pofs += (int)g.plane) {
     if (tid == 0) {
-      if (mbar_wait_bounded(bar(s + 1), parity(s + 1), wait_limit)) waited = s + 1;
+      if (wait(s + 1)) waited = s + 1;
       else *flag = 1;
     }
     __syncthreads();
@@ -444,38 +472,39 @@ __global__ void __launch_bounds__(kSwThreads, 1)
       break;
     }
     if (tid == 0 && s + 3 <= last) {
-      issue(s + 3);
+      issue(s + 3, qi);
       issued = s + 3;
     }
-    const uint8_t* K0 = kbox(s);
-    const uint8_t* Km = kbox(s - 1);
+    const uint8_t* K0 = kbox(q0s);
+    const uint8_t* Km = kbox(qm);
     c1k[0] = c1k[1];
     c1k[1] = c1k[2];
-    c1k[2] = kbox(s + 1)[rr1 * kSwWK + ck];
-    const bool do1 = owned && s >= kA && s <= kB;
+    c1k[2] = kbox(qp)[oK1];
+    const bool mid = s >= kA && s <= kB;
     TV n0[3] = {TV(0), TV(0), TV(0)}, n1[3] = {TV(0), TV(0), TV(0)};
-    if (s <= kB && in0(s + 1)) first_load<T, TV, VM>(vin, r, q, off0(s + 1), n0);
-    if (do1 && in1(s)) first_load<T, TV, VM>(vin, r, q, off1(s), n1);
+    if (s <= kB && t.in0(s + 1, g.NZ)) first_load<T, TV, VM>(vin, r, q, pofs + (int)g.plane + t.g0, n0);
+    if (t.owned && mid && t.in1(s, g.NZ)) first_load<T, TV, VM>(vin, r, q, pofs + t.g0 + g.HP, n1);
+    const int e0 = t.par ^ (s & 1);
+    const int d0 = e0 ? 1 : -1;
 
     // phase A: colour 0 at plane s from x = 0: ((0 - bb)/dd - 0), then 0 + that
     {
-      const uint32_t k0 = K0[rr0 * kSwWK + ck];
+      const uint32_t k0 = K0[oK0];
       T nv = T(0);
-      const bool in = in0(s);
+      const bool in = t.in0(s, g.NZ);
       if (in) {
         const TV bv = first_bb<VM>(a0, firstit, beta, omg, alpha);
         const T b = (T)bv;
-        if (owned && s >= kA && s <= kB) {
-          if (VM != 0) vout[off0(s)] = bv;
-          if (bbT) bbT[off0(s)] = b;
+        if (t.owned && mid) {
+          if (VM != 0) vout[pofs + t.g0] = bv;
+          if (bbT) bbT[pofs + t.g0] = b;
         }
         if (k0 & 0x80u) {
-          const int e = (1 + j + s) & 1, d = e ? 1 : -1;
-          const uint32_t ko = K0[rr1 * kSwWK + ck + d];
-          const uint32_t kym = K0[(rr1 - 2) * kSwWK + ck], kyp = K0[(rr1 + 2) * kSwWK + ck];
-          const uint32_t kxm = e ? c1k[1] : ko, kxp = e ? ko : c1k[1];
+          const uint32_t ko = K0[oK1 + d0];
+          const uint32_t kxm = e0 ? c1k[1] : ko, kxp = e0 ? ko : c1k[1];
           Coef<T> c;
-          sweep_coef<T, DDA>(op, s, k0, kxm, kxp, kym, kyp, c1k[0], c1k[2], off0(s), c);
+          sweep_coef<T, DDA>(op, coef_row(op, s * op.P, k0), s, kxm, kxp, K0[oK1 - 2 * kSwWK], K0[oK1 + 2 * kSwWK],
+                             c1k[0], c1k[2], pofs + t.g0, c);
           const T dp = sub(gs_div(sub(T(0), b), c.dd), T(0));
           nv = add(T(0), dp);
         }
@@ -486,33 +515,34 @@ __global__ void __launch_bounds__(kSwThreads, 1)
       c0k[0] = c0k[1];
       c0k[1] = c0k[2];
       c0k[2] = k0;
-      c0b[((s & 1) * kSwTJ + ty) * kSwTPX + tx] = nv;
-      if (owned && in && s >= kA && s <= kB) xout[off0(s)] = nv;
+      c0b[(s & 1) * (kSwTJ * kSwTPX) + t.c0off] = nv;
+      if (t.owned && in && mid) xout[pofs + t.g0] = nv;
     }
     // phase B: colour 1 at plane s-1 (owned) from x = 0
     const int sb = s - 1;
-    if (owned && sb >= kA) {
+    if (t.owned && sb >= kA) {
       const uint32_t k1 = c1k[0];
       T nv = T(0);
-      const bool in = in1(sb);
+      const int pb = pofs - (int)g.plane;
+      const bool in = t.in1(sb, g.NZ);
       if (in) {
         const TV bv = first_bb<VM>(a1, firstit, beta, omg, alpha);
         const T b = (T)bv;
-        if (VM != 0) vout[off1(sb)] = bv;
-        if (bbT) bbT[off1(sb)] = b;
+        if (VM != 0) vout[pb + t.g0 + g.HP] = bv;
+        if (bbT) bbT[pb + t.g0 + g.HP] = b;
         if (k1 & 0x80u) {
-          const int e = (j + sb) & 1, d = e ? 1 : -1;
-          const T* Cr = c0b + ((sb & 1) * kSwTJ + ty) * kSwTPX + tx;
-          const T xo = Cr[d];
-          const uint32_t ko = Km[rr0 * kSwWK + ck + d];
-          const T ym = Cr[-kSwTPX], yp = Cr[kSwTPX];
-          const uint32_t kym = Km[(rr0 - 2) * kSwWK + ck], kyp = Km[(rr0 + 2) * kSwWK + ck];
-          const T xm = e ? c0v[1] : xo, xp = e ? xo : c0v[1];
-          const uint32_t kxm = e ? c0k[1] : ko, kxp = e ? ko : c0k[1];
-          nv = sweep_update<T, DDA>(op, sb, k1, kxm, kxp, kym, kyp, c0k[0], c0k[2], off1(sb), T(0), b, xm, xp, ym,
-                                    yp, c0v[0], c0v[2]);
+          const int e1 = e0;  // colour 1 at plane s-1 sits at i = 2p + e0
+          const int d1 = e1 ? 1 : -1;
+          const T* Cr = c0b + (sb & 1) * (kSwTJ * kSwTPX) + t.c0off;
+          const T xo = Cr[d1];
+          const uint32_t ko = Km[oK0 + d1];
+          const T xm = e1 ? c0v[1] : xo, xp = e1 ? xo : c0v[1];
+          const uint32_t kxm = e1 ? c0k[1] : ko, kxp = e1 ? ko : c0k[1];
+          nv = sweep_update<T, DDA>(op, sb, sb * op.P, k1, kxm, kxp, Km[oK0 - 2 * kSwWK], Km[oK0 + 2 * kSwWK],
+                                    c0k[0], c0k[2], pb + t.g0 + g.HP, T(0), b, xm, xp, Cr[-kSwTPX], Cr[kSwTPX],
+                                    c0v[0], c0v[2]);
         }
-        xout[off1(sb)] = nv;
+        xout[pb + t.g0 + g.HP] = nv;
       }
     }
 #pragma unroll
@@ -520,6 +550,10 @@ __global__ void __launch_bounds__(kSwThreads, 1)
       a0[u] = n0[u];
       a1[u] = n1[u];
     }
+    qm = q0s;
+    q0s = qp;
+    qp = next_slot(qp);
+    qi = next_slot(qi);
   }
   if (abort && tid == 0) {
     if (err) atomicExch(err, 1);
@@ -527,7 +561,10 @@ __global__ void __launch_bounds__(kSwThreads, 1)
       st->stop = 1;
       st->reason = kTimeout;
     }
-    for (int pl = waited + 1; pl <= issued; ++pl) mbar_wait_bounded(bar(pl), parity(pl), kDrainCycles);
+    for (int pl = waited + 1; pl <= issued; ++pl) {
+      const int u = pl - first;
+      mbar_wait_bounded(bar0 + 8u * (u % kSwStages), (uint32_t)((u / kSwStages) & 1), kDrainCycles);
+    }
   }
 }
 
