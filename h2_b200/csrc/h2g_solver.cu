@@ -166,7 +166,6 @@ struct Solver {
   bool rb_fused = false;   // autotuned
   int sw_chunks = 1;       // z chunks of the fused sweep's grid (autotuned)
   bool sw_dda = false;     // the fused sweep reads dd from the array (autotuned)
-  int sw_r = 2;            // rows per thread of the fused sweep, 1 or 2 (autotuned)
   int sweep_forced = -1;   // h2g_set_sweep: -1 tuner, 0 colour passes, 1 fused
   double* x2_64 = nullptr;
   float* x2_32 = nullptr;
@@ -328,15 +327,11 @@ static int sweep_attrs() {
   static std::once_flag once;
   static cudaError_t e = cudaSuccess;
   std::call_once(once, [] {
-    const cudaFuncAttribute A = cudaFuncAttributeMaxDynamicSharedMemorySize;
-    cudaError_t r[8] = {cudaFuncSetAttribute(k_rb_sweep<double, false, 1>, A, SwCfg<double>::SMEM),
-                        cudaFuncSetAttribute(k_rb_sweep<double, true, 1>, A, SwCfg<double>::SMEM),
-                        cudaFuncSetAttribute(k_rb_sweep<float, false, 1>, A, SwCfg<float>::SMEM),
-                        cudaFuncSetAttribute(k_rb_sweep<float, true, 1>, A, SwCfg<float>::SMEM),
-                        cudaFuncSetAttribute(k_rb_sweep<double, false, 2>, A, SwCfg<double>::SMEM),
-                        cudaFuncSetAttribute(k_rb_sweep<double, true, 2>, A, SwCfg<double>::SMEM),
-                        cudaFuncSetAttribute(k_rb_sweep<float, false, 2>, A, SwCfg<float>::SMEM),
-                        cudaFuncSetAttribute(k_rb_sweep<float, true, 2>, A, SwCfg<float>::SMEM)};
+    cudaError_t r[4] = {
+        cudaFuncSetAttribute(k_rb_sweep<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, SwCfg<double>::SMEM),
+        cudaFuncSetAttribute(k_rb_sweep<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SwCfg<double>::SMEM),
+        cudaFuncSetAttribute(k_rb_sweep<float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, SwCfg<float>::SMEM),
+        cudaFuncSetAttribute(k_rb_sweep<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SwCfg<float>::SMEM)};
     for (cudaError_t x : r)
       if (x != cudaSuccess) e = x;
   });
@@ -359,7 +354,7 @@ static int launch_sweep(Solver* s, cudaStream_t cs, const OpParams<T>& op, const
   if (int rc = kmap(s, &mk)) return rc;
   const Geo& g = op.g;
   const int kc = (g.NZ + s->sw_chunks - 1) / s->sw_chunks;
-  const dim3 grid = sweep_grid(g, s->sw_chunks), blk(kSwTPX, kSwTJ / s->sw_r);
+  const dim3 grid = sweep_grid(g, s->sw_chunks), blk(kSwTPX, kSwTJ);
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = grid;
   cfg.blockDim = blk;
@@ -370,9 +365,10 @@ static int launch_sweep(Solver* s, cudaStream_t cs, const OpParams<T>& op, const
   attr[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attr;
   cfg.numAttrs = s->pdl ? 1 : 0;
-  auto kern = s->sw_r == 2 ? (s->sw_dda ? k_rb_sweep<T, true, 2> : k_rb_sweep<T, false, 2>)
-                           : (s->sw_dda ? k_rb_sweep<T, true, 1> : k_rb_sweep<T, false, 1>);
-  cudaLaunchKernelEx(&cfg, kern, op, *mx, *mk, xout, bb, kc, st, s->sweep_err, s->wait_limit);
+  if (s->sw_dda)
+    cudaLaunchKernelEx(&cfg, k_rb_sweep<T, true>, op, *mx, *mk, xout, bb, kc, st, s->sweep_err, s->wait_limit);
+  else
+    cudaLaunchKernelEx(&cfg, k_rb_sweep<T, false>, op, *mx, *mk, xout, bb, kc, st, s->sweep_err, s->wait_limit);
   return H2G_OK;
 }
 
@@ -1577,7 +1573,7 @@ static int adjoint_transient(Solver* s, const FaceBC& f, int nt, const double* w
 // H2G_RB_PLANES, H2G_RB_DD and H2G_AX_DD in the environment force them (all four: no timing; a
 // forced rows, planes or dd source also restricts the timed variants to it).
 static std::mutex g_tune_mu;
-static std::map<std::array<int, 12>, int> g_tune_cache;
+static std::map<std::array<int, 11>, int> g_tune_cache;
 
 static bool valid_rows(int r) {
   for (int q : kRbRows)
@@ -1682,7 +1678,7 @@ static std::vector<int> sweep_chunk_candidates(const Solver* s) {
 // only_fused / only_chunks / only_dda: -1 = free, else forced by the environment.
 template <typename T>
 static int tune_sweep_t(Solver* s, const OpParams<T>& op, float unfused_ms, int only_fused, int only_chunks,
-                        int only_dda, int only_r, int* choice) {
+                        int only_dda, int* choice) {
   *choice = 0;
   if (only_fused == 0) return H2G_OK;
   if (int rc = sweep_attrs()) return rc;
@@ -1705,18 +1701,16 @@ static int tune_sweep_t(Solver* s, const OpParams<T>& op, float unfused_ms, int 
     cudaEventDestroy(e0);
     return fail(H2G_CUDA_ERROR, "event creation failed");
   }
-  const int saved_c = s->sw_chunks, saved_r = s->sw_r;
+  const int saved_c = s->sw_chunks;
   const bool saved_d = s->sw_dda;
   float best = only_fused == 1 ? 1e30f : unfused_ms;
   int rc = H2G_OK;
   for (int round = 0; round < 2 && rc == H2G_OK; ++round)
     for (int c : cands)
-      for (int v = 0; v < 4 && rc == H2G_OK; ++v) {
-        const int d = v & 1, rr = 1 + (v >> 1);
-        if ((only_dda >= 0 && d != only_dda) || (only_r > 0 && rr != only_r)) continue;
+      for (int d = 0; d < 2 && rc == H2G_OK; ++d) {
+        if (only_dda >= 0 && d != only_dda) continue;
         s->sw_chunks = c;
         s->sw_dda = d != 0;
-        s->sw_r = rr;
         for (int r = 0; r < 2 && rc == H2G_OK; ++r) rc = launch_sweep<T>(s, s->stream, op, (r & 1) ? xc : xa,
                                                                          (r & 1) ? xa : xc, xb, nullptr);
         cudaEventRecord(e0, s->stream);
@@ -1729,12 +1723,11 @@ static int tune_sweep_t(Solver* s, const OpParams<T>& op, float unfused_ms, int 
           rc = fail(H2G_CUDA_ERROR, "fused-sweep tuning failed");
         if (rc == H2G_OK && round == 1 && ms < best) {
           best = ms;
-          *choice = 1 | (d << 1) | (c << 2) | ((rr - 1) << 10);
+          *choice = 1 | (d << 1) | (c << 2);
         }
       }
   s->sw_chunks = saved_c;
   s->sw_dda = saved_d;
-  s->sw_r = saved_r;
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (rc == H2G_OK) rc = sweep_status(s);
@@ -1780,7 +1773,7 @@ static int tune_ax(Solver* s, int* use_dd) {
 static int autotune(Solver* s) {
   if (s->rb_tuned) return H2G_OK;
   // choices forced by the environment or h2g_set_sweep (-1: not forced)
-  int rows = -1, planes = -1, rbdd = -1, dd = -1, fused = -1, chunks = -1, swdd = -1, swr = -1;
+  int rows = -1, planes = -1, rbdd = -1, dd = -1, fused = -1, chunks = -1, swdd = -1;
   if (const char* e = getenv("H2G_RB_ROWS")) rows = valid_rows(atoi(e)) ? atoi(e) : -1;
   if (const char* e = getenv("H2G_RB_PLANES")) planes = (atoi(e) == 1 || atoi(e) == 2) ? atoi(e) : -1;
   if (const char* e = getenv("H2G_RB_DD")) rbdd = atoi(e) ? 1 : 0;
@@ -1788,20 +1781,18 @@ static int autotune(Solver* s) {
   if (const char* e = getenv("H2G_RB_FUSED")) fused = atoi(e) ? 1 : 0;
   if (const char* e = getenv("H2G_SW_CHUNKS")) chunks = (atoi(e) >= 1 && atoi(e) <= 255) ? atoi(e) : -1;
   if (const char* e = getenv("H2G_SW_DD")) swdd = atoi(e) ? 1 : 0;
-  if (const char* e = getenv("H2G_SW_ROWS")) swr = (atoi(e) == 1 || atoi(e) == 2) ? atoi(e) : -1;
   if (s->sweep_forced >= 0) {
     fused = s->sweep_forced;
     chunks = s->sweep_forced ? s->sw_chunks : -1;
     swdd = s->sweep_forced ? (s->sw_dda ? 1 : 0) : -1;
-    if (s->sweep_forced && swr < 0) swr = s->sw_r;
   }
   if (chunks > s->g.NZ) chunks = s->g.NZ;
-  const bool sweep_known = fused == 0 || (fused == 1 && chunks > 0 && swdd >= 0 && swr > 0);
+  const bool sweep_known = fused == 0 || (fused == 1 && chunks > 0 && swdd >= 0);
   if (rows < 0 || planes < 0 || rbdd < 0 || dd < 0 || !sweep_known) {
     // cached per grid, smoother precision and the choices the environment restricts it to
-    const std::array<int, 12> key = {s->g.MX, s->g.MY,  s->g.MZ, s->precision == H2G_FP64 ? 64 : 32,
+    const std::array<int, 11> key = {s->g.MX, s->g.MY,  s->g.MZ, s->precision == H2G_FP64 ? 64 : 32,
                                      rows,    planes,   rbdd,    dd,
-                                     fused,   chunks,   swdd,    swr};
+                                     fused,   chunks,   swdd};
     int cached = 0;
     {
       // held while tuning, so that handles of one grid solved concurrently (h2g_batch_solve) tune
@@ -1824,14 +1815,14 @@ static int autotune(Solver* s) {
           s->rb_planes = (r2 >> 5) & 7;
           s->rb_dd = (r2 >> 8) & 1;
           rc = s->precision == H2G_FP64
-                   ? tune_sweep_t<double>(s, op_params<double>(s, s->t64), unfused_ms, fused, chunks, swdd, swr, &sw)
-                   : tune_sweep_t<float>(s, op_params<float>(s, s->t32), unfused_ms, fused, chunks, swdd, swr, &sw);
+                   ? tune_sweep_t<double>(s, op_params<double>(s, s->t64), unfused_ms, fused, chunks, swdd, &sw)
+                   : tune_sweep_t<float>(s, op_params<float>(s, s->t32), unfused_ms, fused, chunks, swdd, &sw);
           s->rb_rows = sr;
           s->rb_planes = sp;
           s->rb_dd = sd;
         }
         if (rc) return rc;
-        cached = r2 | (d2 << 9) | (sw << 10) | (1 << 30);  // sw: 11 bits
+        cached = r2 | (d2 << 9) | (sw << 10) | (1 << 30);
         g_tune_cache[key] = cached;
       }
     }
@@ -1840,11 +1831,10 @@ static int autotune(Solver* s) {
     if (rbdd < 0) rbdd = (cached >> 8) & 1;
     if (dd < 0) dd = (cached >> 9) & 1;
     if (!sweep_known) {
-      const int sw = (cached >> 10) & 0x7ff;
+      const int sw = (cached >> 10) & 0x3ff;
       fused = sw & 1;
       swdd = (sw >> 1) & 1;
       chunks = std::max(1, (sw >> 2) & 0xff);
-      swr = 1 + ((sw >> 10) & 1);
     }
   }
   if (fused == 1) {
@@ -1852,10 +1842,9 @@ static int autotune(Solver* s) {
   } else {
     chunks = s->sw_chunks;
     swdd = s->sw_dda ? 1 : 0;
-    swr = s->sw_r;
   }
   if (rows != s->rb_rows || planes != s->rb_planes || (rbdd != 0) != s->rb_dd || (dd != 0) != s->ax_dd ||
-      (fused == 1) != s->rb_fused || chunks != s->sw_chunks || (swdd != 0) != s->sw_dda || swr != s->sw_r)
+      (fused == 1) != s->rb_fused || chunks != s->sw_chunks || (swdd != 0) != s->sw_dda)
     invalidate_graphs(s);
   s->rb_rows = rows;
   s->rb_planes = planes;
@@ -1864,7 +1853,6 @@ static int autotune(Solver* s) {
   s->rb_fused = fused == 1;
   s->sw_chunks = chunks;
   s->sw_dda = swdd != 0;
-  s->sw_r = swr;
   s->rb_tuned = true;
   return H2G_OK;
 }

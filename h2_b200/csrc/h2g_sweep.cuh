@@ -179,11 +179,10 @@ struct SweepThread {
   }
 };
 
-// ty: the thread's row of the tile (threadIdx.y, or threadIdx.y + TJ/R for a thread's second row)
-__device__ __forceinline__ SweepThread sweep_thread(const Geo& g, int ty) {
+__device__ __forceinline__ SweepThread sweep_thread(const Geo& g) {
   SweepThread t;
   t.tx = threadIdx.x;
-  t.ty = ty;
+  t.ty = threadIdx.y;
   const int q0 = (int)blockIdx.x * (kSwTPX - 2) - 1, r0 = (int)blockIdx.y * (kSwTJ - 2);
   t.p = q0 + t.tx;
   t.j = r0 + t.ty;
@@ -200,35 +199,27 @@ __device__ __forceinline__ SweepThread sweep_thread(const Geo& g, int ty) {
 __device__ __forceinline__ int next_slot(int q) { return q == kSwStages - 1 ? 0 : q + 1; }
 
 // One sweep: xout = RB-GS sweep of the x that tmx maps, with right-hand side bb.
-// Grid: (ceil(HI / (TPX-2)), ceil(NY / (TJ-2)), ceil(NZ / kc)); block (kSwTPX, kSwTJ / R): each
-// thread updates R rows of the tile (rows ty and ty + TJ/R), which gives it R independent update
-// chains per phase and leaves 128 registers per thread for R = 2; dynamic shared memory
-// SwCfg<T>::SMEM.
-template <typename T, bool DDA, int R>
-__global__ void __launch_bounds__(kSwThreads / R, 1)
+// Grid: (ceil(HI / (TPX-2)), ceil(NY / (TJ-2)), ceil(NZ / kc)); block (kSwTPX, kSwTJ); dynamic
+// shared memory SwCfg<T>::SMEM.
+template <typename T, bool DDA>
+__global__ void __launch_bounds__(kSwThreads, 1)
     k_rb_sweep(OpParams<T> op, const __grid_constant__ CUtensorMap tmx, const __grid_constant__ CUtensorMap tmk,
                T* __restrict__ xout, const T* __restrict__ bb, int kc, SolverState* st, int* err,
                long long wait_limit) {
   using C = SwCfg<T>;
-  constexpr int RY = kSwTJ / R;  // thread rows of the block
   pdl_enter();
   if (st && st->stop) return;
   extern __shared__ __align__(128) unsigned char sm[];
   const Geo& g = op.g;
-  SweepThread t[R];
-  int oX0[R], oK0[R];
-  const int tid = threadIdx.x + kSwTPX * threadIdx.y;
+  const SweepThread t = sweep_thread(g);
+  const int tid = t.tx + kSwTPX * t.ty;
   const int q0 = (int)blockIdx.x * (kSwTPX - 2) - 1, r0 = (int)blockIdx.y * (kSwTJ - 2);
   const int kA = 1 + (int)blockIdx.z * kc, kB = min(kA + kc - 1, g.NZ);
   const int xs = align_down(q0 - 1, C::A), xk = align_down(q0 - 1, 16), ys = 2 * (r0 - 1);
   const int first = kA - 2, last = kB + 2;  // staged planes
-#pragma unroll
-  for (int r = 0; r < R; ++r) {
-    t[r] = sweep_thread(g, threadIdx.y + r * RY);
-    // this column's colour-0 entries in the staged boxes (colour 1: one half-row further)
-    oX0[r] = (2 * (t[r].ty + 1)) * C::WX + (t[r].p - xs);
-    oK0[r] = (2 * (t[r].ty + 1)) * kSwWK + (t[r].p - xk);
-  }
+  // this column's colour-0 / colour-1 entries in the staged boxes
+  const int oX0 = (2 * (t.ty + 1)) * C::WX + (t.p - xs), oX1 = oX0 + C::WX;
+  const int oK0 = (2 * (t.ty + 1)) * kSwWK + (t.p - xk), oK1 = oK0 + kSwWK;
   T* c0b = reinterpret_cast<T*>(sm + kSwStages * C::STAGE);
   volatile int* flag = reinterpret_cast<volatile int*>(sm + C::BAR_OFF + 8 * kSwStages);
   const uint32_t bar0 = smem_u32(sm + C::BAR_OFF);
@@ -263,23 +254,18 @@ __global__ void __launch_bounds__(kSwThreads / R, 1)
 
   // ring slots of planes s-1, s, s+1 and of the plane issued at this step (s+3)
   int qm = 0, q0s = 1, qp = 2, qi = 4;
-  // windows along z of each row's column: colour-1 old values and keys at planes s-1, s, s+1;
-  // colour-0 new values and keys at planes s-2, s-1, s (after the shift at the top of step s)
-  T c1v[R][3], c0v[R][3], b0[R], b1[R];
-  uint32_t c1k[R][3], c0k[R][3];
+  // windows along z of this column: colour-1 old values and keys at planes s-1, s, s+1; colour-0
+  // new values and keys at planes s-2, s-1, s (after the shift at the top of step s)
+  T c1v[3] = {T(0), T(0), T(0)}, c0v[3] = {T(0), T(0), T(0)};
+  uint32_t c1k[3] = {0u, 0u, 0u}, c0k[3] = {0u, 0u, 0u};
+  T b0 = T(0), b1 = T(0);
   int pofs = (kA - 1) * (int)g.plane;  // s * plane at the current step
-#pragma unroll
-  for (int r = 0; r < R; ++r) {
-    c1v[r][0] = c1v[r][1] = c1v[r][2] = c0v[r][0] = c0v[r][1] = c0v[r][2] = b0[r] = b1[r] = T(0);
-    c1k[r][0] = c1k[r][1] = c1k[r][2] = c0k[r][0] = c0k[r][1] = c0k[r][2] = 0u;
-    if (!abort) {
-      const int o1 = oX0[r] + C::WX, k1o = oK0[r] + kSwWK;
-      c1v[r][1] = xbox(0)[o1];
-      c1k[r][1] = kbox(0)[k1o];
-      c1v[r][2] = xbox(1)[o1];
-      c1k[r][2] = kbox(1)[k1o];
-      if (t[r].in0(kA - 1, g.NZ)) b0[r] = __ldg(bb + pofs + t[r].g0);
-    }
+  if (!abort) {
+    c1v[1] = xbox(0)[oX1];
+    c1k[1] = kbox(0)[oK1];
+    c1v[2] = xbox(1)[oX1];
+    c1k[2] = kbox(1)[oK1];
+    if (t.in0(kA - 1, g.NZ)) b0 = __ldg(bb + pofs + t.g0);
   }
   for (int s = kA - 1; s <= kB + 1 && !abort; ++s, pofs += (int)g.plane) {
     if (tid == 0) {
@@ -298,82 +284,68 @@ __global__ void __launch_bounds__(kSwThreads / R, 1)
     const T* X0 = xbox(q0s);
     const uint8_t* K0 = kbox(q0s);
     const uint8_t* Km = kbox(qm);
+    c1v[0] = c1v[1];
+    c1v[1] = c1v[2];
+    c1v[2] = xbox(qp)[oX1];
+    c1k[0] = c1k[1];
+    c1k[1] = c1k[2];
+    c1k[2] = kbox(qp)[oK1];
     const bool mid = s >= kA && s <= kB;
-    T nb0[R], nb1[R];
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-      const int oX1 = oX0[r] + C::WX, oK1 = oK0[r] + kSwWK;
-      c1v[r][0] = c1v[r][1];
-      c1v[r][1] = c1v[r][2];
-      c1v[r][2] = xbox(qp)[oX1];
-      c1k[r][0] = c1k[r][1];
-      c1k[r][1] = c1k[r][2];
-      c1k[r][2] = kbox(qp)[oK1];
-      // right-hand sides of the next step, in flight during this one
-      nb0[r] = nb1[r] = T(0);
-      if (s <= kB && t[r].in0(s + 1, g.NZ)) nb0[r] = __ldg(bb + pofs + (int)g.plane + t[r].g0);
-      if (t[r].owned && mid && t[r].in1(s, g.NZ)) nb1[r] = __ldg(bb + pofs + t[r].g0 + g.HP);
-    }
+    // right-hand sides of the next step, in flight during this one
+    T nb0 = T(0), nb1 = T(0);
+    if (s <= kB && t.in0(s + 1, g.NZ)) nb0 = __ldg(bb + pofs + (int)g.plane + t.g0);
+    if (t.owned && mid && t.in1(s, g.NZ)) nb1 = __ldg(bb + pofs + t.g0 + g.HP);
+    const int e0 = t.par ^ (s & 1);  // colour 0 at plane s sits at i = 2p + e0
+    const int d0 = e0 ? 1 : -1;
 
     // phase A: colour 0 at plane s (tile and overlap)
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-      const int oX1 = oX0[r] + C::WX, oK1 = oK0[r] + kSwWK;
-      const int e0 = t[r].par ^ (s & 1);  // colour 0 at plane s sits at i = 2p + e0
-      const int d0 = e0 ? 1 : -1;
-      const T pp = X0[oX0[r]];
-      const uint32_t k0 = K0[oK0[r]];
+    {
+      const T pp = X0[oX0];
+      const uint32_t k0 = K0[oK0];
       T nv = pp;
-      const bool in = t[r].in0(s, g.NZ);
+      const bool in = t.in0(s, g.NZ);
       if (in && (k0 & 0x80u)) {
         const T xo = X0[oX1 + d0];
         const uint32_t ko = K0[oK1 + d0];
-        const T xm = e0 ? c1v[r][1] : xo, xp = e0 ? xo : c1v[r][1];
-        const uint32_t kxm = e0 ? c1k[r][1] : ko, kxp = e0 ? ko : c1k[r][1];
-        nv = sweep_update<T, DDA>(op, s, s * op.P, k0, kxm, kxp, K0[oK1 - 2 * kSwWK], K0[oK1 + 2 * kSwWK],
-                                  c1k[r][0], c1k[r][2], pofs + t[r].g0, pp, b0[r], xm, xp, X0[oX1 - 2 * C::WX],
-                                  X0[oX1 + 2 * C::WX], c1v[r][0], c1v[r][2]);
+        const T xm = e0 ? c1v[1] : xo, xp = e0 ? xo : c1v[1];
+        const uint32_t kxm = e0 ? c1k[1] : ko, kxp = e0 ? ko : c1k[1];
+        nv = sweep_update<T, DDA>(op, s, s * op.P, k0, kxm, kxp, K0[oK1 - 2 * kSwWK], K0[oK1 + 2 * kSwWK], c1k[0],
+                                  c1k[2], pofs + t.g0, pp, b0, xm, xp, X0[oX1 - 2 * C::WX], X0[oX1 + 2 * C::WX],
+                                  c1v[0], c1v[2]);
       }
-      c0v[r][0] = c0v[r][1];
-      c0v[r][1] = c0v[r][2];
-      c0v[r][2] = nv;
-      c0k[r][0] = c0k[r][1];
-      c0k[r][1] = c0k[r][2];
-      c0k[r][2] = k0;
-      c0b[(s & 1) * (kSwTJ * kSwTPX) + t[r].c0off] = nv;
-      if (t[r].owned && in && mid) xout[pofs + t[r].g0] = nv;
+      c0v[0] = c0v[1];
+      c0v[1] = c0v[2];
+      c0v[2] = nv;
+      c0k[0] = c0k[1];
+      c0k[1] = c0k[2];
+      c0k[2] = k0;
+      c0b[(s & 1) * (kSwTJ * kSwTPX) + t.c0off] = nv;
+      if (t.owned && in && mid) xout[pofs + t.g0] = nv;
     }
     // phase B: colour 1 at plane s-1 (owned cells), its colour-0 neighbours from step s-1
     const int sb = s - 1;
-    if (sb >= kA) {
-#pragma unroll
-      for (int r = 0; r < R; ++r) {
-        if (!t[r].owned) continue;
-        const T pp = c1v[r][0];
-        const uint32_t k1 = c1k[r][0];
-        T nv = pp;
-        const int pb = pofs - (int)g.plane;
-        const bool in = t[r].in1(sb, g.NZ);
-        if (in && (k1 & 0x80u)) {
-          const int e1 = t[r].par ^ (s & 1);  // colour 1 at plane s-1 sits at i = 2p + e0(s)
-          const int d1 = e1 ? 1 : -1;
-          const T* Cr = c0b + (sb & 1) * (kSwTJ * kSwTPX) + t[r].c0off;
-          const T xo = Cr[d1];
-          const uint32_t ko = Km[oK0[r] + d1];
-          const T xm = e1 ? c0v[r][1] : xo, xp = e1 ? xo : c0v[r][1];
-          const uint32_t kxm = e1 ? c0k[r][1] : ko, kxp = e1 ? ko : c0k[r][1];
-          nv = sweep_update<T, DDA>(op, sb, sb * op.P, k1, kxm, kxp, Km[oK0[r] - 2 * kSwWK], Km[oK0[r] + 2 * kSwWK],
-                                    c0k[r][0], c0k[r][2], pb + t[r].g0 + g.HP, pp, b1[r], xm, xp, Cr[-kSwTPX],
-                                    Cr[kSwTPX], c0v[r][0], c0v[r][2]);
-        }
-        if (in) xout[pb + t[r].g0 + g.HP] = nv;
+    if (t.owned && sb >= kA) {
+      const T pp = c1v[0];
+      const uint32_t k1 = c1k[0];
+      T nv = pp;
+      const int pb = pofs - (int)g.plane;
+      const bool in = t.in1(sb, g.NZ);
+      if (in && (k1 & 0x80u)) {
+        const int e1 = e0;  // colour 1 at plane s-1 sits at i = 2p + e0
+        const int d1 = e1 ? 1 : -1;
+        const T* Cr = c0b + (sb & 1) * (kSwTJ * kSwTPX) + t.c0off;
+        const T xo = Cr[d1];
+        const uint32_t ko = Km[oK0 + d1];
+        const T xm = e1 ? c0v[1] : xo, xp = e1 ? xo : c0v[1];
+        const uint32_t kxm = e1 ? c0k[1] : ko, kxp = e1 ? ko : c0k[1];
+        nv = sweep_update<T, DDA>(op, sb, sb * op.P, k1, kxm, kxp, Km[oK0 - 2 * kSwWK], Km[oK0 + 2 * kSwWK], c0k[0],
+                                  c0k[2], pb + t.g0 + g.HP, pp, b1, xm, xp, Cr[-kSwTPX], Cr[kSwTPX], c0v[0],
+                                  c0v[2]);
       }
+      if (in) xout[pb + t.g0 + g.HP] = nv;
     }
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-      b0[r] = nb0[r];
-      b1[r] = nb1[r];
-    }
+    b0 = nb0;
+    b1 = nb1;
     qm = q0s;
     q0s = qp;
     qp = next_slot(qp);
@@ -430,7 +402,7 @@ __global__ void __launch_bounds__(kSwThreads, 1)
   if (st && st->stop) return;
   extern __shared__ __align__(128) unsigned char sm[];
   const Geo& g = op.g;
-  const SweepThread t = sweep_thread(g, threadIdx.y);
+  const SweepThread t = sweep_thread(g);
   const int tid = t.tx + kSwTPX * t.ty;
   const int q0 = (int)blockIdx.x * (kSwTPX - 2) - 1, r0 = (int)blockIdx.y * (kSwTJ - 2);
   const int kA = 1 + (int)blockIdx.z * kc, kB = min(kA + kc - 1, g.NZ);

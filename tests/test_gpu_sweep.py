@@ -26,11 +26,8 @@ H2G_TIMEOUT = 6
 VARIANTS = [(1, False), (2, True), (3, False), (7, True)]
 
 
-@pytest.mark.parametrize("rows", [1, 2])
 @pytest.mark.parametrize("case", CASES, ids=["mode3", "adiabatic", "odd", "transient"])
-def test_fused_preconditioner_bit_exact(oracle, case, rows, monkeypatch):
-    """Both thread shapes of the fused sweep (one or two rows of the tile per thread)."""
-    monkeypatch.setenv("H2G_SW_ROWS", str(rows))
+def test_fused_preconditioner_bit_exact(oracle, case):
     prob = mode3_model(oracle, **case)
     s = make_solver(prob)
     bb = random_interior(prob.shape, 31)
@@ -45,13 +42,11 @@ def test_fused_preconditioner_bit_exact(oracle, case, rows, monkeypatch):
     s.close()
 
 
-@pytest.mark.parametrize("rows", [1, 2])
 @pytest.mark.parametrize("transient", [False, True], ids=["steady", "transient"])
 @pytest.mark.parametrize("grid", GRIDS, ids=["x".join(map(str, g)) for g in GRIDS])
-def test_fused_preconditioner_boxes(oracle, grid, transient, rows, monkeypatch):
+def test_fused_preconditioner_boxes(oracle, grid, transient):
     """Grids smaller than one tile, odd sizes, NZ = 1 (a chunk count above NZ is clamped), every
     boundary type; the transient boxes take the full 13-term dd (a_p0 per cell)."""
-    monkeypatch.setenv("H2G_SW_ROWS", str(rows))
     prob = box_problem(oracle, *grid, seed=sum(grid) + 3, transient=transient)
     s = make_solver(prob)
     bb = random_interior(prob.shape, 5)
