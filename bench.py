@@ -527,6 +527,7 @@ def run_ours(a, dist: Dist):
     if e2e is not None:
         e2e = {"value": e2e_max, **e2e}
 
+    variants = run_mixed_variants(a, m, th["fp64"], max_dtheta, results, torch, stream, flush)
     cg_sym = run_cg_symmetric(a, dist, torch, stream, flush) if a.cg else None
     batch = run_batch(a, dist, torch, stream, flush) if a.batch > 0 else None
     adjoint = run_adjoint(a, dist, torch, stream) if a.adjoint_steps > 0 else None
@@ -565,6 +566,7 @@ def run_ours(a, dist: Dist):
                   "precision": "FP32 RB-GS preconditioner (tables, smoother vectors); FP64 Krylov vectors, "
                                "inner products, CalcAX and solution"},
         "speedup_mixed_vs_fp64": f64["t"] / mx["t"],
+        "mixed_variants": variants,
         "roofline": roofline_object(rm, peak, peak_kind, a.nx, a.nz),
         "kernels": {f"{k[0]}_{k[1]}": v for k, v in roof.items()},
         "scaling_configs": scaling,
@@ -582,6 +584,52 @@ def run_ours(a, dist: Dist):
     for s in solvers.values():
         s.close()
     dist.close()
+
+
+# Bytes per cell of one PBiCGSTAB iteration on the fused path (keys 1 byte), per precision form:
+# the speed-up each form could reach at equal iterations when every kernel is memory-bound.
+ITERATION_BYTES = {"fp64": 388, "mixed": 276, "mixed_ir": 200}
+
+
+def run_mixed_variants(a, m, th64, max_dtheta, results, torch, stream, flush):
+    """The precision forms side by side on the benchmark grid: FP64, H2G_MIXED (FP32 smoother in
+    FP64 PBiCGSTAB, restarts on the FP64 true residual) and H2G_MIXED_IR (FP32 operator, smoother
+    and Krylov vectors inside FP64 iterative refinement), one solve each after the timed ones (the
+    IR form capped at 4000 inner iterations); time, iterations, status, max |theta - theta_FP64|
+    (th64: the interior of the timed FP64 solve's field) and the byte-model ceiling at equal
+    iterations."""
+    import h2_b200
+    out = {}
+    for name, res_t in (("fp64", results["fp64"]), ("mixed", results["mixed"])):
+        r = res_t["res"]
+        out[name] = {"seconds": res_t["t"], "iterations": r.itr, "status": r.status, "restarts": r.outer,
+                     "ceiling_at_equal_iterations": ITERATION_BYTES["fp64"] / ITERATION_BYTES[name]}
+    out["mixed"]["max_abs_dtheta_vs_fp64_K"] = max_dtheta
+    w = m.wk
+    s = h2_b200.Solver(*m.shape, precision="mixed_ir", stream=stream.cuda_stream)
+    try:
+        s.set_grid(m.ZC, m.dZ, m.dx, m.dy, m.dt, m.HC, True)
+        s.set_fields(w.lam, w.mask)
+        s.set_rhs(w.b)
+        s.set_theta(w.theta)
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        st, r = s.solve("pbicgstab", tol=a.tol, maxItr=4000, smoother="gs")
+        e1.record(stream)
+        e1.synchronize()
+        entry = {"seconds": e0.elapsed_time(e1) * 1e-3, "iterations": r.itr, "status": st, "outer": r.outer,
+                 "final_rel_residual": r.res, "ceiling_at_equal_iterations": ITERATION_BYTES["fp64"] / ITERATION_BYTES["mixed_ir"]}
+        if st == 0:
+            entry["max_abs_dtheta_vs_fp64_K"] = float(np.abs(s.get_theta()[1:-1, 1:-1, 1:-1] - th64).max())
+        out["mixed_ir"] = entry
+    except Exception as e:  # pragma: no cover
+        out["mixed_ir"] = {"error": str(e)}
+    finally:
+        s.close()
+    out["status_codes"] = "0 converged, 1 not converged, 2 breakdown, 3 non-finite"
+    return out
 
 
 def run_cg_symmetric(a, dist, torch, stream, flush):
