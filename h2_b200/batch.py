@@ -158,13 +158,15 @@ class BatchSolver:
                 ids[m.nx] = M.fill_id(m.nx, m.nx, NZ)
             ID = ids[m.nx]
             dx = M.pitch(m.nx)
-            model = M.build_mode3(m.nx, m.nx, NZ, ID=ID, hsrc=heat_map(m, ID, ZC, dx, dx))
+            model = M.build_mode3(m.nx, m.nx, NZ, ID=ID, hsrc=heat_map(m, ID, ZC, dx, dx), calrhs=False)
             w = model.wk
             s = Solver(*model.shape, precision=precision)
             s.set_grid(model.ZC, model.dZ, model.dx, model.dy, model.dt, model.HC, True)
             s.set_fields(w.lam, w.mask)
-            s.set_rhs(w.b)
             s.set_theta(w.theta)
+            # calRHS! on the member's own handle: b = -(hsrc V + boundary terms), from b = 0
+            s.set_hsrc(w.hsrc)
+            s.calrhs(model.bcs, zero_b=True)
             s.snapshot()
             self.solvers.append(s)
         self._handles = (C.c_void_p * len(self.solvers))(*[s.h.value for s in self.solvers])

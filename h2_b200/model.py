@@ -175,10 +175,11 @@ class Model:
 
 def build_mode3(NX: int, NY: int | None = None, NZ: int = 30, *, is_steady: bool = True, dt: float = 1.0e4,
                 theta_init: float = 300.0, symmetric: bool = False, ID: np.ndarray | None = None,
-                hsrc: np.ndarray | None = None, lam_scale: np.ndarray | None = None) -> Model:
+                hsrc: np.ndarray | None = None, lam_scale: np.ndarray | None = None, calrhs: bool = True) -> Model:
     """q3d's set-up (heat3ds.jl:193-230 and main 113-128) for the Mode-3 IC stack.
     lam_scale (MZ factors, optional) multiplies the conductivity of every interior cell of plane
-    k before the boundary conditions copy it into isothermal guards."""
+    k before the boundary conditions copy it into isothermal guards.  calrhs=False leaves b at
+    zero, for a caller that runs calRHS! on its own solver handle (Solver.calrhs)."""
     NY = NX if NY is None else NY
     Z, ZC, dZ = zgrid(NZ)
     if ID is None:
@@ -196,5 +197,6 @@ def build_mode3(NX: int, NY: int | None = None, NZ: int = 30, *, is_steady: bool
     else:
         wk.hsrc[...] = hsrc
     dx, dy = pitch(NX), pitch(NY)
-    calRHS(wk, dx, dy, dt, ZC, dZ, HC, bcs, is_steady)
+    if calrhs:
+        calRHS(wk, dx, dy, dt, ZC, dZ, HC, bcs, is_steady)
     return Model(NX, NY, NZ, dx, dy, dt, is_steady, Z, ZC, dZ, HC, bcs, ID, wk)

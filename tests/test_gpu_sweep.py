@@ -147,3 +147,20 @@ def test_bench_hook_fused_sweep(oracle):
     s.set_sweep(0)
     assert s.bench_kernel(0, 3) == 6
     s.close()
+
+
+def test_sweep_controls_reject_bad_arguments(oracle):
+    """h2g_set_sweep and h2g_set_wait_limit check their arguments on the host (H2G_BAD_ARG)."""
+    from h2_b200 import _lib as L
+    prob = mode3_model(oracle, 40)
+    s = make_solver(prob)
+    lib = L.load()
+    assert lib.h2g_set_sweep(s.h, 2, 1, 0) == L.H2G_BAD_ARG
+    assert lib.h2g_set_sweep(s.h, 1, 0, 0) == L.H2G_BAD_ARG
+    assert lib.h2g_set_sweep(s.h, 1, 256, 0) == L.H2G_BAD_ARG
+    assert lib.h2g_set_sweep(s.h, 1, 2, 5) == L.H2G_BAD_ARG
+    assert lib.h2g_set_wait_limit(s.h, -1) == L.H2G_BAD_ARG
+    assert lib.h2g_set_sweep(None, 0, 1, 0) == L.H2G_BAD_ARG
+    s.set_sweep(1, 200, True)  # more chunks than planes: clamped to NZ
+    assert s.sweep() == (True, 30, True)
+    s.close()
