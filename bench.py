@@ -698,8 +698,8 @@ def run_batch(a, dist, torch, stream, flush):
     bs = B.BatchSolver(mine)
     t_setup = time.perf_counter() - t0
 
-    def timed(fn):
-        bs.restore()
+    def timed(batch, fn):
+        batch.restore()
         torch.cuda.synchronize()
         with torch.cuda.stream(stream):
             flush.zero_()
@@ -711,14 +711,14 @@ def run_batch(a, dist, torch, stream, flush):
         return e0.elapsed_time(e1) * 1e-3, out
 
     try:
-        timed(lambda: bs.solve(tol=a.tol))  # warm-up: graph instantiation per handle
+        timed(bs, lambda: bs.solve(tol=a.tol))  # warm-up: graph instantiation per handle
         dist.barrier()
         ts, res = [], None
         for _ in range(max(1, a.batch_steps)):
-            dt_, (st, res) = timed(lambda: bs.solve(tol=a.tol))
+            dt_, (st, res) = timed(bs, lambda: bs.solve(tol=a.tol))
             ts.append(dt_)
         dist.barrier()
-        t_seq, _ = timed(lambda: bs.solve_sequential(tol=a.tol))
+        t_seq, _ = timed(bs, lambda: bs.solve_sequential(tol=a.tol))
         local = {m.index: {"itr": r.itr, "conv": r.isconverged} for m, r in zip(mine, res)}
         merged = B.gather_results(local)
         out = {"solves": a.batch, "cells": sum(m.cells for m in members),
@@ -733,9 +733,24 @@ def run_batch(a, dist, torch, stream, flush):
         if merged is not None:
             out["iterations_total"] = int(sum(v["itr"] for v in merged.values()))
             out["all_converged"] = bool(all(v["conv"] for v in merged.values()))
-        return out
+        th64 = [s.get_theta() for s in bs.solvers]
     finally:
         bs.close()
+    # the config's precision form: FP32 smoother inside FP64 PBiCGSTAB with FP64 restarts on the
+    # true residual (H2G_MIXED), one timed call after an untimed one; max |dtheta| against FP64
+    bm = B.BatchSolver(mine, precision="mixed")
+    try:
+        timed(bm, lambda: bm.solve(tol=a.tol))
+        t_m, (st_m, res_m) = timed(bm, lambda: bm.solve(tol=a.tol))
+        local_m = float(max(np.abs(s.get_theta() - t).max() for s, t in zip(bm.solvers, th64)))
+        out["mixed"] = {"seconds": dist.max(t_m), "iterations_total_rank0": int(sum(r.itr for r in res_m)),
+                        "restarts_total_rank0": int(sum(r.outer for r in res_m)),
+                        "all_converged_rank0": bool(all(r.isconverged for r in res_m)),
+                        "max_abs_dtheta_vs_fp64_K": dist.max(local_m),
+                        "precision": "FP32 RB-GS smoother in FP64 PBiCGSTAB, restarted on the FP64 true residual"}
+    finally:
+        bm.close()
+    return out
 
 
 def run_adjoint(a, dist, torch, stream):
