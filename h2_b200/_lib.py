@@ -84,6 +84,11 @@ _SIGS = {
                                         C.c_int, _dp, _dp, _dp, C.POINTER(Result)]),
     "h2g_autotune": (C.c_int, [_vp, _ip, _ip, _ip, _ip]),
     "h2g_set_tuning": (C.c_int, [_vp, C.c_int, C.c_int]),
+    "h2g_create_multi": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(_vp)]),
+    "h2g_set_rhs_multi": (C.c_int, [_vp, _dp]),
+    "h2g_set_theta_multi": (C.c_int, [_vp, _dp]),
+    "h2g_get_theta_multi": (C.c_int, [_vp, _dp]),
+    "h2g_pbicgstab_multi": (C.c_int, [_vp, C.c_double, C.c_int, C.c_int, C.POINTER(Result)]),
     "h2g_set_sweep": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int]),
     "h2g_get_sweep": (C.c_int, [_vp, _ip, _ip, _ip]),
     "h2g_set_wait_limit": (C.c_int, [_vp, C.c_longlong]),

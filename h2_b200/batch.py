@@ -198,7 +198,86 @@ class BatchSolver:
             return [s.sor(omega=1.0, tol=tol, maxItr=maxItr)[1] for s in self.solvers]
         return [s.solve(method, tol=tol, maxItr=maxItr, smoother=smoother)[1] for s in self.solvers]
 
+    def thetas(self) -> list:
+        """theta of every member, in member order."""
+        return [s.get_theta() for s in self.solvers]
+
     def close(self):
         for s in self.solvers:
             s.close()
         self.solvers = []
+
+
+class MultiBatchSolver:
+    """The batch as one multi right-hand-side solve per grid size (h2g_create_multi /
+    h2g_pbicgstab_multi): the members of a size share the operator, so each size group is one
+    handle with K right-hand sides, and every member's result is bit for bit its lone solve's.
+    b of every member is calRHS! (GPU) of its heat map on a helper handle of its size.  The groups
+    are solved one after another on the given stream."""
+
+    def __init__(self, members: list[Member], stream: int | None = None):
+        from . import model as M
+        from .nonuniform import MultiSolver, Solver
+        from . import _lib as L
+        self.L = L
+        self.members = list(members)
+        self.groups = []  # (member indices in self.members, MultiSolver, theta0 list)
+        _, ZC, _ = M.zgrid(NZ)
+        for nx in sorted({m.nx for m in self.members}):
+            idx = [q for q, m in enumerate(self.members) if m.nx == nx]
+            ID = M.fill_id(nx, nx, NZ)
+            dx = M.pitch(nx)
+            base = M.build_mode3(nx, nx, NZ, ID=ID, calrhs=False)
+            w = base.wk
+            helper = Solver(*base.shape, stream=stream)
+            bs, th0 = [], []
+            try:
+                helper.set_grid(base.ZC, base.dZ, base.dx, base.dy, base.dt, base.HC, True)
+                helper.set_fields(w.lam, w.mask)
+                for q in idx:
+                    helper.set_theta(w.theta)
+                    helper.set_hsrc(heat_map(self.members[q], ID, ZC, dx, dx))
+                    helper.calrhs(base.bcs, zero_b=True)
+                    bs.append(helper.get_rhs())
+                    th0.append(w.theta.copy(order="F"))
+            finally:
+                helper.close()
+            ms = MultiSolver(*base.shape, len(idx), stream=stream)
+            ms.set_grid(base.ZC, base.dZ, base.dx, base.dy, base.dt, base.HC, True)
+            ms.set_fields(w.lam, w.mask)
+            ms.set_rhs_multi(bs)
+            ms.set_theta_multi(th0)
+            self.groups.append((idx, ms, th0))
+
+    @property
+    def cells(self) -> int:
+        return sum(m.cells for m in self.members)
+
+    def restore(self):
+        for _, ms, th0 in self.groups:
+            ms.set_theta_multi(th0)
+
+    def solve(self, tol=1e-8, maxItr=20_000, smoother="gs"):
+        """All members; returns (status, list of Result in member order)."""
+        L = self.L
+        res = [None] * len(self.members)
+        status = L.H2G_OK
+        for idx, ms, _ in self.groups:
+            st, outs = ms.solve_multi(tol=tol, maxItr=maxItr, smoother=smoother)
+            for q, r in zip(idx, outs):
+                res[q] = r
+            if status == L.H2G_OK and st != L.H2G_OK:
+                status = st
+        return status, res
+
+    def thetas(self) -> list:
+        out = [None] * len(self.members)
+        for idx, ms, _ in self.groups:
+            for q, th in zip(idx, ms.get_theta_multi()):
+                out[q] = th
+        return out
+
+    def close(self):
+        for _, ms, _ in self.groups:
+            ms.close()
+        self.groups = []

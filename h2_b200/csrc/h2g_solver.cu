@@ -27,6 +27,7 @@
 
 #include "../../include/h2g.h"
 #include "h2g_sweep.cuh"
+#include "h2g_multi.cuh"
 
 namespace h2g {
 
@@ -172,6 +173,16 @@ struct Solver {
   int* sweep_err = nullptr;            // set by a fused sweep whose bounded wait ran out
   long long wait_limit = kWaitCycles;  // budget of one bounded wait (clock cycles)
   std::map<std::pair<const void*, int>, CUtensorMap> xmaps;  // TMA maps of x buffers (pointer, bytes/element)
+  // K right-hand sides on the handle's operator (h2g_create_multi): stacked vectors, K states
+  int nrhs = 0;
+  double* mr_th = nullptr;
+  double* mr_b = nullptr;
+  double* mr_kv[8] = {nullptr};  // r, r0, p, p_, q, s, s_, t
+  SolverState* mr_st = nullptr;
+  MultiCtl* mr_ctl = nullptr;
+  double* mr_partials = nullptr;
+  int* mr_flag = nullptr;
+  SolveGraph mr_graph;
   CUtensorMap kmap;                    // TMA map of the key array
   bool kmap_ok = false;
 
@@ -524,6 +535,10 @@ static void destroy(Solver* s) {
   for (auto& p : s->hook) cudaFree(p);
   for (auto& p : s->stage) cudaFree(p);
   cudaFree(s->x2_64); cudaFree(s->x2_32); cudaFree(s->sweep_err);
+  s->mr_graph.reset();
+  cudaFree(s->mr_th); cudaFree(s->mr_b); cudaFree(s->mr_st); cudaFree(s->mr_ctl); cudaFree(s->mr_partials);
+  cudaFree(s->mr_flag);
+  for (auto& p : s->mr_kv) cudaFree(p);
   cudaFree(s->st); cudaFree(s->st_in); cudaFree(s->partials); cudaFree(s->hist);
   if (s->st_host) cudaFreeHost(s->st_host);
   if (s->cap) cudaStreamDestroy(s->cap);
@@ -1196,6 +1211,110 @@ static int solve_mixed(Solver* s, bool cg, double tol, int maxItr, int smoother,
     out->res0 = res0;
     out->res = res;
     out->launches = launches;
+  }
+  return status;
+}
+
+// ------------------------------------------------------------------------------------------
+// K right-hand sides on one operator (h2g_create_multi): PBiCGSTAB! + RB-GS for all of them at
+// once, every right-hand side with its own scalars and stop test (h2g_multi.cuh).
+// ------------------------------------------------------------------------------------------
+static dim3 mr_grid(const Geo& g, int K) {
+  const int G = (K + kMrR - 1) / kMrR;
+  return dim3((g.HN + kBX - 1) / kBX, (g.NY + kBY - 1) / kBY, g.NZ * G);
+}
+
+static int launch_pbicg_body_mr(Solver* s, cudaStream_t cs, const OpParams<double>& op, cudaGraphConditionalHandle hc,
+                                int use_cond) {
+  const Geo& g = s->g;
+  const int K = s->nrhs;
+  const long long n = g.n;
+  double *r = s->mr_kv[0], *r0 = s->mr_kv[1], *p = s->mr_kv[2], *ph = s->mr_kv[3], *q = s->mr_kv[4],
+         *sv = s->mr_kv[5], *sh = s->mr_kv[6], *t = s->mr_kv[7];
+  const dim3 grid = mr_grid(g, K), blk(kBX, kBY);
+  SolverState* st = s->mr_st;
+  // p = r + beta (p - omega q); p_ = M^-1 p                     NonUniform.jl:296-305
+  launch(s, k_rb_first_mr<1, kMrR>, grid, blk, cs, op, ph, p, (const double*)r, (const double*)q,
+         (const SolverState*)st, K, n);
+  for (int pass = 1; pass < 2 * kSweeps; ++pass)
+    launch(s, k_rb_pass_mr<kMrR>, grid, blk, cs, op, ph, (const double*)p, pass & 1, (const SolverState*)st, K, n);
+  // q = A p_;  alpha = rho / (q, r0)                            NonUniform.jl:307-309
+  launch(s, k_ax_mr<1, kMrR>, grid, blk, cs, op, q, (const double*)ph, (const double*)r0, (const double*)nullptr, st,
+         s->mr_partials, (int)kStageAlpha, K, n);
+  // s = r - alpha q; s_ = M^-1 s                                NonUniform.jl:310-315
+  launch(s, k_rb_first_mr<2, kMrR>, grid, blk, cs, op, sh, sv, (const double*)r, (const double*)q,
+         (const SolverState*)st, K, n);
+  for (int pass = 1; pass < 2 * kSweeps; ++pass)
+    launch(s, k_rb_pass_mr<kMrR>, grid, blk, cs, op, sh, (const double*)sv, pass & 1, (const SolverState*)st, K, n);
+  // t = A s_; omega = (t,s)/(t,t)                               NonUniform.jl:317-326
+  launch(s, k_ax_mr<2, kMrR>, grid, blk, cs, op, t, (const double*)sh, (const double*)nullptr, (const double*)sv, st,
+         s->mr_partials, (int)kStageOmega, K, n);
+  // x += alpha p_ + omega s_; r = s - omega t; res; next rho    NonUniform.jl:328-346
+  const dim3 ug(elementwise_blocks(s), K);
+  if (use_cond)
+    launch(s, k_bicg_update_mr<true>, ug, 256, cs, n, s->mr_th, (const double*)ph, (const double*)sh, r,
+           (const double*)sv, (const double*)t, (const double*)r0, st, s->mr_ctl, s->mr_partials, hc, use_cond);
+  else
+    launch(s, k_bicg_update_mr<false>, ug, 256, cs, n, s->mr_th, (const double*)ph, (const double*)sh, r,
+           (const double*)sv, (const double*)t, (const double*)r0, st, s->mr_ctl, s->mr_partials, hc, use_cond);
+  return H2G_OK;
+}
+
+static int solve_multi(Solver* s, double tol, int maxItr, int smoother, h2g_result* outs) {
+  if (!s->grid_set || !s->fields_set) return fail(H2G_BAD_ARG, "h2g_set_grid and h2g_set_fields must come first");
+  if (maxItr < 1 || maxItr > 10000000) return fail(H2G_BAD_ARG, "maxItr out of range: %d", maxItr);
+  if (smoother != H2G_SMOOTHER_GS)
+    return fail(H2G_UNSUPPORTED, "a multi right-hand-side solve runs the RB-GS preconditioner (smoother gs)");
+  if (!(tol >= 0.0) || !std::isfinite(tol)) return fail(H2G_BAD_ARG, "bad tolerance");
+  if (!outs) return fail(H2G_BAD_ARG, "null result array");
+  CK(cudaSetDevice(s->device));
+  const Geo& g = s->g;
+  const int K = s->nrhs;
+  OpParams<double> op = op_params<double>(s, s->t64);
+  launch(s, k_prime_mr, 1, kMrMax, s->stream, s->mr_st, s->mr_ctl, tol, maxItr, K);
+  // r = b - A theta, r0 = r, res0 and rho of every right-hand side   NonUniform.jl:262-274
+  launch(s, k_rk_mr<kMrR>, mr_grid(g, K), dim3(kBX, kBY), s->stream, op, s->mr_kv[0], s->mr_kv[1],
+         (const double*)s->mr_th, (const double*)s->mr_b, s->mr_st, s->mr_partials, (int)kStageInit, K, g.n);
+  CKL();
+  SolveGraph& G = s->mr_graph;
+  std::vector<unsigned char> sig = signature(op, op, smoother, (const void*)s->mr_th);
+  if (!G.exec || G.sig != sig) {
+    int berr = H2G_OK;
+    int rc = make_loop_graph(s, G, [&](cudaStream_t cs, cudaGraphConditionalHandle hc, int use_cond) {
+      for (int u = 0; u < kUnroll && berr == H2G_OK; ++u) berr = launch_pbicg_body_mr(s, cs, op, hc, use_cond);
+    });
+    if (rc == H2G_OK && berr != H2G_OK) G.reset();
+    if (rc) return rc;
+    if (berr) return berr;
+    G.sig = sig;
+  }
+  if (G.cond) {
+    CK(cudaGraphLaunch(G.exec, s->stream));
+  } else {
+    int done = 0, any = 1;
+    while (done < maxItr + 1 && any) {
+      for (int i = 0; i < 8; ++i) CK(cudaGraphLaunch(G.exec, s->stream));
+      done += 8 * kUnroll;
+      k_any_running<<<1, 1, 0, s->stream>>>(s->mr_st, K, s->mr_flag);
+      CK(cudaMemcpyAsync(&any, s->mr_flag, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+      CK(cudaStreamSynchronize(s->stream));
+    }
+  }
+  std::vector<SolverState> fin(K);
+  CK(cudaMemcpyAsync(fin.data(), s->mr_st, sizeof(SolverState) * K, cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  int status = H2G_OK;
+  const long long per_iter = 2 * (2 * kSweeps) + 2 + 1;
+  for (int q = 0; q < K; ++q) {
+    h2g_result& o = outs[q];
+    o.isconverged = fin[q].converged;
+    o.itr = fin[q].itr;
+    o.outer = 0;
+    o.status = status_of(fin[q]);
+    o.res0 = fin[q].res0;
+    o.res = fin[q].res;
+    o.launches = 2 + per_iter * std::max(1, fin[q].itr);
+    if (status == H2G_OK && o.status != H2G_OK) status = o.status;
   }
   return status;
 }
@@ -2436,6 +2555,72 @@ int h2g_set_tuning(h2g_solver* h, int rows, int planes) {
   s->rb_planes = planes;
   s->rb_tuned = true;
   return H2G_OK;
+}
+
+// ---- K right-hand sides on one operator ------------------------------------------------------
+int h2g_create_multi(int MX, int MY, int MZ, int nrhs, h2g_solver** out) {
+  using namespace h2g;
+  if (!out) return fail(H2G_BAD_ARG, "null output pointer");
+  *out = nullptr;
+  if (nrhs < 1 || nrhs > kMrMax) return fail(H2G_BAD_ARG, "nrhs must be in 1..%d", kMrMax);
+  Solver* s = nullptr;
+  if (int rc = create(MX, MY, MZ, H2G_FP64, &s)) return rc;
+  s->nrhs = nrhs;
+  const Geo& g = s->g;
+  const size_t nb = sizeof(double) * (size_t)g.n * nrhs;
+  const dim3 ag = ax_grid(g);
+  const size_t parts = (size_t)nrhs * 2 * std::max((size_t)ag.x * ag.y * ag.z, (size_t)elementwise_blocks(s));
+  auto al = [&](void** ptr, size_t bytes) {
+    return cudaMalloc(ptr, bytes) == cudaSuccess && cudaMemset(*ptr, 0, bytes) == cudaSuccess;
+  };
+  bool ok = al((void**)&s->mr_th, nb) && al((void**)&s->mr_b, nb) &&
+            al((void**)&s->mr_st, sizeof(SolverState) * nrhs) && al((void**)&s->mr_ctl, sizeof(MultiCtl)) &&
+            al((void**)&s->mr_partials, sizeof(double) * parts) && al((void**)&s->mr_flag, sizeof(int));
+  for (auto& p : s->mr_kv) ok = ok && al((void**)&p, nb);
+  if (!ok) {
+    destroy(s);
+    return fail(H2G_CUDA_ERROR, "cudaMalloc of the %d right-hand sides failed", nrhs);
+  }
+  *out = static_cast<h2g_solver*>(s);
+  return H2G_OK;
+}
+
+static int check_multi(h2g_solver* h) {
+  if (int rc = h2g::check_handle(h)) return rc;
+  if (S(h)->nrhs < 1) return fail(H2G_BAD_ARG, "not a multi right-hand-side handle (h2g_create_multi)");
+  return H2G_OK;
+}
+
+int h2g_set_rhs_multi(h2g_solver* h, const double* b) {
+  if (int rc = check_multi(h)) return rc;
+  Solver* s = S(h);
+  if (!b) return fail(H2G_BAD_ARG, "null host array");
+  for (int q = 0; q < s->nrhs; ++q)
+    if (int rc = h2g::upload<double>(s, b + (size_t)q * s->nfort(), s->mr_b + (size_t)q * s->g.n)) return rc;
+  return H2G_OK;
+}
+
+int h2g_set_theta_multi(h2g_solver* h, const double* theta) {
+  if (int rc = check_multi(h)) return rc;
+  Solver* s = S(h);
+  if (!theta) return fail(H2G_BAD_ARG, "null host array");
+  for (int q = 0; q < s->nrhs; ++q)
+    if (int rc = h2g::upload<double>(s, theta + (size_t)q * s->nfort(), s->mr_th + (size_t)q * s->g.n)) return rc;
+  return H2G_OK;
+}
+
+int h2g_get_theta_multi(h2g_solver* h, double* theta) {
+  if (int rc = check_multi(h)) return rc;
+  Solver* s = S(h);
+  if (!theta) return fail(H2G_BAD_ARG, "null host array");
+  for (int q = 0; q < s->nrhs; ++q)
+    if (int rc = h2g::download<double>(s, s->mr_th + (size_t)q * s->g.n, theta + (size_t)q * s->nfort())) return rc;
+  return H2G_OK;
+}
+
+int h2g_pbicgstab_multi(h2g_solver* h, double tol, int maxItr, int smoother, h2g_result* outs) {
+  if (int rc = check_multi(h)) return rc;
+  return h2g::solve_multi(S(h), tol, maxItr, smoother, outs);
 }
 
 int h2g_set_sweep(h2g_solver* h, int fused, int chunks, int dd_array) {

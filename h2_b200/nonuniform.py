@@ -265,6 +265,48 @@ class Solver:
         return n.value
 
 
+class MultiSolver(Solver):
+    """One operator, K right-hand sides (h2g_create_multi): the members of a batch that share a grid
+    size.  Grid and fields as for Solver; b and theta per right-hand side; one solve runs all K
+    PBiCGSTAB! iterations together, each with its lone solve's bits."""
+
+    def __init__(self, MX: int, MY: int, MZ: int, nrhs: int, stream: int | None = None):
+        self.lib = L.load()
+        h = C.c_void_p()
+        L.check(self.lib.h2g_create_multi(MX, MY, MZ, int(nrhs), C.byref(h)))
+        self.h = h
+        self.shape = (MX, MY, MZ)
+        self.precision = "fp64"
+        self.nrhs = int(nrhs)
+        if stream is not None:
+            L.check(self.lib.h2g_set_stream(self.h, C.c_void_p(stream)))
+
+    def _stack(self, arrays, name):
+        if len(arrays) != self.nrhs:
+            raise ValueError(f"{name}: {len(arrays)} arrays for {self.nrhs} right-hand sides")
+        out = np.empty(self.shape + (self.nrhs,), order="F")
+        for q, a in enumerate(arrays):
+            out[..., q] = self._arr(a, name)
+        return out
+
+    def set_rhs_multi(self, bs):
+        L.check(self.lib.h2g_set_rhs_multi(self.h, _ptr(self._stack(bs, "b"))))
+
+    def set_theta_multi(self, thetas):
+        L.check(self.lib.h2g_set_theta_multi(self.h, _ptr(self._stack(thetas, "theta"))))
+
+    def get_theta_multi(self) -> list:
+        out = np.empty(self.shape + (self.nrhs,), order="F")
+        L.check(self.lib.h2g_get_theta_multi(self.h, _ptr(out)))
+        return [np.asfortranarray(out[..., q]) for q in range(self.nrhs)]
+
+    def solve_multi(self, tol=1e-6, maxItr=20_000, smoother="gs"):
+        outs = (L.Result * self.nrhs)()
+        st = self.lib.h2g_pbicgstab_multi(self.h, float(tol), int(maxItr), smoother_selector(smoother), outs)
+        L.check(st, allowed=(L.H2G_OK, L.H2G_NOT_CONVERGED, L.H2G_BREAKDOWN, L.H2G_NONFINITE))
+        return st, list(outs)
+
+
 def _dh(dh):
     if len(dh) < 2:
         raise ValueError("Δh must hold (dx, dy[, dz])")

@@ -164,6 +164,23 @@ int h2g_release_cached(void);
 int h2g_batch_solve(int n, h2g_solver *const *hs, int method, double tol, int maxItr, int smoother, int threads,
                     h2g_result *outs);
 
+/* ---- K right-hand sides on one operator (no reference counterpart) ------------------------
+ * The batched workload's members of one grid size share the operator (geometry, materials,
+ * boundary set) and differ in their heat maps, so in b.  h2g_create_multi makes an FP64 handle for
+ * nrhs (1..64) right-hand sides: grid and fields are set once with h2g_set_grid / h2g_set_fields;
+ * b and theta of every right-hand side with h2g_set_rhs_multi / h2g_set_theta_multi (nrhs
+ * column-major arrays of MX*MY*MZ doubles one after another; h2g_get_theta_multi reads them back).
+ * h2g_pbicgstab_multi runs PBiCGSTAB! + RB-GS (smoother 1 only) for all of them at once: every
+ * stencil kernel computes a cell's coefficients once for a group of right-hand sides, and each
+ * right-hand side keeps its own scalars, stop test and result (outs[nrhs]); its iterates and
+ * result are bit for bit those of its lone solve (h2g_pbicgstab).  Returns H2G_OK when every
+ * right-hand side converged, else the first other status. */
+int h2g_create_multi(int MX, int MY, int MZ, int nrhs, h2g_solver **out);
+int h2g_set_rhs_multi(h2g_solver *h, const double *b);
+int h2g_set_theta_multi(h2g_solver *h, const double *theta);
+int h2g_get_theta_multi(h2g_solver *h, double *theta);
+int h2g_pbicgstab_multi(h2g_solver *h, double tol, int maxItr, int smoother, h2g_result *outs);
+
 /* ---- steady adjoint (no reference counterpart) -------------------------------------------
  * Gradient of J = (sum_c w_c θ_c^p)^(1/p) (w_c >= 0 per cell, column-major with guards, e.g.
  * the cell volume on the silicon cells and 0 elsewhere; p >= 1) where θ solves the handle's
