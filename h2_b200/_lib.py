@@ -91,6 +91,8 @@ _SIGS = {
     "h2g_pbicgstab_multi": (C.c_int, [_vp, C.c_double, C.c_int, C.c_int, C.POINTER(Result)]),
     "h2g_set_sweep": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int]),
     "h2g_get_sweep": (C.c_int, [_vp, _ip, _ip, _ip]),
+    "h2g_set_coop": (C.c_int, [_vp, C.c_int]),
+    "h2g_get_coop": (C.c_int, [_vp, _ip]),
     "h2g_set_wait_limit": (C.c_int, [_vp, C.c_longlong]),
     "h2g_release_cached": (C.c_int, []),
     "h2g_calcax": (C.c_int, [_vp, _dp, _dp]),

@@ -17,7 +17,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libh2g.so")
 # (source, extra flags): the model builder is compiled without FMA contraction
 SOURCES = [("h2g_solver.cu", []), ("h2g_model.cu", ["-fmad=false"]), ("h2g_noalloc.cu", [])]
-DEPS = ["h2g_internal.cuh", "h2g_kernels.cuh", "h2g_sweep.cuh", "h2g_multi.cuh", os.path.join("..", "..", "include", "h2g.h")]
+DEPS = ["h2g_internal.cuh", "h2g_kernels.cuh", "h2g_sweep.cuh", "h2g_multi.cuh", "h2g_coop.cuh", os.path.join("..", "..", "include", "h2g.h")]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

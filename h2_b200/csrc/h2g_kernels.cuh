@@ -377,10 +377,18 @@ constexpr unsigned kFull = 0xffffffffu;
 
 template <typename T>
 __device__ __forceinline__ T ldro(const T* p) { return __ldg(p); }
+// Loads of a vector that this launch itself writes (the cooperative preconditioner, whose passes
+// read what other blocks wrote before a grid barrier) go through the coherent path: ld.global.ca
+// obeys the memory model's acquire/release ordering, the read-only path does not.
+template <bool NC, typename T>
+__device__ __forceinline__ T ldx(const T* p) {
+  if constexpr (NC) return __ldg(p);
+  else return __ldca(p);
+}
 
 // x-neighbours of a colour-c cell at position p with parity e (x-1 = o[p-1+e], x+1 = o[p+e]),
 // given the o-colour value and key of this lane's column at that plane.  All lanes must call it.
-template <typename T, bool VAL, typename TI = T, bool KEYS = true>
+template <typename T, bool VAL, typename TI = T, bool KEYS = true, bool NC = true>
 __device__ __forceinline__ void x_nbrs(T oc, int okc, int e, int lane, int p, int HN, const TI* x,
                                        const uint8_t* key, int rowo, T& xm, T& xp, int& kxm, int& kxp) {
 #if H2G_XNB_LOAD
@@ -390,7 +398,7 @@ __device__ __forceinline__ void x_nbrs(T oc, int okc, int e, int lane, int p, in
   T other = T(0);
   int ko = 0;
   if (q >= 0 && q < HN) {
-    if (VAL) other = (T)ldro(x + rowo + q);
+    if (VAL) other = (T)ldx<NC>(x + rowo + q);
     if (KEYS) ko = key[rowo + q];
   }
   if (e) {
@@ -430,7 +438,7 @@ __device__ __forceinline__ void x_nbrs(T oc, int okc, int e, int lane, int p, in
 // returns the sum of the squared SOR residuals r = (dd + omega*(c_xm + c_ym + c_zm))*dp/omega of
 // the updated cells (rbsor_core!, NonUniform.jl:907-908); the preconditioner discards them and
 // skips the work.  With NP = 2 the two cells share the o-colour column loads.
-template <typename T, bool RES, int NP = 2, bool DD = true>
+template <typename T, bool RES, int NP = 2, bool DD = true, bool NC = true>
 __device__ __forceinline__ double rb_pass_column(const OpParams<T>& op, T* x, const T* __restrict__ bb, int color,
                                                  T omega, int lane, int p, int j, int k0) {
   const Geo& g = op.g;
@@ -449,7 +457,7 @@ __device__ __forceinline__ double rb_pass_column(const OpParams<T>& op, T* x, co
     kcol[t] = 0;
     if (pok && k0 - 1 + t <= g.MZ - 1) {
       const int a = ro0 + (t - 1) * PL + p;
-      col[t] = ldro(x + a);
+      col[t] = ldx<NC>(x + a);
       if (!NK) kcol[t] = key[a];
     }
   }
@@ -466,8 +474,8 @@ __device__ __forceinline__ double rb_pass_column(const OpParams<T>& op, T* x, co
     nk[u] = 0ull;
     if (ok[u]) {
       const int ao = ro0 + u * PL + p, ac = rc0 + u * PL + p;
-      ym[u] = ldro(x + ao - HP2);
-      yp[u] = ldro(x + ao + HP2);
+      ym[u] = ldx<NC>(x + ao - HP2);
+      yp[u] = ldx<NC>(x + ao + HP2);
       if (NK) {
         nk[u] = __ldg(op.nkey + ac);
       } else {
@@ -476,7 +484,7 @@ __device__ __forceinline__ double rb_pass_column(const OpParams<T>& op, T* x, co
         kc[u] = key[ac];
       }
       pp[u] = x[ac];
-      bv[u] = bb[ac];
+      bv[u] = NC ? bb[ac] : ldx<false>(bb + ac);
     }
   }
   T xm[NP], xp[NP];
@@ -484,8 +492,8 @@ __device__ __forceinline__ double rb_pass_column(const OpParams<T>& op, T* x, co
 #pragma unroll
   for (int u = 0; u < NP; ++u) {
     const int e = (1 + color + j + k0 + u) & 1;
-    x_nbrs<T, true, T, !NK>(col[u + 1], kcol[u + 1], e, lane, p, g.HN, x, key, ro0 + u * PL, xm[u], xp[u], kxm[u],
-                            kxp[u]);
+    x_nbrs<T, true, T, !NK, NC>(col[u + 1], kcol[u + 1], e, lane, p, g.HN, x, key, ro0 + u * PL, xm[u], xp[u],
+                                kxm[u], kxp[u]);
   }
   double acc = 0.0;
 #pragma unroll
@@ -570,17 +578,11 @@ __global__ void __launch_bounds__(kThreads) k_sor_pass(OpParams<double> op, doub
 // smoother's copy of the right-hand side in T.  Thread = both colours of column (p,j) at plane k.
 // ------------------------------------------------------------------------------------------
 template <typename T, typename TV, int VM>
-__global__ void __launch_bounds__(kThreads) k_rb_first(OpParams<T> op, T* __restrict__ xx, TV* __restrict__ v,
-                                                        T* __restrict__ bbT, const TV* __restrict__ r,
-                                                        const TV* __restrict__ q, const SolverState* __restrict__ st,
-                                                        int copy_only) {
-  pdl_enter();
-  if (st && st->stop) return;
+__device__ __forceinline__ void rb_first_column(const OpParams<T>& op, T* __restrict__ xx, TV* __restrict__ v,
+                                                T* __restrict__ bbT, const TV* __restrict__ r,
+                                                const TV* __restrict__ q, const SolverState* __restrict__ st,
+                                                int copy_only, int lane, int p, int j, int k) {
   const Geo& g = op.g;
-  const int lane = threadIdx.x, p = blockIdx.x * kBX + lane;
-  const int j = 1 + blockIdx.y * kBY + threadIdx.y;
-  const int k = 1 + blockIdx.z;
-  if (j > g.NY) return;
   const bool pok = p < g.HN;
   const uint8_t* key = op.key;
   const int HP2 = 2 * g.HP, PL = (int)g.plane;
@@ -661,6 +663,20 @@ __global__ void __launch_bounds__(kThreads) k_rb_first(OpParams<T> op, T* __rest
     }
     xx[ci] = out;
   }
+}
+
+template <typename T, typename TV, int VM>
+__global__ void __launch_bounds__(kThreads) k_rb_first(OpParams<T> op, T* __restrict__ xx, TV* __restrict__ v,
+                                                        T* __restrict__ bbT, const TV* __restrict__ r,
+                                                        const TV* __restrict__ q, const SolverState* __restrict__ st,
+                                                        int copy_only) {
+  pdl_enter();
+  if (st && st->stop) return;
+  const int lane = threadIdx.x, p = blockIdx.x * kBX + lane;
+  const int j = 1 + blockIdx.y * kBY + threadIdx.y;
+  const int k = 1 + blockIdx.z;
+  if (j > op.g.NY) return;
+  rb_first_column<T, TV, VM>(op, xx, v, bbT, r, q, st, copy_only, lane, p, j, k);
 }
 
 // Both colours of column (p, j) at plane k: the values (centre and z-neighbours) and keys of the

@@ -28,6 +28,7 @@
 #include "../../include/h2g.h"
 #include "h2g_sweep.cuh"
 #include "h2g_multi.cuh"
+#include "h2g_coop.cuh"
 
 namespace h2g {
 
@@ -170,7 +171,13 @@ struct Solver {
   int sweep_forced = -1;   // h2g_set_sweep: -1 tuner, 0 colour passes, 1 fused
   double* x2_64 = nullptr;
   float* x2_32 = nullptr;
-  int* sweep_err = nullptr;            // set by a fused sweep whose bounded wait ran out
+  int* sweep_err = nullptr;            // set by a fused sweep or grid barrier whose bounded wait ran out
+  // cooperative preconditioner (k_precond_coop): all 10 passes of Preconditioner! in one launch
+  int rb_coop = 0;          // chosen (tuner or h2g_set_coop)
+  int coop_forced = -1;     // h2g_set_coop: -1 tuner, 0 off, 1 on
+  int coop_blocks = 0;      // blocks of the launch: SMs x resident blocks per SM
+  bool coop_barred = false; // set while h2g_batch_solve runs the handle beside others
+  GridBar* gbar = nullptr;
   long long wait_limit = kWaitCycles;  // budget of one bounded wait (clock cycles)
   std::map<std::pair<const void*, int>, CUtensorMap> xmaps;  // TMA maps of x buffers (pointer, bytes/element)
   // K right-hand sides on the handle's operator (h2g_create_multi): stacked vectors, K states
@@ -383,14 +390,58 @@ static int launch_sweep(Solver* s, cudaStream_t cs, const OpParams<T>& op, const
   return H2G_OK;
 }
 
-// H2G_TIMEOUT (and the flag cleared) if a fused sweep's bounded wait ran out since the last check.
+// H2G_TIMEOUT (and the flag and grid barrier reset) if a bounded wait of a fused sweep or of the
+// cooperative preconditioner's grid barrier ran out since the last check.
 static int sweep_status(Solver* s) {
   int e = 0;
   CK(cudaMemcpy(&e, s->sweep_err, sizeof(int), cudaMemcpyDeviceToHost));
   if (!e) return H2G_OK;
   CK(cudaMemset(s->sweep_err, 0, sizeof(int)));
-  return fail(H2G_TIMEOUT, "a bounded wait of the fused RB-GS sweep ran out");
+  CK(cudaMemset(s->gbar, 0, sizeof(GridBar)));
+  return fail(H2G_TIMEOUT, "a bounded wait of the RB-GS preconditioner ran out");
 }
+
+// Blocks of the cooperative preconditioner: every SM's resident blocks, so that all of them run
+// at once (the cooperative launch checks it).
+template <int VM, int NP, bool DD>
+static int coop_grid(Solver* s) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_precond_coop<VM, NP, DD>, kThreads, 0) != cudaSuccess ||
+      per_sm < 1)
+    return 0;
+  return per_sm * s->num_sms;
+}
+
+template <int VM, int NP, bool DD>
+static int launch_coop_np(Solver* s, cudaStream_t cs, const OpParams<double>& op, double* xx, double* v,
+                          const double* r, const double* q, SolverState* st) {
+  const int nblk = coop_grid<VM, NP, DD>(s);
+  if (nblk < 1) return fail(H2G_CUDA_ERROR, "no resident block for the cooperative preconditioner");
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(nblk);
+  cfg.blockDim = dim3(kBX, kBY);
+  cfg.stream = cs;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  if (cudaLaunchKernelEx(&cfg, k_precond_coop<VM, NP, DD>, op, xx, v, r, q, st, s->gbar, s->sweep_err,
+                         s->wait_limit) != cudaSuccess)
+    return fail(H2G_CUDA_ERROR, "cooperative launch of %d blocks failed: %s", nblk,
+                cudaGetErrorString(cudaGetLastError()));
+  return H2G_OK;
+}
+template <int VM>
+static int launch_coop(Solver* s, cudaStream_t cs, const OpParams<double>& op, double* xx, double* v,
+                       const double* r, const double* q, SolverState* st) {
+  if (s->rb_planes == 1)
+    return s->rb_dd ? launch_coop_np<VM, 1, true>(s, cs, op, xx, v, r, q, st)
+                    : launch_coop_np<VM, 1, false>(s, cs, op, xx, v, r, q, st);
+  return s->rb_dd ? launch_coop_np<VM, 2, true>(s, cs, op, xx, v, r, q, st)
+                  : launch_coop_np<VM, 2, false>(s, cs, op, xx, v, r, q, st);
+}
+static bool use_coop(const Solver* s) { return s->rb_coop && !s->coop_barred && !s->rb_fused; }
 
 template <typename T>
 static T* x2buf(Solver* s);
@@ -445,6 +496,9 @@ static int launch_precond(Solver* s, cudaStream_t cs, const OpParams<T>& op, T* 
   }
   // k_rb_first updates v in place (VM 1 reads and writes p there)
   TV* v = VM == 0 ? vin : vout;
+  if constexpr (std::is_same<T, double>::value && std::is_same<TV, double>::value) {
+    if (use_coop(s) && !none && !bbT) return launch_coop<VM>(s, cs, op, xx, v, r, q, st);
+  }
   launch(s, k_rb_first<T, TV, VM>, first_grid(op.g), dim3(kBX, kBY), cs, op, xx, v, bbT, r, q, st, none);
   if (none) return H2G_OK;
   for (int pass = 1; pass < 2 * kSweeps; ++pass) launch_rb<T>(s, cs, op, xx, bb, pass & 1, T(1), st);
@@ -534,7 +588,7 @@ static void destroy(Solver* s) {
   for (auto& p : s->kv) cudaFree(p);
   for (auto& p : s->hook) cudaFree(p);
   for (auto& p : s->stage) cudaFree(p);
-  cudaFree(s->x2_64); cudaFree(s->x2_32); cudaFree(s->sweep_err);
+  cudaFree(s->x2_64); cudaFree(s->x2_32); cudaFree(s->sweep_err); cudaFree(s->gbar);
   s->mr_graph.reset();
   cudaFree(s->mr_th); cudaFree(s->mr_b); cudaFree(s->mr_st); cudaFree(s->mr_ctl); cudaFree(s->mr_partials);
   cudaFree(s->mr_flag);
@@ -836,6 +890,7 @@ static int get_graph(Solver* s, int kind, int smoother, const OpParams<T>& op, c
                      SolverState* st, SolveGraph** out) {
   SolveGraph& G = s->graphs[kind][smoother ? 1 : 0];
   std::vector<unsigned char> sig = signature(op, opM, smoother, (const void*)x);
+  sig.push_back(use_coop(s) ? 1 : 0);
   if (G.exec && G.sig == sig) {
     *out = &G;
     return H2G_OK;
@@ -941,14 +996,15 @@ static void print_log(const SolverState& st, const double* hist, int nhist, int 
 
 // Kernels of one preconditioner call: the first pass and 9 colour passes, or 5 fused sweeps (the
 // first one with the Krylov update).
-static int precond_kernels(const Solver* s, int smoother) {
-  if (smoother == H2G_SMOOTHER_NONE) return 1;
+static int precond_kernels(const Solver* s, int smoother, bool coop = false) {
+  if (smoother == H2G_SMOOTHER_NONE || coop) return 1;
   return s->rb_fused ? kSweeps : 2 * kSweeps;
 }
 
-// Kernels in one WHILE-body pass (one Krylov iteration).
-static long long body_kernels(const Solver* s, bool cg, int smoother) {
-  const int pc = precond_kernels(s, smoother);
+// Kernels in one WHILE-body pass (one Krylov iteration); coop: the preconditioner is the one
+// cooperative launch (FP64 smoother).
+static long long body_kernels(const Solver* s, bool cg, int smoother, bool coop = false) {
+  const int pc = precond_kernels(s, smoother, coop);
   return cg ? (1 + 1 + pc + 1 + 1) : (2 * pc + 2 + 1);
 }
 
@@ -998,8 +1054,9 @@ static int solve_krylov(Solver* s, bool cg, double tol, int maxItr, int smoother
   const int nprint = (fin.reason == kBreakdown || fin.reason == kNonFinite) ? std::min(nh, std::max(0, fin.itr - 1)) : nh;
   if (verbose) print_log(fin, hh.data(), nprint, fin.converged);
   if (out) {
-    const long long body = body_kernels(s, cg, smoother);
-    const long long pre = 2 + (cg ? precond_kernels(s, smoother) + 1 : 0);
+    const bool coop = std::is_same<TP, double>::value && use_coop(s);
+    const long long body = body_kernels(s, cg, smoother, coop);
+    const long long pre = 2 + (cg ? precond_kernels(s, smoother, coop) + 1 : 0);
     out->launches = pre + body * std::max(1, fin.itr);
     out->isconverged = fin.converged;
     out->itr = fin.itr;
@@ -1905,6 +1962,8 @@ static int autotune(Solver* s) {
     chunks = s->sweep_forced ? s->sw_chunks : -1;
     swdd = s->sweep_forced ? (s->sw_dda ? 1 : 0) : -1;
   }
+  // the cooperative preconditioner runs on the colour-pass path: asking for it fixes that path
+  if (s->coop_forced == 1 && s->sweep_forced != 1) fused = 0;
   if (chunks > s->g.NZ) chunks = s->g.NZ;
   const bool sweep_known = fused == 0 || (fused == 1 && chunks > 0 && swdd >= 0);
   if (rows < 0 || planes < 0 || rbdd < 0 || dd < 0 || !sweep_known) {
@@ -1962,9 +2021,17 @@ static int autotune(Solver* s) {
     chunks = s->sw_chunks;
     swdd = s->sw_dda ? 1 : 0;
   }
+  // the cooperative preconditioner (FP64 handles, colour-pass path): on request only
+  int coop = s->coop_forced;
+  if (coop < 0) {
+    coop = 0;
+    if (const char* e = getenv("H2G_RB_COOP")) coop = atoi(e) ? 1 : 0;
+  }
+  if (s->precision != H2G_FP64 || fused == 1) coop = 0;
   if (rows != s->rb_rows || planes != s->rb_planes || (rbdd != 0) != s->rb_dd || (dd != 0) != s->ax_dd ||
-      (fused == 1) != s->rb_fused || chunks != s->sw_chunks || (swdd != 0) != s->sw_dda)
+      (fused == 1) != s->rb_fused || chunks != s->sw_chunks || (swdd != 0) != s->sw_dda || coop != s->rb_coop)
     invalidate_graphs(s);
+  s->rb_coop = coop;
   s->rb_rows = rows;
   s->rb_planes = planes;
   s->rb_dd = rbdd != 0;
@@ -2016,6 +2083,7 @@ static int create(int MX, int MY, int MZ, int precision, Solver** out) {
   AL(s->x2_64, nb);
   if (precision != H2G_FP64) AL(s->x2_32, sizeof(float) * (size_t)g.n);
   AL(s->sweep_err, sizeof(int));
+  AL(s->gbar, sizeof(GridBar));
   if (precision == H2G_MIXED_IR) {
     AL(s->kv[KE], kvb);
     AL(s->r64, nb);
@@ -2474,6 +2542,9 @@ int h2g_batch_solve(int n, h2g_solver* const* hs, int method, double tol, int ma
   // other's vectors from L2 (measured on the 64-member workload: 1 -> 3.55 s, 2 -> 3.05 s,
   // 4 -> 3.46 s, 16 -> 3.63 s)
   const int nt = std::max(1, std::min(threads > 0 ? threads : 2, n));
+  // a cooperative launch needs the whole device: handles that run beside others use the colour
+  // passes
+  for (int q = 0; q < n; ++q) S(hs[q])->coop_barred = nt > 1;
   std::atomic<int> next(0);
   std::vector<std::string> errs(n);
   auto work = [&]() {
@@ -2498,6 +2569,7 @@ int h2g_batch_solve(int n, h2g_solver* const* hs, int method, double tol, int ma
     cudaSetDevice(s->device);
     cudaStreamSynchronize(own[q]);
     s->stream = saved[q];
+    s->coop_barred = false;
     cudaStreamDestroy(own[q]);
   }
   int worst = H2G_OK;
@@ -2636,6 +2708,30 @@ int h2g_set_sweep(h2g_solver* h, int fused, int chunks, int dd_array) {
   }
   s->rb_tuned = false;  // the next solve applies the choice (and tunes what is left free)
   h2g::invalidate_graphs(s);
+  return H2G_OK;
+}
+
+int h2g_set_coop(h2g_solver* h, int mode) {
+  if (int rc = h2g::check_handle(h)) return rc;
+  Solver* s = S(h);
+  if (mode < -1 || mode > 1) return fail(H2G_BAD_ARG, "mode must be -1 (default), 0 or 1");
+  if (mode == 1 && s->precision != H2G_FP64)
+    return fail(H2G_UNSUPPORTED, "the cooperative preconditioner runs on FP64 handles");
+  s->coop_forced = mode;
+  if (mode == 1 && s->sweep_forced == 1) s->sweep_forced = 0;
+  s->rb_tuned = false;
+  h2g::invalidate_graphs(s);
+  return H2G_OK;
+}
+
+int h2g_get_coop(h2g_solver* h, int* on) {
+  if (int rc = h2g::check_handle(h)) return rc;
+  Solver* s = S(h);
+  if (!on) return fail(H2G_BAD_ARG, "null output");
+  if (!s->grid_set || !s->fields_set) return fail(H2G_BAD_ARG, "h2g_set_grid and h2g_set_fields must come first");
+  CK(cudaSetDevice(s->device));
+  if (int rc = h2g::autotune(s)) return rc;
+  *on = s->rb_coop;
   return H2G_OK;
 }
 

@@ -255,6 +255,16 @@ class Solver:
         L.check(self.lib.h2g_get_sweep(self.h, C.byref(f), C.byref(c), C.byref(d)))
         return bool(f.value), c.value, bool(d.value)
 
+    def set_coop(self, mode: int):
+        """The PBiCGSTAB preconditioner as one cooperative launch: 1 on, 0 off, -1 default."""
+        L.check(self.lib.h2g_set_coop(self.h, int(mode)))
+
+    def coop(self) -> bool:
+        """Whether the next solve runs the cooperative preconditioner."""
+        on = C.c_int(0)
+        L.check(self.lib.h2g_get_coop(self.h, C.byref(on)))
+        return bool(on.value)
+
     def set_wait_limit(self, cycles: int):
         """Budget of one bounded device wait in clock cycles (0: every wait gives up at once)."""
         L.check(self.lib.h2g_set_wait_limit(self.h, int(cycles)))

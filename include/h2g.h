@@ -249,10 +249,20 @@ int h2g_set_tuning(h2g_solver *h, int rows, int planes);
  * after another over the whole grid). */
 int h2g_set_sweep(h2g_solver *h, int fused, int chunks, int dd_array);
 int h2g_get_sweep(h2g_solver *h, int *fused, int *chunks, int *dd_array);
-/* Budget of one bounded device wait (the fused sweep's waits for its TMA copies), in SM clock
- * cycles; default about one second.  0 makes every such wait give up at once: the solve then ends
- * with H2G_TIMEOUT, the copies in flight are drained and the context stays usable (the failure
- * path of the bounded waits, exercised by the tests without a GPU fault). */
+/* The whole preconditioner of a PBiCGSTAB iteration (first pass and 9 colour passes) as one
+ * cooperative launch with a bounded grid barrier between passes (k_precond_coop), instead of ten
+ * launches; results bit-identical.  FP64 handles on the colour-pass path only.  mode 1 on, 0 off,
+ * -1 default (off unless H2G_RB_COOP=1 in the environment).  h2g_batch_solve runs its handles
+ * without it while more than one solve is in flight (a cooperative launch needs the device to
+ * itself; beside another cooperative launch a barrier would wait until its budget ran out).
+ * h2g_get_coop reports what the next solve uses.  No reference counterpart. */
+int h2g_set_coop(h2g_solver *h, int mode);
+int h2g_get_coop(h2g_solver *h, int *on);
+/* Budget of one bounded device wait (the fused sweep's waits for its TMA copies, the cooperative
+ * preconditioner's grid barriers), in SM clock cycles; default about one second.  0 makes every
+ * such wait give up at once: the solve then ends with H2G_TIMEOUT, copies in flight are drained
+ * and the context stays usable (the failure path of the bounded waits, exercised by the tests
+ * without a GPU fault). */
 int h2g_set_wait_limit(h2g_solver *h, long long cycles);
 
 /* ---- kernels of the path, callable one at a time (host arrays in and out) ---------------
