@@ -111,7 +111,7 @@ struct TileWalk {
 // colour passes on xx with right-hand side v.
 // Tiles of the first pass: the first_grid blocks (32 x kBY columns of one plane); of the colour
 // passes: the rb_grid blocks with NP planes per thread.  Block (32, kBY).
-template <int VM, int NP, bool DD>
+template <int VM, int NP, int DDM>
 __global__ void __launch_bounds__(kThreads, H2G_MINB)
     k_precond_coop(OpParams<double> op, double* xx, double* v, const double* __restrict__ r,
                    const double* __restrict__ q, SolverState* st, GridBar* bar, int* err, long long limit) {
@@ -123,7 +123,7 @@ __global__ void __launch_bounds__(kThreads, H2G_MINB)
   // first pass, fused with the Krylov update
   for (TileWalk w(blockIdx.x, nblocks, gx, gy, g.NZ); w.valid(); w.next()) {
     const int p = w.bx * kBX + lane, j = 1 + w.by * kBY + ty, k = 1 + w.bz;
-    if (j <= g.NY) rb_first_column<double, double, VM>(op, xx, v, nullptr, r, q, st, 0, lane, p, j, k);
+    if (j <= g.NY) rb_first_column<double, double, VM, DDM == 2>(op, xx, v, nullptr, r, q, st, 0, lane, p, j, k);
   }
   const TileWalk w0(blockIdx.x, nblocks, gx, gy, (g.NZ + NP - 1) / NP);
   for (int pass = 1; pass < 2 * kSweeps; ++pass) {
@@ -131,7 +131,7 @@ __global__ void __launch_bounds__(kThreads, H2G_MINB)
     const int color = pass & 1;
     for (TileWalk w = w0; w.valid(); w.next()) {
       const int p = w.bx * kBX + lane, j = 1 + w.by * kBY + ty, k0 = 1 + NP * w.bz;
-      if (j <= g.NY) rb_pass_column<double, false, NP, DD, false>(op, xx, v, color, 1.0, lane, p, j, k0);
+      if (j <= g.NY) rb_pass_column<double, false, NP, DDM, false>(op, xx, v, color, 1.0, lane, p, j, k0);
     }
   }
 }

@@ -303,6 +303,32 @@ __device__ __forceinline__ bool cell_coef(const OpParams<T>& op, int k, uint8_t 
   return true;
 }
 
+// Stencil classes (FP64).  The coefficients of a cell depend only on its plane k and the 7 key
+// bytes of its stencil, so the cells of a grid fall into few classes: one per distinct (k, keys)
+// pair.  k_class_coef fills one table row per class with cell_coef itself, for a steady grid, so
+// every value is the one cell_coef gives the cell; a cell then reads a 2-byte class index and one
+// 64-byte row instead of the 8-byte key word, six table entries and dd.  A transient grid adds
+// a_p0 per cell, so there dd is read from the per-cell array (the same value again).
+constexpr unsigned kNoClass = 0xffffu;
+constexpr int kClassSlots = 1 << 17;   // hash slots of the (plane, keys) pairs
+constexpr int kMaxClasses = 65535;     // class indices are 16-bit; 0xffff marks "not updated"
+
+template <typename T>
+__device__ __forceinline__ bool class_coef(const OpParams<T>& op, unsigned cl, int ci, Coef<T>& c) {
+  static_assert(sizeof(T) == 8, "stencil classes are FP64 only");
+  if (cl == kNoClass) return false;
+  const double2* t = reinterpret_cast<const double2*>(op.ctab) + 4 * cl;
+  const double2 a = __ldg(t), b = __ldg(t + 1), z = __ldg(t + 2);
+  c.cxm = a.x;
+  c.cxp = a.y;
+  c.cym = b.x;
+  c.cyp = b.y;
+  c.czm = z.x;
+  c.czp = z.y;
+  c.dd = op.steady ? __ldg(reinterpret_cast<const double*>(t + 3)) : __ldg(op.ddv + ci);
+  return true;
+}
+
 // ss of NonUniform.jl:505-507 (products summed left to right).  FP64: separately rounded, as the
 // reference.  FP32 (the mixed smoother): fused multiply-adds, written out so that every launch
 // shape computes the same bits.
@@ -438,7 +464,7 @@ __device__ __forceinline__ void x_nbrs(T oc, int okc, int e, int lane, int p, in
 // returns the sum of the squared SOR residuals r = (dd + omega*(c_xm + c_ym + c_zm))*dp/omega of
 // the updated cells (rbsor_core!, NonUniform.jl:907-908); the preconditioner discards them and
 // skips the work.  With NP = 2 the two cells share the o-colour column loads.
-template <typename T, bool RES, int NP = 2, bool DD = true, bool NC = true>
+template <typename T, bool RES, int NP = 2, int DDM = 1, bool NC = true>
 __device__ __forceinline__ double rb_pass_column(const OpParams<T>& op, T* x, const T* __restrict__ bb, int color,
                                                  T omega, int lane, int p, int j, int k0) {
   const Geo& g = op.g;
@@ -450,7 +476,8 @@ __device__ __forceinline__ double rb_pass_column(const OpParams<T>& op, T* x, co
   // o-colour column at (p, j), planes k0-1 .. k0+NP
   T col[NP + 2];
   int kcol[NP + 2];
-  constexpr bool NK = H2G_NKEY != 0;
+  constexpr bool CL = DDM == 2;                // coefficients from the class table
+  constexpr bool NK = H2G_NKEY != 0 || CL;     // no key bytes loaded one by one
 #pragma unroll
   for (int t = 0; t < NP + 2; ++t) {
     col[t] = T(0);
@@ -464,6 +491,7 @@ __device__ __forceinline__ double rb_pass_column(const OpParams<T>& op, T* x, co
   T ym[NP], yp[NP], pp[NP], bv[NP];
   int kym[NP], kyp[NP], kc[NP];
   unsigned long long nk[NP];
+  unsigned cl[NP];
   bool ok[NP];
 #pragma unroll
   for (int u = 0; u < NP; ++u) {
@@ -472,11 +500,14 @@ __device__ __forceinline__ double rb_pass_column(const OpParams<T>& op, T* x, co
     ym[u] = yp[u] = pp[u] = bv[u] = T(0);
     kym[u] = kyp[u] = kc[u] = 0;
     nk[u] = 0ull;
+    cl[u] = kNoClass;
     if (ok[u]) {
       const int ao = ro0 + u * PL + p, ac = rc0 + u * PL + p;
       ym[u] = ldx<NC>(x + ao - HP2);
       yp[u] = ldx<NC>(x + ao + HP2);
-      if (NK) {
+      if (CL) {
+        cl[u] = __ldg(op.cls + ac);
+      } else if (NK) {
         nk[u] = __ldg(op.nkey + ac);
       } else {
         kym[u] = key[ao - HP2];
@@ -502,12 +533,15 @@ __device__ __forceinline__ double rb_pass_column(const OpParams<T>& op, T* x, co
     const int ac = rc0 + u * PL + p;
     Coef<T> c;
     bool has;
-    if (NK) {
+    if constexpr (CL) {
+      has = class_coef<T>(op, cl[u], ac, c);
+    } else if (NK) {
       const unsigned long long w = nk[u];  // own, x-, x+, y-, y+, z-, z+ keys in bytes 0..6
-      has = cell_coef<T, DD>(op, k0 + u, (uint8_t)w, (uint8_t)(w >> 8), (uint8_t)(w >> 16), (uint8_t)(w >> 24),
-                               (uint8_t)(w >> 32), (uint8_t)(w >> 40), (uint8_t)(w >> 48), ac, c);
+      has = cell_coef<T, DDM == 1>(op, k0 + u, (uint8_t)w, (uint8_t)(w >> 8), (uint8_t)(w >> 16),
+                                   (uint8_t)(w >> 24), (uint8_t)(w >> 32), (uint8_t)(w >> 40), (uint8_t)(w >> 48),
+                                   ac, c);
     } else {
-      has = cell_coef<T, DD>(op, k0 + u, (uint8_t)kc[u], (uint8_t)kxm[u], (uint8_t)kxp[u], (uint8_t)kym[u],
+      has = cell_coef<T, DDM == 1>(op, k0 + u, (uint8_t)kc[u], (uint8_t)kxm[u], (uint8_t)kxp[u], (uint8_t)kym[u],
                                (uint8_t)kyp[u], (uint8_t)kcol[u], (uint8_t)kcol[u + 2], ac, c);
     }
     if (!has) continue;
@@ -527,10 +561,11 @@ __device__ __forceinline__ double rb_pass_column(const OpParams<T>& op, T* x, co
 // shape keeps the register cap of H2G_MINB blocks of 256 threads per SM.
 constexpr int kRbRows[4] = {2, 4, 8, 16};
 
-// DD: dd read from the per-cell array (fewer instructions; faster while the vectors stay in L2)
-// or summed per cell (8 bytes fewer per cell; faster on grids that stream from HBM).  The tuner
-// picks it with the shape.
-template <typename T, int BY = kBY, int NP = 2, bool DD = true>
+// DDM: how a cell gets dd and its coefficients.  0: coefficients from the key tables, dd summed
+// per cell (8 bytes fewer per cell than 1); 1: dd read from the per-cell array (fewer
+// instructions); 2 (FP64): the stencil-class table (2 bytes per cell instead of the 8-byte key
+// word and dd).  The tuner picks it with the shape.
+template <typename T, int BY = kBY, int NP = 2, int DDM = 1>
 __global__ void __launch_bounds__(kBX * BY, (H2G_MINB * kBY) / BY)
     k_rb_pass(OpParams<T> op, T* x, const T* __restrict__ bb, int color, T omega,
               const SolverState* __restrict__ st) {
@@ -540,7 +575,7 @@ __global__ void __launch_bounds__(kBX * BY, (H2G_MINB * kBY) / BY)
   const int j = 1 + blockIdx.y * BY + threadIdx.y;
   const int k0 = 1 + NP * blockIdx.z;
   if (j > op.g.NY) return;  // uniform per warp
-  rb_pass_column<T, false, NP, DD>(op, x, bb, color, omega, lane, p, j, k0);
+  rb_pass_column<T, false, NP, DDM>(op, x, bb, color, omega, lane, p, j, k0);
 }
 
 // rbsor_core! with its residual (NonUniform.jl:848-915) for solveSOR! (NonUniform.jl:1004-1051):
@@ -577,7 +612,7 @@ __global__ void __launch_bounds__(kThreads) k_sor_pass(OpParams<double> op, doub
 // (xx, operator tables); TV: precision of the Krylov vectors; when they differ, bbT receives the
 // smoother's copy of the right-hand side in T.  Thread = both colours of column (p,j) at plane k.
 // ------------------------------------------------------------------------------------------
-template <typename T, typename TV, int VM>
+template <typename T, typename TV, int VM, bool CL = false>
 __device__ __forceinline__ void rb_first_column(const OpParams<T>& op, T* __restrict__ xx, TV* __restrict__ v,
                                                 T* __restrict__ bbT, const TV* __restrict__ r,
                                                 const TV* __restrict__ q, const SolverState* __restrict__ st,
@@ -610,10 +645,13 @@ __device__ __forceinline__ void rb_first_column(const OpParams<T>& op, T* __rest
     else if (VM == 1) bvv[col] = first ? r[ci] : add(r[ci], mul(beta, sub(v[ci], mul(omg, q[ci]))));
     else bvv[col] = add(mul(-alpha, q[ci]), r[ci]);
   }
-  // keys for the colour-0 cell: its own and its colour-1 neighbours
+  // keys for the colour-0 cell: its own and its colour-1 neighbours (or its stencil class)
   int k1c = 0, k1m = 0, k1p = 0, kym = 0, kyp = 0, k0c = 0;
   int kxm = 0, kxp = 0;
-  if (H2G_NKEY) {
+  unsigned cl = kNoClass;
+  if (CL) {
+    if (!copy_only && ok[0]) cl = __ldg(op.cls + r0 + p);
+  } else if (H2G_NKEY) {
     if (!copy_only && ok[0]) {
       const unsigned long long w = __ldg(op.nkey + r0 + p);  // own, x-, x+, y-, y+, z-, z+
       k0c = (int)(w & 0xff);
@@ -654,8 +692,12 @@ __device__ __forceinline__ void rb_first_column(const OpParams<T>& op, T* __rest
       out = b;
     } else if (col == 0) {
       Coef<T> c;
-      if (cell_coef<T, true>(op, k, (uint8_t)k0c, (uint8_t)kxm, (uint8_t)kxp, (uint8_t)kym, (uint8_t)kyp,
-                             (uint8_t)k1m, (uint8_t)k1p, ci, c)) {
+      bool has;
+      if constexpr (CL) has = class_coef<T>(op, cl, ci, c);
+      else
+        has = cell_coef<T, true>(op, k, (uint8_t)k0c, (uint8_t)kxm, (uint8_t)kxp, (uint8_t)kym, (uint8_t)kyp,
+                                 (uint8_t)k1m, (uint8_t)k1p, ci, c);
+      if (has) {
         const T ss = T(0);
         const T dp = sub(gs_div(sub(ss, b), c.dd), T(0));
         out = add(T(0), dp);  // pp + omega*dp with pp = 0, omega = 1
@@ -665,7 +707,7 @@ __device__ __forceinline__ void rb_first_column(const OpParams<T>& op, T* __rest
   }
 }
 
-template <typename T, typename TV, int VM>
+template <typename T, typename TV, int VM, bool CL = false>
 __global__ void __launch_bounds__(kThreads) k_rb_first(OpParams<T> op, T* __restrict__ xx, TV* __restrict__ v,
                                                         T* __restrict__ bbT, const TV* __restrict__ r,
                                                         const TV* __restrict__ q, const SolverState* __restrict__ st,
@@ -676,7 +718,7 @@ __global__ void __launch_bounds__(kThreads) k_rb_first(OpParams<T> op, T* __rest
   const int j = 1 + blockIdx.y * kBY + threadIdx.y;
   const int k = 1 + blockIdx.z;
   if (j > op.g.NY) return;
-  rb_first_column<T, TV, VM>(op, xx, v, bbT, r, q, st, copy_only, lane, p, j, k);
+  rb_first_column<T, TV, VM, CL>(op, xx, v, bbT, r, q, st, copy_only, lane, p, j, k);
 }
 
 // Both colours of column (p, j) at plane k: the values (centre and z-neighbours) and keys of the
@@ -729,9 +771,10 @@ __device__ __forceinline__ void load_pair(const Geo& g, const TI* x, const uint8
 // and the stage finisher.  TI: type of x (the preconditioner output may be FP32 while A is
 // applied in FP64).  Grid (ceil(HN/32), ceil(NY/kBY), NZ).
 // ------------------------------------------------------------------------------------------
-// DD: read dd from the per-cell array (FP64 only; the FP32 operator uses the difference form).
-// Which is faster depends on whether the vectors stay in L2; the launch-shape tuner decides.
-template <typename T, int NDOT, typename TI = T, bool DD = false>
+// DDM: 0 coefficients from the key tables with dd summed; 1 dd read from the per-cell array (FP64
+// only; the FP32 operator uses the difference form); 2 the stencil-class table (FP64).  Which is
+// faster depends on whether the vectors stay in L2; the launch-shape tuner decides.
+template <typename T, int NDOT, typename TI = T, int DDM = 0>
 __global__ void __launch_bounds__(kThreads, H2G_AX_MINB) k_ax(OpParams<T> op, T* __restrict__ y, const TI* __restrict__ x,
                                                   const T* __restrict__ u, const T* __restrict__ w,
                                                   SolverState* st, double* __restrict__ partials, int stage) {
@@ -761,9 +804,15 @@ __global__ void __launch_bounds__(kThreads, H2G_AX_MINB) k_ax(OpParams<T> op, T*
         if (NDOT >= 2) ww[col] = w[ci];
       }
     }
-    constexpr bool NK = H2G_NKEY != 0;
+    constexpr bool CL = DDM == 2;
+    constexpr bool NK = H2G_NKEY != 0 || CL;
     unsigned long long nk[2] = {0ull, 0ull};
-    if (NK) {
+    unsigned cl[2] = {kNoClass, kNoClass};
+    if (CL) {
+#pragma unroll
+      for (int col = 0; col < 2; ++col)
+        if (ok[col]) cl[col] = __ldg(op.cls + (col ? r1 : r0) + p);
+    } else if (NK) {
 #pragma unroll
       for (int col = 0; col < 2; ++col)
         if (ok[col]) nk[col] = __ldg(op.nkey + (col ? r1 : r0) + p);
@@ -782,17 +831,19 @@ __global__ void __launch_bounds__(kThreads, H2G_AX_MINB) k_ax(OpParams<T> op, T*
       Coef<T> c;
       T out = T(0);
       bool has;
-      if (NK) {
+      if constexpr (CL) {
+        has = class_coef<T>(op, cl[col], ci, c);
+      } else if (NK) {
         const unsigned long long wk = nk[col];  // own, x-, x+, y-, y+, z-, z+ keys in bytes 0..6
-        has = cell_coef<T, DD && sizeof(T) == 8>(op, k, (uint8_t)wk, (uint8_t)(wk >> 8), (uint8_t)(wk >> 16),
+        has = cell_coef<T, DDM == 1 && sizeof(T) == 8>(op, k, (uint8_t)wk, (uint8_t)(wk >> 8), (uint8_t)(wk >> 16),
                                                  (uint8_t)(wk >> 24), (uint8_t)(wk >> 32), (uint8_t)(wk >> 40),
                                                  (uint8_t)(wk >> 48), ci, c);
       } else if (col == 0) {
-        has = cell_coef<T, DD && sizeof(T) == 8>(op, k, (uint8_t)P.kc0[1], (uint8_t)kxm0, (uint8_t)kxp0,
+        has = cell_coef<T, DDM == 1 && sizeof(T) == 8>(op, k, (uint8_t)P.kc0[1], (uint8_t)kxm0, (uint8_t)kxp0,
                                                  (uint8_t)P.ky1m, (uint8_t)P.ky1p, (uint8_t)P.kc1[0],
                                                  (uint8_t)P.kc1[2], ci, c);
       } else {
-        has = cell_coef<T, DD && sizeof(T) == 8>(op, k, (uint8_t)P.kc1[1], (uint8_t)kxm1, (uint8_t)kxp1,
+        has = cell_coef<T, DDM == 1 && sizeof(T) == 8>(op, k, (uint8_t)P.kc1[1], (uint8_t)kxm1, (uint8_t)kxp1,
                                                  (uint8_t)P.ky0m, (uint8_t)P.ky0p, (uint8_t)P.kc0[0],
                                                  (uint8_t)P.kc0[2], ci, c);
       }
@@ -1387,6 +1438,80 @@ __global__ void __launch_bounds__(256) k_make_nkeys(Geo g, const uint8_t* __rest
 #pragma unroll
   for (int f = 0; f < 6; ++f) w |= (unsigned long long)key[nb[f]] << (8 * (f + 1));
   nk[o] = w;
+}
+
+// Stencil classes, step 1: every updated interior cell enters its (plane, 7 keys) pair into an
+// open-addressing table of kClassSlots words (plane in the top byte; the own key's mask bit makes
+// every entry non-zero).  At most kClassSlots probes per cell: a full table sets *overflow.
+__device__ __forceinline__ unsigned class_hash(unsigned long long w) {
+  return (unsigned)((w * 0x9E3779B97F4A7C15ull) >> (64 - 17)) & (kClassSlots - 1);
+}
+__device__ __forceinline__ unsigned long long class_word(const unsigned long long* nk, int o, int k) {
+  return (nk[o] & 0x00ffffffffffffffull) | ((unsigned long long)k << 56);
+}
+__global__ void __launch_bounds__(256) k_class_insert(Geo g, const unsigned long long* __restrict__ nk,
+                                                       unsigned long long* slots, int* overflow) {
+  const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = 1 + blockIdx.y, k = 1 + blockIdx.z;
+  if (i > g.NX) return;
+  const int o = g.off(i, j, k);
+  if (!(nk[o] & 0x80)) return;  // masked: never updated
+  const unsigned long long w = class_word(nk, o, k);
+  unsigned h = class_hash(w);
+  for (int t = 0; t < kClassSlots; ++t) {
+    const unsigned long long prev = atomicCAS(slots + h, 0ull, w);
+    if (prev == 0ull || prev == w) return;
+    h = (h + 1) & (kClassSlots - 1);
+  }
+  atomicExch(overflow, 1);
+}
+
+// Step 2 (after the host numbered the occupied slots): the class index of every cell; cells that
+// are never updated (guards, masked cells, padding) keep kNoClass from the fill before.
+__global__ void __launch_bounds__(256) k_class_assign(Geo g, const unsigned long long* __restrict__ nk,
+                                                       const unsigned long long* __restrict__ slots,
+                                                       const uint16_t* __restrict__ slot_class,
+                                                       uint16_t* __restrict__ cls) {
+  const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = 1 + blockIdx.y, k = 1 + blockIdx.z;
+  if (i > g.NX) return;
+  const int o = g.off(i, j, k);
+  if (!(nk[o] & 0x80)) return;
+  const unsigned long long w = class_word(nk, o, k);
+  unsigned h = class_hash(w);
+  for (int t = 0; t < kClassSlots; ++t) {
+    const unsigned long long v = slots[h];
+    if (v == w) {
+      cls[o] = slot_class[h];
+      return;
+    }
+    if (v == 0ull) return;  // not entered (cannot happen after a complete step 1)
+    h = (h + 1) & (kClassSlots - 1);
+  }
+}
+
+// Step 3: one table row per class from cell_coef on the class's (plane, keys) pair, with the
+// grid taken as steady (a_p0 = 0: dd is then the sum of the 12 face terms, what a steady cell of
+// the class gets).
+__global__ void __launch_bounds__(128) k_class_coef(OpParams<double> op, const unsigned long long* __restrict__ words,
+                                                     int ncls, double* __restrict__ ctab) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncls) return;
+  const unsigned long long w = words[c];
+  const int k = (int)(w >> 56);
+  op.steady = 1;
+  Coef<double> cf;
+  cell_coef<double, false>(op, k, (uint8_t)w, (uint8_t)(w >> 8), (uint8_t)(w >> 16), (uint8_t)(w >> 24),
+                           (uint8_t)(w >> 32), (uint8_t)(w >> 40), (uint8_t)(w >> 48), 0, cf);
+  double* t = ctab + 8 * (size_t)c;
+  t[0] = cf.cxm;
+  t[1] = cf.cxp;
+  t[2] = cf.cym;
+  t[3] = cf.cyp;
+  t[4] = cf.czm;
+  t[5] = cf.czp;
+  t[6] = cf.dd;
+  t[7] = 0.0;
 }
 
 // ------------------------------------------------------------------------------------------

@@ -162,6 +162,17 @@ struct Solver {
   int rb_planes = 2;      // planes per thread of the colour pass (autotuned)
   bool rb_dd = true;      // colour pass reads dd from the per-cell array (autotuned)
   bool ax_dd = false;     // CalcAX reads dd from the per-cell array (autotuned)
+  bool rb_cls = false;    // FP64 colour passes read the stencil-class table (autotuned)
+  bool ax_cls = false;    // FP64 CalcAX reads the stencil-class table (autotuned)
+  // stencil classes of the FP64 operator (k_class_*): per-cell index, table, build scratch
+  bool cls_ok = false;    // the grid's classes are built (at most kMaxClasses, NZ <= 255)
+  int ncls = 0;
+  uint16_t* cls = nullptr;
+  double* ctab = nullptr;
+  unsigned long long* cslots = nullptr;
+  uint16_t* slot_class = nullptr;
+  unsigned long long* cwords = nullptr;
+  int* cflag = nullptr;
   bool rb_tuned = false;  // rb_rows chosen (by the tuner or h2g_set_tuning)
   // fused sweeps (k_rb_sweep): sweeps 2-5 of the preconditioner as one launch each, ping-ponging
   // between the preconditioner's output and x2 (one per precision; guards zero, never written)
@@ -240,12 +251,19 @@ template <typename T, int NDOT, typename TI>
 static void launch_ax(const Solver* s, cudaStream_t cs, const OpParams<T>& op, T* y, const TI* x, const T* u,
                       const T* w, SolverState* st, int stage) {
   const dim3 ag((op.g.HN + kBX - 1) / kBX, (op.g.NY + kBY - 1) / kBY, op.g.NZ), blk(kBX, kBY);
-  if (s->ax_dd) launch(s, k_ax<T, NDOT, TI, true>, ag, blk, cs, op, y, x, u, w, st, s->partials, stage);
-  else launch(s, k_ax<T, NDOT, TI, false>, ag, blk, cs, op, y, x, u, w, st, s->partials, stage);
+  if constexpr (sizeof(T) == 8) {
+    if (s->ax_cls && op.cls) {
+      launch(s, k_ax<T, NDOT, TI, 2>, ag, blk, cs, op, y, x, u, w, st, s->partials, stage);
+      return;
+    }
+  }
+  if (s->ax_dd) launch(s, k_ax<T, NDOT, TI, 1>, ag, blk, cs, op, y, x, u, w, st, s->partials, stage);
+  else launch(s, k_ax<T, NDOT, TI, 0>, ag, blk, cs, op, y, x, u, w, st, s->partials, stage);
 }
 
-// One colour pass with the handle's launch shape (rows per block, planes per thread).
-template <typename T, int NP, bool DD>
+// One colour pass with the handle's launch shape (rows per block, planes per thread) and source of
+// the coefficients (DDM as in k_rb_pass).
+template <typename T, int NP, int DDM>
 static void launch_rb_np(const Solver* s, cudaStream_t cs, const OpParams<T>& op, T* x, const T* bb, int color,
                          T omega, const SolverState* st) {
   const Geo& g = op.g;
@@ -253,31 +271,37 @@ static void launch_rb_np(const Solver* s, cudaStream_t cs, const OpParams<T>& op
   const int gx = (g.HN + kBX - 1) / kBX;
   switch (s->rb_rows) {
     case 2:
-      launch(s, k_rb_pass<T, 2, NP, DD>, dim3(gx, (g.NY + 1) / 2, gz), dim3(kBX, 2), cs, op, x, bb, color, omega, st);
+      launch(s, k_rb_pass<T, 2, NP, DDM>, dim3(gx, (g.NY + 1) / 2, gz), dim3(kBX, 2), cs, op, x, bb, color, omega, st);
       break;
     case 4:
-      launch(s, k_rb_pass<T, 4, NP, DD>, dim3(gx, (g.NY + 3) / 4, gz), dim3(kBX, 4), cs, op, x, bb, color, omega, st);
+      launch(s, k_rb_pass<T, 4, NP, DDM>, dim3(gx, (g.NY + 3) / 4, gz), dim3(kBX, 4), cs, op, x, bb, color, omega, st);
       break;
     case 16:
-      launch(s, k_rb_pass<T, 16, NP, DD>, dim3(gx, (g.NY + 15) / 16, gz), dim3(kBX, 16), cs, op, x, bb, color, omega,
+      launch(s, k_rb_pass<T, 16, NP, DDM>, dim3(gx, (g.NY + 15) / 16, gz), dim3(kBX, 16), cs, op, x, bb, color, omega,
              st);
       break;
     default:
-      launch(s, k_rb_pass<T, 8, NP, DD>, dim3(gx, (g.NY + 7) / 8, gz), dim3(kBX, 8), cs, op, x, bb, color, omega, st);
+      launch(s, k_rb_pass<T, 8, NP, DDM>, dim3(gx, (g.NY + 7) / 8, gz), dim3(kBX, 8), cs, op, x, bb, color, omega, st);
       break;
   }
 }
-template <typename T, bool DD>
+template <typename T, int DDM>
 static void launch_rb_dd(const Solver* s, cudaStream_t cs, const OpParams<T>& op, T* x, const T* bb, int color,
                          T omega, const SolverState* st) {
-  if (s->rb_planes == 1) launch_rb_np<T, 1, DD>(s, cs, op, x, bb, color, omega, st);
-  else launch_rb_np<T, 2, DD>(s, cs, op, x, bb, color, omega, st);
+  if (s->rb_planes == 1) launch_rb_np<T, 1, DDM>(s, cs, op, x, bb, color, omega, st);
+  else launch_rb_np<T, 2, DDM>(s, cs, op, x, bb, color, omega, st);
 }
 template <typename T>
 static void launch_rb(const Solver* s, cudaStream_t cs, const OpParams<T>& op, T* x, const T* bb, int color, T omega,
                       const SolverState* st) {
-  if (s->rb_dd) launch_rb_dd<T, true>(s, cs, op, x, bb, color, omega, st);
-  else launch_rb_dd<T, false>(s, cs, op, x, bb, color, omega, st);
+  if constexpr (sizeof(T) == 8) {
+    if (s->rb_cls && op.cls) {
+      launch_rb_dd<T, 2>(s, cs, op, x, bb, color, omega, st);
+      return;
+    }
+  }
+  if (s->rb_dd) launch_rb_dd<T, 1>(s, cs, op, x, bb, color, omega, st);
+  else launch_rb_dd<T, 0>(s, cs, op, x, bb, color, omega, st);
 }
 
 // ---- fused sweep (k_rb_sweep) ---------------------------------------------------------------
@@ -403,19 +427,19 @@ static int sweep_status(Solver* s) {
 
 // Blocks of the cooperative preconditioner: every SM's resident blocks, so that all of them run
 // at once (the cooperative launch checks it).
-template <int VM, int NP, bool DD>
+template <int VM, int NP, int DDM>
 static int coop_grid(Solver* s) {
   int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_precond_coop<VM, NP, DD>, kThreads, 0) != cudaSuccess ||
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_precond_coop<VM, NP, DDM>, kThreads, 0) != cudaSuccess ||
       per_sm < 1)
     return 0;
   return per_sm * s->num_sms;
 }
 
-template <int VM, int NP, bool DD>
+template <int VM, int NP, int DDM>
 static int launch_coop_np(Solver* s, cudaStream_t cs, const OpParams<double>& op, double* xx, double* v,
                           const double* r, const double* q, SolverState* st) {
-  const int nblk = coop_grid<VM, NP, DD>(s);
+  const int nblk = coop_grid<VM, NP, DDM>(s);
   if (nblk < 1) return fail(H2G_CUDA_ERROR, "no resident block for the cooperative preconditioner");
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(nblk);
@@ -426,7 +450,7 @@ static int launch_coop_np(Solver* s, cudaStream_t cs, const OpParams<double>& op
   attr[0].val.cooperative = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  if (cudaLaunchKernelEx(&cfg, k_precond_coop<VM, NP, DD>, op, xx, v, r, q, st, s->gbar, s->sweep_err,
+  if (cudaLaunchKernelEx(&cfg, k_precond_coop<VM, NP, DDM>, op, xx, v, r, q, st, s->gbar, s->sweep_err,
                          s->wait_limit) != cudaSuccess)
     return fail(H2G_CUDA_ERROR, "cooperative launch of %d blocks failed: %s", nblk,
                 cudaGetErrorString(cudaGetLastError()));
@@ -435,11 +459,14 @@ static int launch_coop_np(Solver* s, cudaStream_t cs, const OpParams<double>& op
 template <int VM>
 static int launch_coop(Solver* s, cudaStream_t cs, const OpParams<double>& op, double* xx, double* v,
                        const double* r, const double* q, SolverState* st) {
+  const int m = s->rb_cls && op.cls ? 2 : s->rb_dd ? 1 : 0;
   if (s->rb_planes == 1)
-    return s->rb_dd ? launch_coop_np<VM, 1, true>(s, cs, op, xx, v, r, q, st)
-                    : launch_coop_np<VM, 1, false>(s, cs, op, xx, v, r, q, st);
-  return s->rb_dd ? launch_coop_np<VM, 2, true>(s, cs, op, xx, v, r, q, st)
-                  : launch_coop_np<VM, 2, false>(s, cs, op, xx, v, r, q, st);
+    return m == 2 ? launch_coop_np<VM, 1, 2>(s, cs, op, xx, v, r, q, st)
+                  : m == 1 ? launch_coop_np<VM, 1, 1>(s, cs, op, xx, v, r, q, st)
+                           : launch_coop_np<VM, 1, 0>(s, cs, op, xx, v, r, q, st);
+  return m == 2 ? launch_coop_np<VM, 2, 2>(s, cs, op, xx, v, r, q, st)
+                : m == 1 ? launch_coop_np<VM, 2, 1>(s, cs, op, xx, v, r, q, st)
+                         : launch_coop_np<VM, 2, 0>(s, cs, op, xx, v, r, q, st);
 }
 static bool use_coop(const Solver* s) { return s->rb_coop && !s->coop_barred && !s->rb_fused; }
 
@@ -499,7 +526,14 @@ static int launch_precond(Solver* s, cudaStream_t cs, const OpParams<T>& op, T* 
   if constexpr (std::is_same<T, double>::value && std::is_same<TV, double>::value) {
     if (use_coop(s) && !none && !bbT) return launch_coop<VM>(s, cs, op, xx, v, r, q, st);
   }
-  launch(s, k_rb_first<T, TV, VM>, first_grid(op.g), dim3(kBX, kBY), cs, op, xx, v, bbT, r, q, st, none);
+  bool cl = false;
+  if constexpr (sizeof(T) == 8) {
+    cl = s->rb_cls && op.cls && !none;
+    if (cl)
+      launch(s, k_rb_first<T, TV, VM, true>, first_grid(op.g), dim3(kBX, kBY), cs, op, xx, v, bbT, r, q, st, none);
+  }
+  if (!cl)
+    launch(s, k_rb_first<T, TV, VM, false>, first_grid(op.g), dim3(kBX, kBY), cs, op, xx, v, bbT, r, q, st, none);
   if (none) return H2G_OK;
   for (int pass = 1; pass < 2 * kSweeps; ++pass) launch_rb<T>(s, cs, op, xx, bb, pass & 1, T(1), st);
   return H2G_OK;
@@ -539,6 +573,8 @@ static OpParams<T> op_params_rc(const Solver* s, const OpTables<T>& t, const T* 
   op.ddv = t.ddv;
   op.tq = t.tq;
   op.nkey = s->nkey;
+  op.cls = nullptr;
+  op.ctab = nullptr;
   const double dx0 = s->dx, dy0 = s->dy;
   op.czm = (T)((s->HC[4] * dx0) * dy0);
   op.czp = (T)((s->HC[5] * dx0) * dy0);
@@ -551,7 +587,12 @@ static OpParams<T> op_params_rc(const Solver* s, const OpTables<T>& t, const T* 
 }
 template <>
 OpParams<double> op_params<double>(const Solver* s, const OpTables<double>& t) {
-  return op_params_rc<double>(s, t, s->rc64);
+  OpParams<double> op = op_params_rc<double>(s, t, s->rc64);
+  if (s->cls_ok) {
+    op.cls = s->cls;
+    op.ctab = s->ctab;
+  }
+  return op;
 }
 template <>
 OpParams<float> op_params<float>(const Solver* s, const OpTables<float>& t) {
@@ -589,6 +630,8 @@ static void destroy(Solver* s) {
   for (auto& p : s->hook) cudaFree(p);
   for (auto& p : s->stage) cudaFree(p);
   cudaFree(s->x2_64); cudaFree(s->x2_32); cudaFree(s->sweep_err); cudaFree(s->gbar);
+  cudaFree(s->cls); cudaFree(s->ctab); cudaFree(s->cslots); cudaFree(s->slot_class); cudaFree(s->cwords);
+  cudaFree(s->cflag);
   s->mr_graph.reset();
   cudaFree(s->mr_th); cudaFree(s->mr_b); cudaFree(s->mr_st); cudaFree(s->mr_ctl); cudaFree(s->mr_partials);
   cudaFree(s->mr_flag);
@@ -637,6 +680,71 @@ static void invalidate_graphs(Solver* s) {
 // ------------------------------------------------------------------------------------------
 // Operator tables (host, FP64, in the reference's operation order; FP32 copies by rounding).
 // ------------------------------------------------------------------------------------------
+// Stencil classes of the FP64 operator (k_class_insert / k_class_assign / k_class_coef): the
+// distinct (plane, 7 keys) pairs of the updated cells, numbered in the order of their hash slots,
+// and their coefficients.  Left unbuilt (the kernels keep the key tables) when disabled
+// (H2G_CLS=0), when NZ > 255 (the plane shares the 64-bit word with the keys) or when the grid has
+// more than kMaxClasses pairs.
+static int build_classes(Solver* s) {
+  const Geo& g = s->g;
+  const bool was = s->cls_ok;
+  s->cls_ok = false;
+  s->ncls = 0;
+  const char* e = getenv("H2G_CLS");
+  if ((e && atoi(e) == 0) || g.NZ > 255 || !s->nkey) {
+    if (was) invalidate_graphs(s);
+    return H2G_OK;
+  }
+  if (!s->cls) {
+    CK(cudaMalloc(&s->cls, sizeof(uint16_t) * (size_t)g.n));
+    CK(cudaMalloc(&s->ctab, sizeof(double) * 8 * (size_t)kMaxClasses));
+    CK(cudaMalloc(&s->cslots, sizeof(unsigned long long) * kClassSlots));
+    CK(cudaMalloc(&s->slot_class, sizeof(uint16_t) * kClassSlots));
+    CK(cudaMalloc(&s->cwords, sizeof(unsigned long long) * kMaxClasses));
+    CK(cudaMalloc(&s->cflag, sizeof(int)));
+  }
+  CK(cudaMemsetAsync(s->cslots, 0, sizeof(unsigned long long) * kClassSlots, s->stream));
+  CK(cudaMemsetAsync(s->cflag, 0, sizeof(int), s->stream));
+  CK(cudaMemsetAsync(s->cls, 0xff, sizeof(uint16_t) * (size_t)g.n, s->stream));
+  const dim3 gi((g.NX + 255) / 256, g.NY, g.NZ);
+  k_class_insert<<<gi, 256, 0, s->stream>>>(g, s->nkey, s->cslots, s->cflag);
+  CKL();
+  std::vector<unsigned long long> slots(kClassSlots);
+  int flag = 0;
+  CK(cudaMemcpyAsync(slots.data(), s->cslots, sizeof(unsigned long long) * kClassSlots, cudaMemcpyDeviceToHost,
+                     s->stream));
+  CK(cudaMemcpyAsync(&flag, s->cflag, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  std::vector<uint16_t> sc(kClassSlots, (uint16_t)kNoClass);
+  std::vector<unsigned long long> words;
+  bool fits = flag == 0;
+  for (int h = 0; h < kClassSlots && fits; ++h) {
+    if (!slots[h]) continue;
+    if ((int)words.size() >= kMaxClasses) fits = false;
+    else {
+      sc[h] = (uint16_t)words.size();
+      words.push_back(slots[h]);
+    }
+  }
+  if (!fits || words.empty()) {
+    if (was) invalidate_graphs(s);
+    return H2G_OK;
+  }
+  CK(cudaMemcpyAsync(s->slot_class, sc.data(), sizeof(uint16_t) * kClassSlots, cudaMemcpyHostToDevice, s->stream));
+  CK(cudaMemcpyAsync(s->cwords, words.data(), sizeof(unsigned long long) * words.size(), cudaMemcpyHostToDevice,
+                     s->stream));
+  k_class_assign<<<gi, 256, 0, s->stream>>>(g, s->nkey, s->cslots, s->slot_class, s->cls);
+  const int ncls = (int)words.size();
+  OpParams<double> o64 = op_params_rc<double>(s, s->t64, s->rc64);
+  k_class_coef<<<(ncls + 127) / 128, 128, 0, s->stream>>>(o64, s->cwords, ncls, s->ctab);
+  CKL();
+  CK(cudaStreamSynchronize(s->stream));  // the host vectors must outlive the copies
+  s->ncls = ncls;
+  s->cls_ok = true;
+  if (!was) invalidate_graphs(s);
+  return H2G_OK;
+}
+
 static int build_tables(Solver* s) {
   if (!s->grid_set || !s->fields_set) return H2G_OK;
   const Geo& g = s->g;
@@ -743,7 +851,7 @@ static int build_tables(Solver* s) {
   }
   // host vectors must stay alive until the copies ran
   CK(cudaStreamSynchronize(s->stream));
-  return H2G_OK;
+  return build_classes(s);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -1749,7 +1857,7 @@ static int adjoint_transient(Solver* s, const FaceBC& f, int nt, const double* w
 // H2G_RB_PLANES, H2G_RB_DD and H2G_AX_DD in the environment force them (all four: no timing; a
 // forced rows, planes or dd source also restricts the timed variants to it).
 static std::mutex g_tune_mu;
-static std::map<std::array<int, 11>, int> g_tune_cache;
+static std::map<std::array<int, 12>, int> g_tune_cache;
 
 static bool valid_rows(int r) {
   for (int q : kRbRows)
@@ -1778,7 +1886,8 @@ static int tune_rows_t(Solver* s, const OpParams<T>& op, int only_rows, int only
     return fail(H2G_CUDA_ERROR, "event creation failed");
   }
   const int saved = s->rb_rows, saved_np = s->rb_planes;
-  const bool saved_dd = s->rb_dd;
+  const bool saved_dd = s->rb_dd, saved_cls = s->rb_cls;
+  const int nmodes = op.cls ? 3 : 2;  // coefficient sources: dd summed, dd read, class table
   float best = 1e30f;
   int rc = H2G_OK;
   // warm the GPU up first (clocks ramp), then time every shape twice, interleaved, keeping the
@@ -1787,18 +1896,20 @@ static int tune_rows_t(Solver* s, const OpParams<T>& op, int only_rows, int only
     launch_rb<T>(s, s->stream, op, xa, (const T*)xb, 0, T(1), nullptr);
     launch_rb<T>(s, s->stream, op, xa, (const T*)xb, 1, T(1), nullptr);
   }
-  constexpr int kShapes = 16;  // 4 block heights x 2 plane counts x 2 dd sources
+  constexpr int kShapes = 24;  // 4 block heights x 2 plane counts x 3 coefficient sources
   float tbest[kShapes];
   for (int q = 0; q < kShapes; ++q) tbest[q] = 1e30f;
   constexpr int kRounds = 3;
   for (int round = 0; round < kRounds && rc == H2G_OK; ++round)
   for (int shape = 0; shape < kShapes; ++shape) {
     const int by = kRbRows[shape & 3], np = 1 + ((shape >> 2) & 1), dd = shape >> 3;
-    if ((only_rows >= 0 && by != only_rows) || (only_np >= 0 && np != only_np) || (only_dd >= 0 && dd != only_dd))
+    if ((only_rows >= 0 && by != only_rows) || (only_np >= 0 && np != only_np) || (only_dd >= 0 && dd != only_dd) ||
+        dd >= nmodes)
       continue;
     s->rb_rows = by;
     s->rb_planes = np;
-    s->rb_dd = dd != 0;
+    s->rb_dd = dd == 1;
+    s->rb_cls = dd == 2;
     for (int r = 0; r < 2; ++r) {
       launch_rb<T>(s, s->stream, op, xa, (const T*)xb, 0, T(1), nullptr);
       launch_rb<T>(s, s->stream, op, xa, (const T*)xb, 1, T(1), nullptr);
@@ -1818,7 +1929,7 @@ static int tune_rows_t(Solver* s, const OpParams<T>& op, int only_rows, int only
     tbest[shape] = std::min(tbest[shape], ms);
     if (round == kRounds - 1 && tbest[shape] < best) {
       best = tbest[shape];
-      *best_rows = by | (np << 5) | (dd << 8);
+      *best_rows = by | (np << 5) | ((dd & 1) << 8) | ((dd >> 1) << 20);
     }
   }
   if (best == 1e30f) *best_rows = kBY | (2 << 5) | (1 << 8);  // nothing timed: the defaults
@@ -1826,6 +1937,7 @@ static int tune_rows_t(Solver* s, const OpParams<T>& op, int only_rows, int only
   s->rb_rows = saved;
   s->rb_planes = saved_np;
   s->rb_dd = saved_dd;
+  s->rb_cls = saved_cls;
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   return rc;
@@ -1926,11 +2038,13 @@ static int tune_ax(Solver* s, int* use_dd) {
     cudaEventDestroy(e0);
     return fail(H2G_CUDA_ERROR, "event creation failed");
   }
-  const bool saved = s->ax_dd;
-  float t[2] = {0.f, 0.f};
+  const bool saved = s->ax_dd, saved_cls = s->ax_cls;
+  const int nmodes = op.cls ? 3 : 2;  // dd summed, dd read, class table
+  float t[3] = {0.f, 0.f, 1e30f};
   int rc = H2G_OK;
-  for (int v = 0; v < 2 && rc == H2G_OK; ++v) {
+  for (int v = 0; v < nmodes && rc == H2G_OK; ++v) {
     s->ax_dd = v == 1;
+    s->ax_cls = v == 2;
     for (int r = 0; r < 2; ++r) launch_ax<double, 0, double>(s, s->stream, op, xb, xa, nullptr, nullptr, nullptr, 0);
     cudaEventRecord(e0, s->stream);
     for (int r = 0; r < 10; ++r) launch_ax<double, 0, double>(s, s->stream, op, xb, xa, nullptr, nullptr, nullptr, 0);
@@ -1940,9 +2054,13 @@ static int tune_ax(Solver* s, int* use_dd) {
       rc = fail(H2G_CUDA_ERROR, "CalcAX tuning failed");
   }
   s->ax_dd = saved;
+  s->ax_cls = saved_cls;
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  *use_dd = t[1] < t[0] ? 1 : 0;
+  int bestv = 0;
+  for (int v = 1; v < nmodes; ++v)
+    if (t[v] < t[bestv]) bestv = v;
+  *use_dd = bestv;
   return rc;
 }
 
@@ -1952,8 +2070,10 @@ static int autotune(Solver* s) {
   int rows = -1, planes = -1, rbdd = -1, dd = -1, fused = -1, chunks = -1, swdd = -1;
   if (const char* e = getenv("H2G_RB_ROWS")) rows = valid_rows(atoi(e)) ? atoi(e) : -1;
   if (const char* e = getenv("H2G_RB_PLANES")) planes = (atoi(e) == 1 || atoi(e) == 2) ? atoi(e) : -1;
-  if (const char* e = getenv("H2G_RB_DD")) rbdd = atoi(e) ? 1 : 0;
-  if (const char* e = getenv("H2G_AX_DD")) dd = atoi(e) ? 1 : 0;
+  // coefficient sources: 0 dd summed, 1 dd read, 2 stencil-class table (FP64, when built)
+  const int nmodes = s->precision == H2G_FP64 && s->cls_ok ? 3 : 2;
+  if (const char* e = getenv("H2G_RB_DD")) rbdd = std::min(std::max(atoi(e), 0), nmodes - 1);
+  if (const char* e = getenv("H2G_AX_DD")) dd = std::min(std::max(atoi(e), 0), nmodes - 1);
   if (const char* e = getenv("H2G_RB_FUSED")) fused = atoi(e) ? 1 : 0;
   if (const char* e = getenv("H2G_SW_CHUNKS")) chunks = (atoi(e) >= 1 && atoi(e) <= 255) ? atoi(e) : -1;
   if (const char* e = getenv("H2G_SW_DD")) swdd = atoi(e) ? 1 : 0;
@@ -1968,9 +2088,9 @@ static int autotune(Solver* s) {
   const bool sweep_known = fused == 0 || (fused == 1 && chunks > 0 && swdd >= 0);
   if (rows < 0 || planes < 0 || rbdd < 0 || dd < 0 || !sweep_known) {
     // cached per grid, smoother precision and the choices the environment restricts it to
-    const std::array<int, 11> key = {s->g.MX, s->g.MY,  s->g.MZ, s->precision == H2G_FP64 ? 64 : 32,
+    const std::array<int, 12> key = {s->g.MX, s->g.MY,  s->g.MZ, s->precision == H2G_FP64 ? 64 : 32,
                                      rows,    planes,   rbdd,    dd,
-                                     fused,   chunks,   swdd};
+                                     fused,   chunks,   swdd,    nmodes};
     int cached = 0;
     {
       // held while tuning, so that handles of one grid solved concurrently (h2g_batch_solve) tune
@@ -1991,7 +2111,7 @@ static int autotune(Solver* s) {
           const bool sd = s->rb_dd;
           s->rb_rows = r2 & 0x1f;
           s->rb_planes = (r2 >> 5) & 7;
-          s->rb_dd = (r2 >> 8) & 1;
+          s->rb_dd = (r2 >> 8) & 1;  // the fused sweep has no class mode: its first pass reads dd
           rc = s->precision == H2G_FP64
                    ? tune_sweep_t<double>(s, op_params<double>(s, s->t64), unfused_ms, fused, chunks, swdd, &sw)
                    : tune_sweep_t<float>(s, op_params<float>(s, s->t32), unfused_ms, fused, chunks, swdd, &sw);
@@ -2000,14 +2120,14 @@ static int autotune(Solver* s) {
           s->rb_dd = sd;
         }
         if (rc) return rc;
-        cached = r2 | (d2 << 9) | (sw << 10) | (1 << 30);
+        cached = r2 | ((d2 & 1) << 9) | (sw << 10) | ((d2 >> 1) << 21) | (1 << 30);
         g_tune_cache[key] = cached;
       }
     }
     if (rows < 0) rows = cached & 0x1f;
     if (planes < 0) planes = (cached >> 5) & 7;
-    if (rbdd < 0) rbdd = (cached >> 8) & 1;
-    if (dd < 0) dd = (cached >> 9) & 1;
+    if (rbdd < 0) rbdd = ((cached >> 8) & 1) | (((cached >> 20) & 1) << 1);
+    if (dd < 0) dd = ((cached >> 9) & 1) | (((cached >> 21) & 1) << 1);
     if (!sweep_known) {
       const int sw = (cached >> 10) & 0x3ff;
       fused = sw & 1;
@@ -2028,14 +2148,17 @@ static int autotune(Solver* s) {
     if (const char* e = getenv("H2G_RB_COOP")) coop = atoi(e) ? 1 : 0;
   }
   if (s->precision != H2G_FP64 || fused == 1) coop = 0;
-  if (rows != s->rb_rows || planes != s->rb_planes || (rbdd != 0) != s->rb_dd || (dd != 0) != s->ax_dd ||
-      (fused == 1) != s->rb_fused || chunks != s->sw_chunks || (swdd != 0) != s->sw_dda || coop != s->rb_coop)
+  if (rows != s->rb_rows || planes != s->rb_planes || (rbdd == 1) != s->rb_dd || (rbdd == 2) != s->rb_cls ||
+      (dd == 1) != s->ax_dd || (dd == 2) != s->ax_cls || (fused == 1) != s->rb_fused || chunks != s->sw_chunks ||
+      (swdd != 0) != s->sw_dda || coop != s->rb_coop)
     invalidate_graphs(s);
   s->rb_coop = coop;
   s->rb_rows = rows;
   s->rb_planes = planes;
-  s->rb_dd = rbdd != 0;
-  s->ax_dd = dd != 0;
+  s->rb_dd = rbdd == 1;
+  s->rb_cls = rbdd == 2;
+  s->ax_dd = dd == 1;
+  s->ax_cls = dd == 2;
   s->rb_fused = fused == 1;
   s->sw_chunks = chunks;
   s->sw_dda = swdd != 0;
@@ -2608,8 +2731,8 @@ int h2g_autotune(h2g_solver* h, int* rows, int* planes, int* rb_dd, int* ax_dd) 
   if (int rc = h2g::autotune(s)) return rc;
   if (rows) *rows = s->rb_rows;
   if (planes) *planes = s->rb_planes;
-  if (rb_dd) *rb_dd = s->rb_dd ? 1 : 0;
-  if (ax_dd) *ax_dd = s->ax_dd ? 1 : 0;
+  if (rb_dd) *rb_dd = s->rb_cls ? 2 : s->rb_dd ? 1 : 0;
+  if (ax_dd) *ax_dd = s->ax_cls ? 2 : s->ax_dd ? 1 : 0;
   return H2G_OK;
 }
 

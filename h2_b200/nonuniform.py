@@ -234,11 +234,12 @@ class Solver:
         return self.tuning()[:2]
 
     def tuning(self) -> tuple:
-        """The tuner's choices (running it if needed): (rows, planes, colour pass reads dd,
-        CalcAX reads dd)."""
+        """The tuner's choices (running it if needed): (rows, planes, coefficient source of the
+        colour pass, of CalcAX) with the sources 0 (dd summed per cell), 1 (dd read from the
+        per-cell array), 2 (stencil-class table, FP64)."""
         r, p, a, b = C.c_int(0), C.c_int(0), C.c_int(0), C.c_int(0)
         L.check(self.lib.h2g_autotune(self.h, C.byref(r), C.byref(p), C.byref(a), C.byref(b)))
-        return r.value, p.value, bool(a.value), bool(b.value)
+        return r.value, p.value, a.value, b.value
 
     def set_tuning(self, rows: int, planes: int = 2):
         """Force the colour pass's shape (rows 2, 4, 8, 16; planes 1, 2); rows = 0 tunes again."""

@@ -228,14 +228,18 @@ int h2g_transient(h2g_solver *h, const h2g_bc *bc, int nt, int method, double to
 /* ---- launch-shape tuning (no reference counterpart) ---------------------------------------
  * The smoother's colour pass has no reduction, so its launch variant changes no result.  The
  * first solve of a handle times blocks of 2, 4, 8 and 16 rows with 1 or 2 planes per thread and
- * dd read from the per-cell array or summed per cell (a few sweeps each on scratch vectors) and
- * keeps the fastest; it also times the FP64 CalcAX with either dd source (the same bits in every
- * case).  The choices are cached per grid size and smoother precision for the process;
- * H2G_RB_ROWS, H2G_RB_PLANES, H2G_RB_DD and H2G_AX_DD (0/1) in the environment force them (all
- * four: no timing at all; a forced rows, planes or dd source restricts the timing to it).  h2g_autotune runs the tuner now and reports its choices (each
- * pointer nullable): the colour pass's rows and planes, whether it reads dd (*rb_dd) and whether
- * CalcAX does (*ax_dd).  h2g_set_tuning forces a shape (rows 2, 4, 8 or 16 and planes 1 or 2;
- * rows = 0: tune again on the next solve). */
+ * three sources of a cell's coefficients (a few sweeps each on scratch vectors) and keeps the
+ * fastest; it also times the FP64 CalcAX with each source (the same bits in every case).  The
+ * sources: 0 the key tables with dd summed per cell, 1 the key tables with dd read from a
+ * per-cell array, 2 (FP64) the stencil-class table: the distinct (plane, 7 stencil keys) pairs
+ * of the grid, at most 65535 and NZ <= 255 (else not built; H2G_CLS=0 disables it), each with
+ * its coefficients, and a 2-byte class index per cell.  The choices are cached per grid size and
+ * smoother precision for the process; H2G_RB_ROWS, H2G_RB_PLANES, H2G_RB_DD and H2G_AX_DD
+ * (sources 0/1/2) in the environment force them (all four: no timing at all; a forced rows,
+ * planes or source restricts the timing to it).  h2g_autotune runs the tuner now and reports its
+ * choices (each pointer nullable): the colour pass's rows and planes and its source (*rb_dd), and
+ * CalcAX's source (*ax_dd).  h2g_set_tuning forces a shape (rows 2, 4, 8 or 16 and planes 1 or
+ * 2; rows = 0: tune again on the next solve). */
 int h2g_autotune(h2g_solver *h, int *rows, int *planes, int *rb_dd, int *ax_dd);
 int h2g_set_tuning(h2g_solver *h, int rows, int planes);
 /* The preconditioner's sweeps 2-5 as one fused launch each (k_rb_sweep: both colours of a sweep,

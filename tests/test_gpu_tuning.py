@@ -71,7 +71,7 @@ def test_dd_source_gives_identical_results(oracle, monkeypatch):
 def test_forced_choices_restrict_the_tuner(oracle, monkeypatch):
     """A forced plane count or dd source is kept and the other choices are tuned around it."""
     prob = mode3_model(oracle, 32)
-    for planes, dd in (("1", None), ("2", "0"), ("1", "1")):
+    for planes, dd in (("1", None), ("2", "0"), ("1", "1"), ("2", "2")):
         monkeypatch.setenv("H2G_RB_PLANES", planes)
         if dd is None:
             monkeypatch.delenv("H2G_RB_DD", raising=False)
@@ -81,5 +81,5 @@ def test_forced_choices_restrict_the_tuner(oracle, monkeypatch):
         rows, p, rb_dd, _ = s.tuning()
         assert rows in (2, 4, 8, 16) and p == int(planes)
         if dd is not None:
-            assert rb_dd == (dd == "1")
+            assert rb_dd == int(dd)
         s.close()
