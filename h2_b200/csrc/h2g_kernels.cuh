@@ -582,7 +582,7 @@ __global__ void __launch_bounds__(kBX * BY, (H2G_MINB * kBY) / BY)
 // colour `color` updated with relaxation omega, sum of r^2 -> stage (kStageSorHalf after colour
 // 0, kStageSorIter after colour 1).  The colour-1 launch ends a WHILE-body pass: block 0 counts
 // the pass and ends the loop provisionally; only the finisher can continue it.
-template <bool COND>
+template <bool COND, int DDM = 1>
 __global__ void __launch_bounds__(kThreads) k_sor_pass(OpParams<double> op, double* x,
                                                        const double* __restrict__ bb, int color, double omega,
                                                        SolverState* st, double* __restrict__ partials, int stage,
@@ -597,7 +597,7 @@ __global__ void __launch_bounds__(kThreads) k_sor_pass(OpParams<double> op, doub
   const int j = 1 + blockIdx.y * kBY + threadIdx.y;
   const int k0 = 1 + 2 * blockIdx.z;
   double v[1] = {0.0};
-  if (j <= op.g.NY) v[0] = rb_pass_column<double, true>(op, x, bb, color, omega, lane, p, j, k0);
+  if (j <= op.g.NY) v[0] = rb_pass_column<double, true, 2, DDM>(op, x, bb, color, omega, lane, p, j, k0);
   reduce_finish<1, COND>(v, partials, st, stage, hc, color == 1 ? use_cond : 0);
 }
 

@@ -51,6 +51,19 @@ __global__ void k_prime_mr(SolverState* st, MultiCtl* ctl, double tol, int maxIt
   }
 }
 
+// Coefficients of cell ci at plane k: from its packed key word and the key tables (CL false) or
+// from its stencil class (CL true); both give cell_coef's values.
+template <bool CL>
+__device__ __forceinline__ bool mr_coef(const OpParams<double>& op, int k, int ci, Coef<double>& c) {
+  if constexpr (CL) {
+    return class_coef<double>(op, __ldg(op.cls + ci), ci, c);
+  } else {
+    const unsigned long long w = __ldg(op.nkey + ci);
+    return cell_coef<double, true>(op, k, (uint8_t)w, (uint8_t)(w >> 8), (uint8_t)(w >> 16), (uint8_t)(w >> 24),
+                                   (uint8_t)(w >> 32), (uint8_t)(w >> 40), (uint8_t)(w >> 48), ci, c);
+  }
+}
+
 // Sum of one right-hand side's partials [NV][nb] in reduce_finish's order, by the whole block.
 template <int NV>
 __device__ __forceinline__ void seg_sum(const double* __restrict__ part, int nb, double (&acc)[NV],
@@ -118,7 +131,7 @@ __device__ __forceinline__ void group_finish(double (&v)[R][NV], double* __restr
 
 // CalcRK! for K right-hand sides: r = b - A th, r0 = r, (r,r) -> stage (kStageInit).
 // Grid (gx, gy, NZ * G), block (32, kBY).
-template <int R>
+template <int R, bool CL>
 __global__ void __launch_bounds__(kThreads) k_rk_mr(OpParams<double> op, double* __restrict__ r,
                                                      double* __restrict__ r0c, const double* __restrict__ th,
                                                      const double* __restrict__ b, SolverState* st,
@@ -142,22 +155,15 @@ __global__ void __launch_bounds__(kThreads) k_rk_mr(OpParams<double> op, double*
     const int r0 = g.row(0, j, k), r1 = r0 + g.HP;
     const int e0 = (1 + j + k) & 1;
     bool ok[2];
-    unsigned long long nk[2] = {0ull, 0ull};
 #pragma unroll
     for (int col = 0; col < 2; ++col) {
       const int i = 2 * p + (e0 ^ col);
       ok[col] = pok && i >= 1 && i <= g.NX;
-      if (ok[col]) nk[col] = __ldg(op.nkey + (col ? r1 : r0) + p);
     }
     Coef<double> c[2];
     bool has[2];
 #pragma unroll
-    for (int col = 0; col < 2; ++col) {
-      const unsigned long long w = nk[col];
-      has[col] = ok[col] && cell_coef<double, true>(op, k, (uint8_t)w, (uint8_t)(w >> 8), (uint8_t)(w >> 16),
-                                                    (uint8_t)(w >> 24), (uint8_t)(w >> 32), (uint8_t)(w >> 40),
-                                                    (uint8_t)(w >> 48), (col ? r1 : r0) + p, c[col]);
-    }
+    for (int col = 0; col < 2; ++col) has[col] = ok[col] && mr_coef<CL>(op, k, (col ? r1 : r0) + p, c[col]);
 #pragma unroll
     for (int rr = 0; rr < R; ++rr) {
       if (!run[rr]) continue;
@@ -190,7 +196,7 @@ __global__ void __launch_bounds__(kThreads) k_rk_mr(OpParams<double> op, double*
 
 // k_rb_first for K right-hand sides (VM 1: p update; VM 2: s update), then colour 0 of the first
 // sweep from zero.  Grid (gx, gy, NZ * G), block (32, kBY).
-template <int VM, int R>
+template <int VM, int R, bool CL>
 __global__ void __launch_bounds__(kThreads) k_rb_first_mr(OpParams<double> op, double* __restrict__ xx,
                                                            double* __restrict__ v, const double* __restrict__ r,
                                                            const double* __restrict__ q, const SolverState* st, int K,
@@ -213,11 +219,7 @@ __global__ void __launch_bounds__(kThreads) k_rb_first_mr(OpParams<double> op, d
   }
   Coef<double> c;
   bool has = false;
-  if (ok[0]) {
-    const unsigned long long w = __ldg(op.nkey + r0 + p);
-    has = cell_coef<double, true>(op, k, (uint8_t)w, (uint8_t)(w >> 8), (uint8_t)(w >> 16), (uint8_t)(w >> 24),
-                                  (uint8_t)(w >> 32), (uint8_t)(w >> 40), (uint8_t)(w >> 48), r0 + p, c);
-  }
+  if (ok[0]) has = mr_coef<CL>(op, k, r0 + p, c);
 #pragma unroll
   for (int rr = 0; rr < R; ++rr) {
     const int qq = gq * R + rr;
@@ -252,7 +254,7 @@ __global__ void __launch_bounds__(kThreads) k_rb_first_mr(OpParams<double> op, d
 
 // One colour pass (rbsor_core!, omega = 1) for K right-hand sides; one plane per thread.
 // Grid (gx, gy, NZ * G), block (32, kBY).
-template <int R>
+template <int R, bool CL>
 __global__ void __launch_bounds__(kThreads) k_rb_pass_mr(OpParams<double> op, double* x, const double* __restrict__ bb,
                                                           int color, const SolverState* st, int K, long long n) {
   pdl_enter();
@@ -267,11 +269,8 @@ __global__ void __launch_bounds__(kThreads) k_rb_pass_mr(OpParams<double> op, do
   if (!(pok && i >= 1 && i <= g.NX)) return;
   const int ro = g.row(o, j, k), ac = g.row(color, j, k) + p;
   const int HP2 = 2 * g.HP, PL = (int)g.plane;
-  const unsigned long long w = __ldg(op.nkey + ac);
   Coef<double> c;
-  if (!cell_coef<double, true>(op, k, (uint8_t)w, (uint8_t)(w >> 8), (uint8_t)(w >> 16), (uint8_t)(w >> 24),
-                               (uint8_t)(w >> 32), (uint8_t)(w >> 40), (uint8_t)(w >> 48), ac, c))
-    return;
+  if (!mr_coef<CL>(op, k, ac, c)) return;
   const int qx = p - 1 + 2 * e;  // the x-neighbour in the other column
   const bool qok = qx >= 0 && qx < g.HN;
 #pragma unroll
@@ -293,7 +292,7 @@ __global__ void __launch_bounds__(kThreads) k_rb_pass_mr(OpParams<double> op, do
 
 // CalcAX! with its dot products for K right-hand sides: y = A x; NDOT 1: (y, u); NDOT 2: (y,y),
 // (y, w) -> stage.  Grid (gx, gy, NZ * G), block (32, kBY).
-template <int NDOT, int R>
+template <int NDOT, int R, bool CL>
 __global__ void __launch_bounds__(kThreads, 2) k_ax_mr(OpParams<double> op, double* __restrict__ y,
                                                                   const double* __restrict__ x,
                                                                   const double* __restrict__ u,
@@ -321,22 +320,15 @@ __global__ void __launch_bounds__(kThreads, 2) k_ax_mr(OpParams<double> op, doub
     const int r0 = g.row(0, j, k), r1 = r0 + g.HP;
     const int e0 = (1 + j + k) & 1;
     bool ok[2];
-    unsigned long long nk[2] = {0ull, 0ull};
 #pragma unroll
     for (int col = 0; col < 2; ++col) {
       const int i = 2 * p + (e0 ^ col);
       ok[col] = pok && i >= 1 && i <= g.NX;
-      if (ok[col]) nk[col] = __ldg(op.nkey + (col ? r1 : r0) + p);
     }
     Coef<double> c[2];
     bool has[2];
 #pragma unroll
-    for (int col = 0; col < 2; ++col) {
-      const unsigned long long wk = nk[col];
-      has[col] = ok[col] && cell_coef<double, true>(op, k, (uint8_t)wk, (uint8_t)(wk >> 8), (uint8_t)(wk >> 16),
-                                                    (uint8_t)(wk >> 24), (uint8_t)(wk >> 32), (uint8_t)(wk >> 40),
-                                                    (uint8_t)(wk >> 48), (col ? r1 : r0) + p, c[col]);
-    }
+    for (int col = 0; col < 2; ++col) has[col] = ok[col] && mr_coef<CL>(op, k, (col ? r1 : r0) + p, c[col]);
 #pragma unroll
     for (int rr = 0; rr < R; ++rr) {
       if (!run[rr]) continue;

@@ -1389,6 +1389,7 @@ static dim3 mr_grid(const Geo& g, int K) {
   return dim3((g.HN + kBX - 1) / kBX, (g.NY + kBY - 1) / kBY, g.NZ * G);
 }
 
+template <bool CL>
 static int launch_pbicg_body_mr(Solver* s, cudaStream_t cs, const OpParams<double>& op, cudaGraphConditionalHandle hc,
                                 int use_cond) {
   const Geo& g = s->g;
@@ -1399,20 +1400,20 @@ static int launch_pbicg_body_mr(Solver* s, cudaStream_t cs, const OpParams<doubl
   const dim3 grid = mr_grid(g, K), blk(kBX, kBY);
   SolverState* st = s->mr_st;
   // p = r + beta (p - omega q); p_ = M^-1 p                     NonUniform.jl:296-305
-  launch(s, k_rb_first_mr<1, kMrR>, grid, blk, cs, op, ph, p, (const double*)r, (const double*)q,
+  launch(s, k_rb_first_mr<1, kMrR, CL>, grid, blk, cs, op, ph, p, (const double*)r, (const double*)q,
          (const SolverState*)st, K, n);
   for (int pass = 1; pass < 2 * kSweeps; ++pass)
-    launch(s, k_rb_pass_mr<kMrR>, grid, blk, cs, op, ph, (const double*)p, pass & 1, (const SolverState*)st, K, n);
+    launch(s, k_rb_pass_mr<kMrR, CL>, grid, blk, cs, op, ph, (const double*)p, pass & 1, (const SolverState*)st, K, n);
   // q = A p_;  alpha = rho / (q, r0)                            NonUniform.jl:307-309
-  launch(s, k_ax_mr<1, kMrR>, grid, blk, cs, op, q, (const double*)ph, (const double*)r0, (const double*)nullptr, st,
+  launch(s, k_ax_mr<1, kMrR, CL>, grid, blk, cs, op, q, (const double*)ph, (const double*)r0, (const double*)nullptr, st,
          s->mr_partials, (int)kStageAlpha, K, n);
   // s = r - alpha q; s_ = M^-1 s                                NonUniform.jl:310-315
-  launch(s, k_rb_first_mr<2, kMrR>, grid, blk, cs, op, sh, sv, (const double*)r, (const double*)q,
+  launch(s, k_rb_first_mr<2, kMrR, CL>, grid, blk, cs, op, sh, sv, (const double*)r, (const double*)q,
          (const SolverState*)st, K, n);
   for (int pass = 1; pass < 2 * kSweeps; ++pass)
-    launch(s, k_rb_pass_mr<kMrR>, grid, blk, cs, op, sh, (const double*)sv, pass & 1, (const SolverState*)st, K, n);
+    launch(s, k_rb_pass_mr<kMrR, CL>, grid, blk, cs, op, sh, (const double*)sv, pass & 1, (const SolverState*)st, K, n);
   // t = A s_; omega = (t,s)/(t,t)                               NonUniform.jl:317-326
-  launch(s, k_ax_mr<2, kMrR>, grid, blk, cs, op, t, (const double*)sh, (const double*)nullptr, (const double*)sv, st,
+  launch(s, k_ax_mr<2, kMrR, CL>, grid, blk, cs, op, t, (const double*)sh, (const double*)nullptr, (const double*)sv, st,
          s->mr_partials, (int)kStageOmega, K, n);
   // x += alpha p_ + omega s_; r = s - omega t; res; next rho    NonUniform.jl:328-346
   const dim3 ug(elementwise_blocks(s), K);
@@ -1438,15 +1439,21 @@ static int solve_multi(Solver* s, double tol, int maxItr, int smoother, h2g_resu
   OpParams<double> op = op_params<double>(s, s->t64);
   launch(s, k_prime_mr, 1, kMrMax, s->stream, s->mr_st, s->mr_ctl, tol, maxItr, K);
   // r = b - A theta, r0 = r, res0 and rho of every right-hand side   NonUniform.jl:262-274
-  launch(s, k_rk_mr<kMrR>, mr_grid(g, K), dim3(kBX, kBY), s->stream, op, s->mr_kv[0], s->mr_kv[1],
-         (const double*)s->mr_th, (const double*)s->mr_b, s->mr_st, s->mr_partials, (int)kStageInit, K, g.n);
+  if (op.cls)
+    launch(s, k_rk_mr<kMrR, true>, mr_grid(g, K), dim3(kBX, kBY), s->stream, op, s->mr_kv[0], s->mr_kv[1],
+           (const double*)s->mr_th, (const double*)s->mr_b, s->mr_st, s->mr_partials, (int)kStageInit, K, g.n);
+  else
+    launch(s, k_rk_mr<kMrR, false>, mr_grid(g, K), dim3(kBX, kBY), s->stream, op, s->mr_kv[0], s->mr_kv[1],
+           (const double*)s->mr_th, (const double*)s->mr_b, s->mr_st, s->mr_partials, (int)kStageInit, K, g.n);
   CKL();
   SolveGraph& G = s->mr_graph;
   std::vector<unsigned char> sig = signature(op, op, smoother, (const void*)s->mr_th);
   if (!G.exec || G.sig != sig) {
     int berr = H2G_OK;
     int rc = make_loop_graph(s, G, [&](cudaStream_t cs, cudaGraphConditionalHandle hc, int use_cond) {
-      for (int u = 0; u < kUnroll && berr == H2G_OK; ++u) berr = launch_pbicg_body_mr(s, cs, op, hc, use_cond);
+      for (int u = 0; u < kUnroll && berr == H2G_OK; ++u)
+        berr = op.cls ? launch_pbicg_body_mr<true>(s, cs, op, hc, use_cond)
+                      : launch_pbicg_body_mr<false>(s, cs, op, hc, use_cond);
     });
     if (rc == H2G_OK && berr != H2G_OK) G.reset();
     if (rc) return rc;
@@ -1515,6 +1522,21 @@ static int solve(Solver* s, bool cg, double tol, int maxItr, int smoother, int v
 // ------------------------------------------------------------------------------------------
 // creation and set-up
 // ------------------------------------------------------------------------------------------
+// One rbsor! (colour 0, colour 1, each with its residual sum) with the coefficients from the key
+// tables (DDM 1) or the stencil-class table (DDM 2).
+template <int DDM>
+static void sor_passes(Solver* s, cudaStream_t cs, const OpParams<double>& op, dim3 rg, dim3 blk, double omega,
+                       SolverState* st, cudaGraphConditionalHandle hc, int use_cond) {
+  launch(s, k_sor_pass<false, DDM>, rg, blk, cs, op, s->th, (const double*)s->b, 0, omega, st, s->partials,
+         (int)kStageSorHalf, hc, 0);
+  if (use_cond)
+    launch(s, k_sor_pass<true, DDM>, rg, blk, cs, op, s->th, (const double*)s->b, 1, omega, st, s->partials,
+           (int)kStageSorIter, hc, use_cond);
+  else
+    launch(s, k_sor_pass<false, DDM>, rg, blk, cs, op, s->th, (const double*)s->b, 1, omega, st, s->partials,
+           (int)kStageSorIter, hc, use_cond);
+}
+
 // solveSOR! (NonUniform.jl:1004-1051): res0 = resSOR, then rbsor! passes (colour 0, colour 1,
 // each with its sum of squared residuals) until sqrt(sum)/res0 < tol.  FP64 on every handle
 // precision.  Deviation: a non-finite residual stops the loop (the reference would run maxItr
@@ -1540,14 +1562,8 @@ static int solve_sor(Solver* s, double omega, double tol, int maxItr, int verbos
   memcpy(sig.data() + sizeof op, &omega, sizeof omega);
   if (!G.exec || G.sig != sig) {
     rc = make_loop_graph(s, G, [&](cudaStream_t cs, cudaGraphConditionalHandle hc, int use_cond) {
-      launch(s, k_sor_pass<false>, rg, blk, cs, op, s->th, (const double*)s->b, 0, omega, st, s->partials,
-             (int)kStageSorHalf, hc, 0);
-      if (use_cond)
-        launch(s, k_sor_pass<true>, rg, blk, cs, op, s->th, (const double*)s->b, 1, omega, st, s->partials,
-               (int)kStageSorIter, hc, use_cond);
-      else
-        launch(s, k_sor_pass<false>, rg, blk, cs, op, s->th, (const double*)s->b, 1, omega, st, s->partials,
-               (int)kStageSorIter, hc, use_cond);
+      if (op.cls) sor_passes<2>(s, cs, op, rg, blk, omega, st, hc, use_cond);
+      else sor_passes<1>(s, cs, op, rg, blk, omega, st, hc, use_cond);
     });
     if (rc) return rc;
     G.sig = sig;
