@@ -289,8 +289,8 @@ def cpu_baseline_leg(a, it64: int) -> dict:
 
 
 # DRAM bytes (read + write) per launch of the dominant kernel, from one ncu capture each (see the
-# profiles/ summaries): key (nx, nz, fused).
-SWEEP_TRAFFIC_F64 = {(240, 30, False): 37.463e6}
+# profiles/ summaries): key (nx, nz, fused, coefficient source: 1 dd array + key word, 2 class table).
+SWEEP_TRAFFIC_F64 = {(240, 30, False, 1): 37.463e6, (240, 30, False, 2): 24.584e6, (480, 60, False, 2): 222.2e6}
 
 
 def kernel_rates(nx, nz, solvers, torch, stream, flush, reps):
@@ -304,6 +304,7 @@ def kernel_rates(nx, nz, solvers, torch, stream, flush, reps):
     for name, s in solvers.items():
         w_elem = 8 if name == "fp64" else 4
         fused = bool(s.sweep()[0])
+        source = s.tuning()[2]
         for kind, bytes_per_cell, label in ((0, 3 * w_elem + 1, "rb_sweep"), (1, 2 * 8 + 1, "calcax")):
             cold = []
             for r in range(reps + 3):
@@ -328,15 +329,17 @@ def kernel_rates(nx, nz, solvers, torch, stream, flush, reps):
             out[(name, label)] = {"seconds": warm, "gbs": nbytes / warm / 1e9, "seconds_cold": tc,
                                   "gbs_cold": nbytes / tc / 1e9, "bytes": nbytes,
                                   "launches": (1 if fused else 2) if kind == 0 else 1,
-                                  "fused": fused if kind == 0 else None}
+                                  "fused": fused if kind == 0 else None, "source": source}
     return out
 
 
 def roofline_object(rm, peak, peak_kind, nx, nz):
     fused = bool(rm["fused"])
+    src = rm.get("source", 1)
     name = ("k_rb_sweep<double>: one fused RB-GS sweep (both colours, TMA-staged z-march) of the FP64 smoother"
-            if fused else "k_rb_pass<double>: one RB-GS sweep (colour 0 then colour 1) of the FP64 smoother")
-    traffic = SWEEP_TRAFFIC_F64.get((nx, nz, fused))
+            if fused else "k_rb_pass<double>: one RB-GS sweep (colour 0 then colour 1) of the FP64 smoother, "
+            + {0: "dd summed per cell", 1: "dd read per cell", 2: "coefficients from the stencil-class table"}[src])
+    traffic = SWEEP_TRAFFIC_F64.get((nx, nz, fused, src))
     return {"bound": "hbm", "achieved": rm["gbs"], "peak": peak, "unit": "GB/s", "frac": rm["gbs"] / peak,
             "traffic": None if traffic is None else traffic * rm["launches"],
             "traffic_unit": f"DRAM bytes per sweep ({rm['launches']} launch(es)), ncu, L2 flushed",
