@@ -82,28 +82,32 @@ def from_json(text: str) -> list[Member]:
 
 
 def heat_map(m: Member, ID: np.ndarray, ZC: np.ndarray, dx: float, dy: float) -> np.ndarray:
-    """hsrc (MX, MY, MZ), Fortran order, guards zero."""
+    """hsrc (MX, MY, MZ), Fortran order, guards zero.  A hotspot spans its die's thickness, so each
+    die's map is summed once in (x, y), hotspot by hotspot in draw order, and copied to the die's
+    planes."""
     MX, MY, MZ = ID.shape
     xc = (np.arange(MX) - 0.5) * dx  # centre of cell i (0-based; interior i = 1..NX)
     yc = (np.arange(MY) - 0.5) * dy
-    silicon = np.isin(ID, SILICON_IDS)
     hs = np.zeros((MX, MY, MZ), order="F")
-    acc = np.zeros((MX, MY, MZ), order="F")
     for d, (z0, z1) in enumerate(DIE_Z):
-        kin = (ZC >= z0) & (ZC <= z1)
-        hs[:, :, kin] = BACKGROUND
+        kin = np.flatnonzero((ZC >= z0) & (ZC <= z1))
+        if kin.size == 0:
+            continue
+        acc = np.zeros((MX, MY))
         for h in m.hotspots:
             if h.die != d:
                 continue
             ix = (xc >= h.x0) & (xc < h.x1)
             iy = (yc >= h.y0) & (yc < h.y1)
-            acc[np.ix_(ix, iy, kin)] += h.q
-    hs = np.where(acc > 0.0, acc, hs)
-    hs[~silicon] = 0.0
+            acc[np.ix_(ix, iy)] += h.q
+        plane = np.where(acc > 0.0, acc, BACKGROUND)
+        sub = ID[:, :, kin]
+        silicon = (sub == SILICON_IDS[0]) | (sub == SILICON_IDS[1])
+        hs[:, :, kin] = np.where(silicon, plane[:, :, None], 0.0)
     hs[0, :, :] = hs[-1, :, :] = 0.0
     hs[:, 0, :] = hs[:, -1, :] = 0.0
     hs[:, :, 0] = hs[:, :, -1] = 0.0
-    return np.asfortranarray(hs)
+    return hs
 
 
 def shard(members: list[Member], world: int) -> list[list[int]]:
@@ -151,21 +155,21 @@ class BatchSolver:
         self.L, self.C = L, C
         self.members = list(members)
         self.solvers = []
-        ids: dict[int, np.ndarray] = {}
+        # the members of one grid size differ only in their heat map: the model (geometry,
+        # conductivities, mask, start temperature, boundary conditions) is built once per size
+        models: dict[int, object] = {}
         _, ZC, _ = M.zgrid(NZ)
         for m in self.members:
-            if m.nx not in ids:
-                ids[m.nx] = M.fill_id(m.nx, m.nx, NZ)
-            ID = ids[m.nx]
-            dx = M.pitch(m.nx)
-            model = M.build_mode3(m.nx, m.nx, NZ, ID=ID, hsrc=heat_map(m, ID, ZC, dx, dx), calrhs=False)
+            if m.nx not in models:
+                models[m.nx] = M.build_mode3(m.nx, m.nx, NZ, calrhs=False)
+            model = models[m.nx]
             w = model.wk
             s = Solver(*model.shape, precision=precision)
             s.set_grid(model.ZC, model.dZ, model.dx, model.dy, model.dt, model.HC, True)
             s.set_fields(w.lam, w.mask)
             s.set_theta(w.theta)
             # calRHS! on the member's own handle: b = -(hsrc V + boundary terms), from b = 0
-            s.set_hsrc(w.hsrc)
+            s.set_hsrc(heat_map(m, model.ID, ZC, model.dx, model.dy))
             s.calrhs(model.bcs, zero_b=True)
             s.snapshot()
             self.solvers.append(s)
@@ -225,9 +229,8 @@ class MultiBatchSolver:
         _, ZC, _ = M.zgrid(NZ)
         for nx in sorted({m.nx for m in self.members}):
             idx = [q for q, m in enumerate(self.members) if m.nx == nx]
-            ID = M.fill_id(nx, nx, NZ)
-            dx = M.pitch(nx)
-            base = M.build_mode3(nx, nx, NZ, ID=ID, calrhs=False)
+            base = M.build_mode3(nx, nx, NZ, calrhs=False)
+            ID, dx = base.ID, base.dx
             w = base.wk
             helper = Solver(*base.shape, stream=stream)
             bs, th0 = [], []
