@@ -24,6 +24,12 @@ namespace h2g {
 #ifndef H2G_MINB
 #define H2G_MINB 4
 #endif
+// The colour pass reading the stencil-class table needs fewer registers: 5 resident blocks of 256
+// threads per SM (48 registers, no spills) measured -1 % per FP64 solve at 240x240x30 and -2.4 %
+// at 480x480x60 (-5.5 % per sweep) against 4; 6 blocks (40 registers) spill and were slower.
+#ifndef H2G_MINB_CLS
+#define H2G_MINB_CLS 5
+#endif
 // x-neighbours by direct loads (1) or warp shuffles (0): loads measured 6 % faster per solve
 // on the 240x240x30 grid (fewer LSU instructions)
 #ifndef H2G_XNB_LOAD
@@ -566,7 +572,7 @@ constexpr int kRbRows[4] = {2, 4, 8, 16};
 // instructions); 2 (FP64): the stencil-class table (2 bytes per cell instead of the 8-byte key
 // word and dd).  The tuner picks it with the shape.
 template <typename T, int BY = kBY, int NP = 2, int DDM = 1>
-__global__ void __launch_bounds__(kBX * BY, (H2G_MINB * kBY) / BY)
+__global__ void __launch_bounds__(kBX * BY, ((DDM == 2 ? H2G_MINB_CLS : H2G_MINB) * kBY) / BY)
     k_rb_pass(OpParams<T> op, T* x, const T* __restrict__ bb, int color, T omega,
               const SolverState* __restrict__ st) {
   pdl_enter();
