@@ -1,0 +1,78 @@
+"""The kernels at the scaling configurations' full sizes (480x480x60: 13.8 M cells, and
+960x960x120: 110.6 M cells, Z refined), where no oracle solve finishes in seconds but the oracle's
+single kernels do (OpenMP over all host cores):
+
+* CalcAX and the 5-sweep RB-GS preconditioner equal the oracle bit for bit on the Mode-3 stack
+  (the GPU model's own fields, wrapped in an oracle problem);
+* at 960x960x120 every coefficient source (stencil-class table, key tables with dd read, key
+  tables with dd summed) gives the same bits, and the class table is built there;
+* the operator is symmetric, x.(A y) = y.(A x) to rounding, as the adjoint solve relies on.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import h2_b200
+from h2_b200 import model as M
+from test_gpu_kernels import random_interior
+
+pytestmark = pytest.mark.gpu
+
+THREADS = os.cpu_count()
+
+
+def _problem(oracle, m):
+    """An oracle problem over the GPU model's arrays (the oracle's kernels read lam, mask, rho and
+    cp of the work buffers and the grid)."""
+    w = m.wk
+    wk = {n: np.asfortranarray(getattr(w, n)) for n in ("theta", "b", "mask", "rho", "lam", "cp")}
+    return oracle.Problem(m.NX, m.NY, m.NZ, m.dx, m.dy, m.dt, m.is_steady, m.Z, m.ZC, m.dZ, m.HC, m.bcs, m.ID, wk)
+
+
+def _solver(m):
+    w = m.wk
+    s = h2_b200.Solver(*m.shape)
+    s.set_grid(m.ZC, m.dZ, m.dx, m.dy, m.dt, m.HC, True)
+    s.set_fields(w.lam, w.mask)
+    s.set_rhs(w.b)
+    s.set_theta(w.theta)
+    return s
+
+
+def _source(monkeypatch, s, src):
+    """Force a coefficient source (and the tuner's usual shape, so that nothing is timed)."""
+    for k, v in (("H2G_RB_ROWS", "4"), ("H2G_RB_PLANES", "2"), ("H2G_RB_DD", src), ("H2G_AX_DD", src),
+                 ("H2G_RB_FUSED", "0")):
+        monkeypatch.setenv(k, v)
+    s.set_tuning(0)  # the next call applies the forced choices
+    assert s.tuning()[2:] == (int(src), int(src))
+
+
+@pytest.mark.parametrize("nx,nz", [(480, 60), (960, 120)], ids=["480x480x60", "960x960x120"])
+def test_kernels_match_oracle_full_size(oracle, monkeypatch, nx, nz):
+    m = M.build_mode3(nx, nx, nz)
+    prob = _problem(oracle, m)
+    s = _solver(m)
+    try:
+        x = random_interior(m.shape, nx)
+        ref_ax = oracle.calc_ax(prob, x, threads=THREADS)
+        ref_pc = oracle.preconditioner(prob, x, "gs", threads=THREADS)
+        sources = ("2", "1", "0") if nx == 960 else ("2",)
+        for src in sources:
+            _source(monkeypatch, s, src)
+            ax = s.calc_ax(x)
+            assert np.array_equal(ax[1:-1, 1:-1, 1:-1], ref_ax[1:-1, 1:-1, 1:-1]), src
+            assert np.array_equal(s.preconditioner(x, "gs"), ref_pc), src
+        if nx == 960:
+            # symmetry of A over the interior (guards of x and y are zero)
+            y = random_interior(m.shape, nx + 1)
+            ay = s.calc_ax(y)
+            inner = (slice(1, -1),) * 3
+            xa = x[inner].ravel()
+            lhs = float(np.dot(xa, ay[inner].ravel()))
+            rhs = float(np.dot(y[inner].ravel(), ax[inner].ravel()))
+            scale = float(np.abs(xa * ay[inner].ravel()).sum())
+            assert abs(lhs - rhs) <= 1e-12 * scale, (lhs, rhs, scale)
+    finally:
+        s.close()
