@@ -1430,6 +1430,17 @@ __global__ void __launch_bounds__(256) k_make_dd(OpParams<T> op, T* __restrict__
   ddv[o] = has ? c.dd : T(1);
 }
 
+// *flag = 1 if the arrays a and b (n 16-byte words) differ anywhere.
+__global__ void __launch_bounds__(256) k_bytes_differ(const uint4* __restrict__ a, const uint4* __restrict__ b,
+                                                       long long n, int* flag) {
+  int d = 0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const uint4 x = a[i], y = b[i];
+    d |= (x.x != y.x) | (x.y != y.y) | (x.z != y.z) | (x.w != y.w);
+  }
+  if (__syncthreads_or(d) && threadIdx.x == 0) *flag = 1;
+}
+
 // Per interior cell, the 7 keys its stencil reads packed in one word: own key (byte 0) and the
 // keys of its x-, x+, y-, y+, z-, z+ neighbours (bytes 1..6).  Guards and padding: 0.
 __global__ void __launch_bounds__(256) k_make_nkeys(Geo g, const uint8_t* __restrict__ key,

@@ -166,6 +166,12 @@ struct Solver {
   bool ax_cls = false;    // FP64 CalcAX reads the stencil-class table (autotuned)
   // stencil classes of the FP64 operator (k_class_*): per-cell index, table, build scratch
   bool cls_ok = false;    // the grid's classes are built (at most kMaxClasses, NZ <= 255)
+  // operator data rebuilt only when its inputs change (build_tables): the inputs of the last
+  // build, and whether h2g_set_fields produced a key array different from the last one
+  std::vector<unsigned char> tables_sig;
+  bool keys_changed = true;
+  uint8_t* key_prev = nullptr;
+  int* kdiff = nullptr;
   int ncls = 0;
   uint16_t* cls = nullptr;
   double* ctab = nullptr;
@@ -631,7 +637,7 @@ static void destroy(Solver* s) {
   for (auto& p : s->stage) cudaFree(p);
   cudaFree(s->x2_64); cudaFree(s->x2_32); cudaFree(s->sweep_err); cudaFree(s->gbar);
   cudaFree(s->cls); cudaFree(s->ctab); cudaFree(s->cslots); cudaFree(s->slot_class); cudaFree(s->cwords);
-  cudaFree(s->cflag);
+  cudaFree(s->cflag); cudaFree(s->key_prev); cudaFree(s->kdiff);
   s->mr_graph.reset();
   cudaFree(s->mr_th); cudaFree(s->mr_b); cudaFree(s->mr_st); cudaFree(s->mr_ctl); cudaFree(s->mr_partials);
   cudaFree(s->mr_flag);
@@ -745,8 +751,35 @@ static int build_classes(Solver* s) {
   return H2G_OK;
 }
 
+// Everything the operator tables, dd and the stencil classes are built from, besides the key array.
+static std::vector<unsigned char> tables_signature(const Solver* s) {
+  std::vector<unsigned char> v;
+  auto put = [&](const void* p, size_t n) {
+    const unsigned char* c = static_cast<const unsigned char*>(p);
+    v.insert(v.end(), c, c + n);
+  };
+  put(&s->P, sizeof s->P);
+  put(s->lam_values.data(), sizeof(double) * s->lam_values.size());
+  put(s->ZC.data(), sizeof(double) * s->ZC.size());
+  put(s->dZ.data(), sizeof(double) * s->dZ.size());
+  put(&s->dx, sizeof s->dx);
+  put(&s->dy, sizeof s->dy);
+  put(&s->dt, sizeof s->dt);
+  put(s->HC, sizeof s->HC);
+  put(&s->steady, sizeof s->steady);
+  const char* e = getenv("H2G_CLS");
+  const std::string cls_env = e ? e : "";
+  put(cls_env.data(), cls_env.size());
+  return v;
+}
+
 static int build_tables(Solver* s) {
   if (!s->grid_set || !s->fields_set) return H2G_OK;
+  // a steady grid whose keys and table inputs equal those of the last build keeps its tables,
+  // dd and classes (repeated one-call solves of one operator)
+  std::vector<unsigned char> sig = tables_signature(s);
+  if (!s->keys_changed && s->steady && sig == s->tables_sig) return H2G_OK;
+  s->tables_sig.clear();
   const Geo& g = s->g;
   const int P = s->P;
   const int pc = std::max(P, 8);
@@ -851,7 +884,10 @@ static int build_tables(Solver* s) {
   }
   // host vectors must stay alive until the copies ran
   CK(cudaStreamSynchronize(s->stream));
-  return build_classes(s);
+  if (int rc = build_classes(s)) return rc;
+  s->tables_sig = std::move(sig);
+  s->keys_changed = false;
+  return H2G_OK;
 }
 
 // ------------------------------------------------------------------------------------------
@@ -2272,8 +2308,9 @@ static int create(int MX, int MY, int MZ, int precision, Solver** out) {
   return H2G_OK;
 }
 
+// build = false leaves the operator tables to the h2g_set_fields that follows (one-call path).
 static int set_grid(Solver* s, const double* ZC, const double* dZ, double dx, double dy, double dt, const double* HC,
-                    int is_steady) {
+                    int is_steady, bool build = true) {
   if (!ZC || !dZ || !HC) return fail(H2G_BAD_ARG, "null ZC/dZ/HC");
   if (!(dx > 0) || !(dy > 0) || !std::isfinite(dx) || !std::isfinite(dy)) return fail(H2G_BAD_ARG, "bad dx/dy");
   if (!is_steady && !(dt > 0 && std::isfinite(dt))) return fail(H2G_BAD_ARG, "bad dt");
@@ -2293,7 +2330,7 @@ static int set_grid(Solver* s, const double* ZC, const double* dZ, double dx, do
   s->grid_set = true;
   if (s->fields_set && !s->steady && (was_steady || !s->rc_valid))
     return fail(H2G_BAD_ARG, "switching to a transient grid needs h2g_set_fields with rho and cp");
-  return build_tables(s);
+  return build ? build_tables(s) : H2G_OK;
 }
 
 static int set_fields(Solver* s, const double* lam, const double* mask, const double* rho, const double* cp) {
@@ -2358,12 +2395,31 @@ static int set_fields(Solver* s, const double* lam, const double* mask, const do
                                                     s->slot_index, s->key, s->rc32);
     CKL();
   }
-  if (!s->nkey) {
-    CK(cudaMalloc(&s->nkey, sizeof(unsigned long long) * (size_t)g.n));
-    CK(cudaMemsetAsync(s->nkey, 0, sizeof(unsigned long long) * (size_t)g.n, s->stream));
-    invalidate_graphs(s);
+  // is the key array the last one?  (transient grids rebuild always: rho*cp enters dd)
+  bool same = false;
+  if (s->key_prev && !rho && s->nkey) {
+    int diff = 1;
+    CK(cudaMemsetAsync(s->kdiff, 0, sizeof(int), s->stream));
+    k_bytes_differ<<<s->num_sms * 4, 256, 0, s->stream>>>(reinterpret_cast<const uint4*>(s->key),
+                                                          reinterpret_cast<const uint4*>(s->key_prev),
+                                                          (long long)g.n / 16, s->kdiff);
+    CKL();
+    CK(cudaMemcpyAsync(&diff, s->kdiff, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    same = diff == 0;
   }
-  {
+  if (!s->key_prev) {
+    CK(cudaMalloc(&s->key_prev, (size_t)g.n));
+    CK(cudaMalloc(&s->kdiff, sizeof(int)));
+  }
+  if (!same) {
+    CK(cudaMemcpyAsync(s->key_prev, s->key, (size_t)g.n, cudaMemcpyDeviceToDevice, s->stream));
+    s->keys_changed = true;
+    if (!s->nkey) {
+      CK(cudaMalloc(&s->nkey, sizeof(unsigned long long) * (size_t)g.n));
+      CK(cudaMemsetAsync(s->nkey, 0, sizeof(unsigned long long) * (size_t)g.n, s->stream));
+      invalidate_graphs(s);
+    }
     const dim3 gi((g.NX + 127) / 128, g.NY, g.NZ);
     k_make_nkeys<<<gi, 128, 0, s->stream>>>(g, s->key, s->nkey);
     CKL();
@@ -2616,7 +2672,8 @@ static int oneshot(int method, int MX, int MY, int MZ, double* theta, const doub
   }
   int rc;
   if (!h && (rc = h2g_create(MX, MY, MZ, precision, &h))) return rc;
-  if ((rc = h2g_set_grid(h, ZC, dZ, dx, dy, dt, HC, is_steady))) return rc;
+  // the tables are built once, by set_fields, from the new grid and fields
+  if ((rc = h2g::set_grid(S(h), ZC, dZ, dx, dy, dt, HC, is_steady, false))) return rc;
   if ((rc = h2g_set_fields(h, lambda, mask, is_steady ? nullptr : rho, is_steady ? nullptr : cp))) return rc;
   if ((rc = h2g_set_rhs(h, b))) return rc;
   if ((rc = h2g_set_theta(h, theta))) return rc;

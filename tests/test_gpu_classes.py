@@ -100,3 +100,34 @@ def test_classes_disabled_or_too_many(oracle, monkeypatch):
     x = random_interior(prob.shape, 2)
     assert np.array_equal(s.calc_ax(x)[1:-1, 1:-1, 1:-1], oracle.calc_ax(prob, x)[1:-1, 1:-1, 1:-1])
     s.close()
+
+
+def test_operator_rebuilt_when_inputs_change(oracle):
+    """One handle given new conductivity values (same key layout), new boundary coefficients, the
+    first fields again and the same fields twice: every CalcAX and preconditioner equals the
+    oracle's for the inputs of that moment.  A build is skipped only when nothing changed."""
+    import copy
+    a = mode3_model(oracle, 40)
+    a2 = copy.deepcopy(a)
+    a2.wk["lam"][...] = a2.wk["lam"] * 1.5
+    a3 = copy.deepcopy(a)
+    a3.HC = a3.HC * 2.0
+    x = random_interior(a.shape, 17)
+    s = make_solver(a)
+
+    def check(prob):
+        assert np.array_equal(s.calc_ax(x)[1:-1, 1:-1, 1:-1], oracle.calc_ax(prob, x)[1:-1, 1:-1, 1:-1])
+        assert np.array_equal(s.preconditioner(x, "gs"), oracle.preconditioner(prob, x, "gs"))
+
+    check(a)
+    s.set_fields(a2.wk["lam"], a2.wk["mask"])
+    check(a2)
+    s.set_fields(a.wk["lam"], a.wk["mask"])
+    check(a)
+    s.set_grid(a3.ZC, a3.dZ, a3.dx, a3.dy, a3.dt, a3.HC, True)
+    check(a3)
+    s.set_grid(a.ZC, a.dZ, a.dx, a.dy, a.dt, a.HC, True)
+    s.set_fields(a.wk["lam"], a.wk["mask"])
+    s.set_fields(a.wk["lam"], a.wk["mask"])
+    check(a)
+    s.close()
