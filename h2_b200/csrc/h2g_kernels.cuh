@@ -319,19 +319,32 @@ constexpr unsigned kNoClass = 0xffffu;
 constexpr int kClassSlots = 1 << 17;   // hash slots of the (plane, keys) pairs
 constexpr int kMaxClasses = 65535;     // class indices are 16-bit; 0xffff marks "not updated"
 
+// Row layout (8 values of T): cx-, cx+, cy-, cy+, cz-, cz+, dd, 0.  The FP32 rows serve the FP32
+// smoother only (its CalcAX uses the difference form, which needs a per-cell term the row lacks).
 template <typename T>
 __device__ __forceinline__ bool class_coef(const OpParams<T>& op, unsigned cl, int ci, Coef<T>& c) {
-  static_assert(sizeof(T) == 8, "stencil classes are FP64 only");
   if (cl == kNoClass) return false;
-  const double2* t = reinterpret_cast<const double2*>(op.ctab) + 4 * cl;
-  const double2 a = __ldg(t), b = __ldg(t + 1), z = __ldg(t + 2);
-  c.cxm = a.x;
-  c.cxp = a.y;
-  c.cym = b.x;
-  c.cyp = b.y;
-  c.czm = z.x;
-  c.czp = z.y;
-  c.dd = op.steady ? __ldg(reinterpret_cast<const double*>(t + 3)) : __ldg(op.ddv + ci);
+  if constexpr (sizeof(T) == 8) {
+    const double2* t = reinterpret_cast<const double2*>(op.ctab) + 4 * cl;
+    const double2 a = __ldg(t), b = __ldg(t + 1), z = __ldg(t + 2);
+    c.cxm = a.x;
+    c.cxp = a.y;
+    c.cym = b.x;
+    c.cyp = b.y;
+    c.czm = z.x;
+    c.czp = z.y;
+    c.dd = op.steady ? __ldg(reinterpret_cast<const double*>(t + 3)) : __ldg(op.ddv + ci);
+  } else {
+    const float4* t = reinterpret_cast<const float4*>(op.ctab) + 2 * cl;
+    const float4 a = __ldg(t), z = __ldg(t + 1);
+    c.cxm = a.x;
+    c.cxp = a.y;
+    c.cym = a.z;
+    c.cyp = a.w;
+    c.czm = z.x;
+    c.czp = z.y;
+    c.dd = op.steady ? z.z : __ldg(op.ddv + ci);
+  }
   return true;
 }
 
@@ -1509,18 +1522,19 @@ __global__ void __launch_bounds__(256) k_class_assign(Geo g, const unsigned long
 
 // Step 3: one table row per class from cell_coef on the class's (plane, keys) pair, with the
 // grid taken as steady (a_p0 = 0: dd is then the sum of the 12 face terms, what a steady cell of
-// the class gets).
-__global__ void __launch_bounds__(128) k_class_coef(OpParams<double> op, const unsigned long long* __restrict__ words,
-                                                     int ncls, double* __restrict__ ctab) {
+// the class gets), in the precision of the tables op points to.
+template <typename T>
+__global__ void __launch_bounds__(128) k_class_coef(OpParams<T> op, const unsigned long long* __restrict__ words,
+                                                     int ncls, T* __restrict__ ctab) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= ncls) return;
   const unsigned long long w = words[c];
   const int k = (int)(w >> 56);
   op.steady = 1;
-  Coef<double> cf;
-  cell_coef<double, false>(op, k, (uint8_t)w, (uint8_t)(w >> 8), (uint8_t)(w >> 16), (uint8_t)(w >> 24),
-                           (uint8_t)(w >> 32), (uint8_t)(w >> 40), (uint8_t)(w >> 48), 0, cf);
-  double* t = ctab + 8 * (size_t)c;
+  Coef<T> cf;
+  cell_coef<T, false>(op, k, (uint8_t)w, (uint8_t)(w >> 8), (uint8_t)(w >> 16), (uint8_t)(w >> 24),
+                      (uint8_t)(w >> 32), (uint8_t)(w >> 40), (uint8_t)(w >> 48), 0, cf);
+  T* t = ctab + 8 * (size_t)c;
   t[0] = cf.cxm;
   t[1] = cf.cxp;
   t[2] = cf.cym;
@@ -1528,7 +1542,7 @@ __global__ void __launch_bounds__(128) k_class_coef(OpParams<double> op, const u
   t[4] = cf.czm;
   t[5] = cf.czp;
   t[6] = cf.dd;
-  t[7] = 0.0;
+  t[7] = T(0);
 }
 
 // ------------------------------------------------------------------------------------------

@@ -175,6 +175,7 @@ struct Solver {
   int ncls = 0;
   uint16_t* cls = nullptr;
   double* ctab = nullptr;
+  float* ctab32 = nullptr;  // the FP32 smoother's rows (mixed handles)
   unsigned long long* cslots = nullptr;
   uint16_t* slot_class = nullptr;
   unsigned long long* cwords = nullptr;
@@ -300,11 +301,9 @@ static void launch_rb_dd(const Solver* s, cudaStream_t cs, const OpParams<T>& op
 template <typename T>
 static void launch_rb(const Solver* s, cudaStream_t cs, const OpParams<T>& op, T* x, const T* bb, int color, T omega,
                       const SolverState* st) {
-  if constexpr (sizeof(T) == 8) {
-    if (s->rb_cls && op.cls) {
-      launch_rb_dd<T, 2>(s, cs, op, x, bb, color, omega, st);
-      return;
-    }
+  if (s->rb_cls && op.cls) {
+    launch_rb_dd<T, 2>(s, cs, op, x, bb, color, omega, st);
+    return;
   }
   if (s->rb_dd) launch_rb_dd<T, 1>(s, cs, op, x, bb, color, omega, st);
   else launch_rb_dd<T, 0>(s, cs, op, x, bb, color, omega, st);
@@ -532,13 +531,9 @@ static int launch_precond(Solver* s, cudaStream_t cs, const OpParams<T>& op, T* 
   if constexpr (std::is_same<T, double>::value && std::is_same<TV, double>::value) {
     if (use_coop(s) && !none && !bbT) return launch_coop<VM>(s, cs, op, xx, v, r, q, st);
   }
-  bool cl = false;
-  if constexpr (sizeof(T) == 8) {
-    cl = s->rb_cls && op.cls && !none;
-    if (cl)
-      launch(s, k_rb_first<T, TV, VM, true>, first_grid(op.g), dim3(kBX, kBY), cs, op, xx, v, bbT, r, q, st, none);
-  }
-  if (!cl)
+  if (s->rb_cls && op.cls && !none)
+    launch(s, k_rb_first<T, TV, VM, true>, first_grid(op.g), dim3(kBX, kBY), cs, op, xx, v, bbT, r, q, st, none);
+  else
     launch(s, k_rb_first<T, TV, VM, false>, first_grid(op.g), dim3(kBX, kBY), cs, op, xx, v, bbT, r, q, st, none);
   if (none) return H2G_OK;
   for (int pass = 1; pass < 2 * kSweeps; ++pass) launch_rb<T>(s, cs, op, xx, bb, pass & 1, T(1), st);
@@ -602,7 +597,12 @@ OpParams<double> op_params<double>(const Solver* s, const OpTables<double>& t) {
 }
 template <>
 OpParams<float> op_params<float>(const Solver* s, const OpTables<float>& t) {
-  return op_params_rc<float>(s, t, s->rc32);
+  OpParams<float> op = op_params_rc<float>(s, t, s->rc32);
+  if (s->cls_ok && s->ctab32) {
+    op.cls = s->cls;
+    op.ctab = s->ctab32;
+  }
+  return op;
 }
 template <typename T>
 static OpParams<T> op_params(const Solver* s, const void* tables) {
@@ -636,7 +636,7 @@ static void destroy(Solver* s) {
   for (auto& p : s->hook) cudaFree(p);
   for (auto& p : s->stage) cudaFree(p);
   cudaFree(s->x2_64); cudaFree(s->x2_32); cudaFree(s->sweep_err); cudaFree(s->gbar);
-  cudaFree(s->cls); cudaFree(s->ctab); cudaFree(s->cslots); cudaFree(s->slot_class); cudaFree(s->cwords);
+  cudaFree(s->cls); cudaFree(s->ctab); cudaFree(s->ctab32); cudaFree(s->cslots); cudaFree(s->slot_class); cudaFree(s->cwords);
   cudaFree(s->cflag); cudaFree(s->key_prev); cudaFree(s->kdiff);
   s->mr_graph.reset();
   cudaFree(s->mr_th); cudaFree(s->mr_b); cudaFree(s->mr_st); cudaFree(s->mr_ctl); cudaFree(s->mr_partials);
@@ -704,6 +704,7 @@ static int build_classes(Solver* s) {
   if (!s->cls) {
     CK(cudaMalloc(&s->cls, sizeof(uint16_t) * (size_t)g.n));
     CK(cudaMalloc(&s->ctab, sizeof(double) * 8 * (size_t)kMaxClasses));
+    if (s->precision != H2G_FP64) CK(cudaMalloc(&s->ctab32, sizeof(float) * 8 * (size_t)kMaxClasses));
     CK(cudaMalloc(&s->cslots, sizeof(unsigned long long) * kClassSlots));
     CK(cudaMalloc(&s->slot_class, sizeof(uint16_t) * kClassSlots));
     CK(cudaMalloc(&s->cwords, sizeof(unsigned long long) * kMaxClasses));
@@ -742,7 +743,11 @@ static int build_classes(Solver* s) {
   k_class_assign<<<gi, 256, 0, s->stream>>>(g, s->nkey, s->cslots, s->slot_class, s->cls);
   const int ncls = (int)words.size();
   OpParams<double> o64 = op_params_rc<double>(s, s->t64, s->rc64);
-  k_class_coef<<<(ncls + 127) / 128, 128, 0, s->stream>>>(o64, s->cwords, ncls, s->ctab);
+  k_class_coef<double><<<(ncls + 127) / 128, 128, 0, s->stream>>>(o64, s->cwords, ncls, s->ctab);
+  if (s->ctab32) {
+    OpParams<float> o32 = op_params_rc<float>(s, s->t32, s->rc32);
+    k_class_coef<float><<<(ncls + 127) / 128, 128, 0, s->stream>>>(o32, s->cwords, ncls, s->ctab32);
+  }
   CKL();
   CK(cudaStreamSynchronize(s->stream));  // the host vectors must outlive the copies
   s->ncls = ncls;
@@ -2150,8 +2155,8 @@ static int autotune(Solver* s) {
   int rows = -1, planes = -1, rbdd = -1, dd = -1, fused = -1, chunks = -1, swdd = -1;
   if (const char* e = getenv("H2G_RB_ROWS")) rows = valid_rows(atoi(e)) ? atoi(e) : -1;
   if (const char* e = getenv("H2G_RB_PLANES")) planes = (atoi(e) == 1 || atoi(e) == 2) ? atoi(e) : -1;
-  // coefficient sources: 0 dd summed, 1 dd read, 2 stencil-class table (FP64, when built)
-  const int nmodes = s->precision == H2G_FP64 && s->cls_ok ? 3 : 2;
+  // coefficient sources: 0 dd summed, 1 dd read, 2 stencil-class table (when built)
+  const int nmodes = s->cls_ok ? 3 : 2;
   if (const char* e = getenv("H2G_RB_DD")) rbdd = std::min(std::max(atoi(e), 0), nmodes - 1);
   if (const char* e = getenv("H2G_AX_DD")) dd = std::min(std::max(atoi(e), 0), nmodes - 1);
   if (const char* e = getenv("H2G_RB_FUSED")) fused = atoi(e) ? 1 : 0;

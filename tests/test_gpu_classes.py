@@ -131,3 +131,51 @@ def test_operator_rebuilt_when_inputs_change(oracle):
     s.set_fields(a.wk["lam"], a.wk["mask"])
     check(a)
     s.close()
+
+
+@pytest.mark.parametrize("case", CASES, ids=["mode3", "adiabatic", "odd", "transient"])
+def test_fp32_smoother_classes_equal_key_tables(oracle, monkeypatch, case):
+    """The FP32 smoother of the mixed handles with its own class rows (FP32 copies written by
+    cell_coef<float>) gives the bits of the FP32 key tables, for 1 and 2 planes per thread."""
+    prob = mode3_model(oracle, **case)
+    bb = random_interior(prob.shape, 23)
+    out = {}
+    for src in ("1", "2"):
+        monkeypatch.setenv("H2G_RB_DD", src)
+        s = make_solver(prob, precision="mixed")
+        assert s.tuning()[2] == int(src)
+        out[src] = []
+        for planes in (1, 2):
+            s.set_tuning(8, planes)
+            out[src].append(s.preconditioner(bb, "gs"))
+        s.close()
+    for a, b_ in zip(out["1"], out["2"]):
+        assert np.array_equal(a, b_)
+
+
+@pytest.mark.parametrize("transient", [False, True], ids=["steady", "transient"])
+def test_fp32_smoother_classes_boxes(oracle, monkeypatch, transient):
+    prob = box_problem(oracle, 33, 31, 9, seed=41, transient=transient)
+    bb = random_interior(prob.shape, 3)
+    res = []
+    for src in ("1", "2"):
+        monkeypatch.setenv("H2G_RB_DD", src)
+        s = make_solver(prob, precision="mixed")
+        res.append(s.preconditioner(bb, "gs"))
+        s.close()
+    assert np.array_equal(res[0], res[1])
+
+
+def test_mixed_solve_identical_across_sources(oracle, monkeypatch):
+    prob = mode3_model(oracle, 41, 37)
+    out = []
+    for src in ("1", "2"):
+        monkeypatch.setenv("H2G_RB_DD", src)
+        monkeypatch.setenv("H2G_AX_DD", src)
+        s = make_solver(prob, precision="mixed")
+        st, res = s.solve("pbicgstab", tol=1e-8, maxItr=20000, smoother="gs")
+        assert st == 0 and res.isconverged
+        out.append((res.itr, res.outer, res.res, s.get_theta()))
+        s.close()
+    assert out[0][:3] == out[1][:3]
+    assert np.array_equal(out[0][3], out[1][3])
