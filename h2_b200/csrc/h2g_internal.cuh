@@ -123,7 +123,7 @@ struct OpParams {
   const T* tq;         // [MZ][P][256][4]: the four face tables of one (plane, own key, neighbour key)
                        // side by side: x, y, z-, z+ (z+ from plane k+1), for the fused sweeps
   const unsigned long long* nkey;  // per cell: own key and the 6 neighbours' keys, one byte each
-  const uint16_t* cls; // per cell: stencil class (FP64 handles; 0xffff: not updated), may be null
+  const uint16_t* cls; // per cell: stencil class (0xffff: not updated), may be null
   const T* ctab;       // [classes][8]: cxm, cxp, cym, cyp, czm, czp, dd of a steady grid, 0
   T czm, czp;          // convective terms of the z-, z+ faces
   T dx0, dy0, ddt;

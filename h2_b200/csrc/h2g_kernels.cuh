@@ -309,7 +309,7 @@ __device__ __forceinline__ bool cell_coef(const OpParams<T>& op, int k, uint8_t 
   return true;
 }
 
-// Stencil classes (FP64).  The coefficients of a cell depend only on its plane k and the 7 key
+// Stencil classes.  The coefficients of a cell depend only on its plane k and the 7 key
 // bytes of its stencil, so the cells of a grid fall into few classes: one per distinct (k, keys)
 // pair.  k_class_coef fills one table row per class with cell_coef itself, for a steady grid, so
 // every value is the one cell_coef gives the cell; a cell then reads a 2-byte class index and one
@@ -582,7 +582,7 @@ constexpr int kRbRows[4] = {2, 4, 8, 16};
 
 // DDM: how a cell gets dd and its coefficients.  0: coefficients from the key tables, dd summed
 // per cell (8 bytes fewer per cell than 1); 1: dd read from the per-cell array (fewer
-// instructions); 2 (FP64): the stencil-class table (2 bytes per cell instead of the 8-byte key
+// instructions); 2: the stencil-class table (2 bytes per cell instead of the 8-byte key
 // word and dd).  The tuner picks it with the shape.
 template <typename T, int BY = kBY, int NP = 2, int DDM = 1>
 __global__ void __launch_bounds__(kBX * BY, ((DDM == 2 ? H2G_MINB_CLS : H2G_MINB) * kBY) / BY)
@@ -791,7 +791,7 @@ __device__ __forceinline__ void load_pair(const Geo& g, const TI* x, const uint8
 // applied in FP64).  Grid (ceil(HN/32), ceil(NY/kBY), NZ).
 // ------------------------------------------------------------------------------------------
 // DDM: 0 coefficients from the key tables with dd summed; 1 dd read from the per-cell array (FP64
-// only; the FP32 operator uses the difference form); 2 the stencil-class table (FP64).  Which is
+// only; the FP32 operator uses the difference form); 2 the stencil-class table (FP64 only).  Which is
 // faster depends on whether the vectors stay in L2; the launch-shape tuner decides.
 template <typename T, int NDOT, typename TI = T, int DDM = 0>
 __global__ void __launch_bounds__(kThreads, H2G_AX_MINB) k_ax(OpParams<T> op, T* __restrict__ y, const TI* __restrict__ x,

@@ -231,9 +231,9 @@ int h2g_transient(h2g_solver *h, const h2g_bc *bc, int nt, int method, double to
  * three sources of a cell's coefficients (a few sweeps each on scratch vectors) and keeps the
  * fastest; it also times the FP64 CalcAX with each source (the same bits in every case).  The
  * sources: 0 the key tables with dd summed per cell, 1 the key tables with dd read from a
- * per-cell array, 2 (FP64) the stencil-class table: the distinct (plane, 7 stencil keys) pairs
- * of the grid, at most 65535 and NZ <= 255 (else not built; H2G_CLS=0 disables it), each with
- * its coefficients, and a 2-byte class index per cell.  The choices are cached per grid size and
+ * per-cell array, 2 the stencil-class table (the FP64 kernels and the FP32 smoother): the
+ * distinct (plane, 7 stencil keys) pairs of the grid, at most 65535 and NZ <= 255 (else not
+ * built; H2G_CLS=0 disables it), each with its coefficients, and a 2-byte class index per cell.  The choices are cached per grid size and
  * smoother precision for the process; H2G_RB_ROWS, H2G_RB_PLANES, H2G_RB_DD and H2G_AX_DD
  * (sources 0/1/2) in the environment force them (all four: no timing at all; a forced rows,
  * planes or source restricts the timing to it).  h2g_autotune runs the tuner now and reports its
