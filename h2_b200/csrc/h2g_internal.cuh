@@ -94,6 +94,8 @@ struct SolverState {
   int first;         // 1 until the first iteration has run (PBiCGSTAB p = r)
   unsigned int ticket;
   int passes;        // WHILE-body passes of this solve (bounds the graph loop independently)
+  double div_limit;  // > 0: stop (reason kNonFinite) once the relative residual exceeds it; set only
+                     // for the FP32-preconditioned passes of the mixed solver
 };
 
 // ---- arithmetic that must not be contracted into FMA: FP64 follows the reference's two-rounding

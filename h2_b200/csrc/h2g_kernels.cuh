@@ -135,7 +135,9 @@ __device__ void finish_stage(int stage, SolverState* st, double s1, double s2) {
       st->res = res;
       st->first = 0;
       if (res < st->tol) { st->stop = 1; st->converged = 1; st->reason = kConverged; break; }
-      if (!isfinite(res)) { st->stop = 1; st->reason = kNonFinite; break; }
+      if (!isfinite(res) || (st->div_limit > 0.0 && res > st->div_limit)) {
+        st->stop = 1; st->reason = kNonFinite; break;
+      }
       if (st->itr >= st->maxItr) { st->stop = 1; st->reason = kMaxItr; break; }
       st->rho_old = st->rho;
       st->rho = s2;
@@ -160,7 +162,7 @@ __device__ void finish_stage(int stage, SolverState* st, double s1, double s2) {
       if (st->hist && st->itr >= 1 && st->itr <= st->hist_len) st->hist[st->itr - 1] = res;
       st->res = res;
       if (res < st->tol) { st->stop = 1; st->converged = 1; st->reason = kConverged; break; }
-      if (!isfinite(res)) { st->stop = 1; st->reason = kNonFinite; }
+      if (!isfinite(res) || (st->div_limit > 0.0 && res > st->div_limit)) { st->stop = 1; st->reason = kNonFinite; }
       break;
     }
     case kStageCgBeta:  // NonUniform.jl:206-222, then the loop bound
@@ -1179,8 +1181,9 @@ __global__ void __launch_bounds__(256) k_ir_prep(long long n, const double* __re
 }
 
 // Host-controlled fields of a state: tolerance, iteration cap and residual history.
-__global__ void k_prime(SolverState* st, double tol, int maxItr, double* hist, int hist_len) {
+__global__ void k_prime(SolverState* st, double tol, int maxItr, double* hist, int hist_len, double div_limit) {
   pdl_enter();
+  st->div_limit = div_limit;
   st->tol = tol;
   st->maxItr = maxItr;
   st->hist = hist;

@@ -42,6 +42,7 @@ __global__ void k_prime_mr(SolverState* st, MultiCtl* ctl, double tol, int maxIt
     st[q].stop = 0;
     st[q].ticket = 0;
     st[q].passes = 0;
+    st[q].div_limit = 0.0;
   }
   if (q == 0) {
     ctl->ticket = 0;

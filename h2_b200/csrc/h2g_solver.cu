@@ -193,6 +193,7 @@ struct Solver {
   // cooperative preconditioner (k_precond_coop): all 10 passes of Preconditioner! in one launch
   int rb_coop = 0;          // chosen (tuner or h2g_set_coop)
   int coop_forced = -1;     // h2g_set_coop: -1 tuner, 0 off, 1 on
+  double div_limit = 0.0;   // divergence stop of the next solves' states (mixed FP32 passes only)
   int coop_blocks = 0;      // blocks of the launch: SMs x resident blocks per SM
   bool coop_barred = false; // set while h2g_batch_solve runs the handle beside others
   GridBar* gbar = nullptr;
@@ -1085,7 +1086,7 @@ static int run_graph(Solver* s, SolveGraph* G, SolverState* st, int maxItr, int 
 
 // Set the host-controlled fields of a device state (tolerance, iteration cap, history).
 static int prime_state(Solver* s, SolverState* st, double tol, int maxItr, double* hist, int hist_len) {
-  launch(s, k_prime, 1, 1, s->stream, st, tol, maxItr, hist, hist_len);
+  launch(s, k_prime, 1, 1, s->stream, st, tol, maxItr, hist, hist_len, s->div_limit);
   CKL();
   return H2G_OK;
 }
@@ -1357,6 +1358,7 @@ static int solve_mixed(Solver* s, bool cg, double tol, int maxItr, int smoother,
   // is within this factor of tol: the recomputed residual carries the rounding of A theta (ss
   // cancelling dd theta), which near 1e-8 is what separates the two.
   constexpr double kTrueSlack = 10.0;
+  constexpr double kDivergedFP32 = 1.0e4;
   int restart = 0;
   if (!s->th_prev) CK(cudaMalloc(&s->th_prev, nb));
   for (; restart < kMaxRestarts && total < maxItr; ++restart) {
@@ -1364,8 +1366,12 @@ static int solve_mixed(Solver* s, bool cg, double tol, int maxItr, int smoother,
     CK(cudaMemcpyAsync(s->th_prev, s->th, nb, cudaMemcpyDeviceToDevice, s->stream));
     h2g_result r;
     memset(&r, 0, sizeof r);
+    // a pass whose residual grows past 1e4 times its start has diverged (the FP32 smoother's
+    // rounding, amplified by the operator): it stops there, and the FP64 finish takes over
+    s->div_limit = kDivergedFP32;
     const int st = solve_krylov<float>(s, cg, tol_cur, maxItr - total, smoother, verbose && restart == 0,
                                        res_hist ? res_hist + total : nullptr, &r);
+    s->div_limit = 0.0;
     if (st == H2G_BAD_ARG || st == H2G_CUDA_ERROR || st == H2G_TIMEOUT) return st;
     ++passes;
     launches += r.launches + 3;
