@@ -76,3 +76,23 @@ def test_kernels_match_oracle_full_size(oracle, monkeypatch, nx, nz):
             assert abs(lhs - rhs) <= 1e-12 * scale, (lhs, rhs, scale)
     finally:
         s.close()
+
+
+def test_solve_960_checked_by_oracle_residual(oracle):
+    """The FP64 solve at 960x960x120 to 1e-8 (no oracle solve finishes in minutes there): the
+    oracle's CalcRK gives the same res0 as the GPU, and evaluated on the GPU's theta it finds the
+    reference's system solved to the rounding floor of a recomputed residual (the FP64 solves
+    recompute to 5e-8 to 1e-7 of res0 after their recurrence met 1e-8)."""
+    m = M.build_mode3(960, 960, 120)
+    prob = _problem(oracle, m)
+    s = _solver(m)
+    try:
+        _, res0_ref = oracle.calc_rk(prob, red_mode=oracle.RED_OMP, threads=THREADS)
+        st, res = s.solve("pbicgstab", tol=1e-8, maxItr=20000, smoother="gs")
+        assert st == 0 and res.isconverged
+        assert abs(res.res0 - res0_ref) <= 1e-12 * res0_ref
+        th = s.get_theta()
+        _, tr = oracle.calc_rk(prob, theta=th, red_mode=oracle.RED_OMP, threads=THREADS)
+        assert tr / res0_ref <= 2e-7, tr / res0_ref
+    finally:
+        s.close()
